@@ -1,0 +1,80 @@
+"""ctypes binding of ``libhc.so`` (the C ABI in ``include/hc.h``).
+
+The library is built in-tree by ``deepcharacters_b200.build``.  There is no
+fallback: if the library is missing or fails to load, every op raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libhc.so")
+
+_lib = None
+
+c_int_p = C.POINTER(C.c_int32)
+c_i64_p = C.POINTER(C.c_int64)
+vp = C.c_void_p
+
+# name -> argument types (all functions return hc_status / int32 unless listed)
+_SIGS: dict[str, list] = {
+    "hc_renderer_create": [C.POINTER(vp), vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                           C.c_int32, C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.c_char_p],
+    "hc_renderer_destroy": [vp],
+    "hc_renderer_reserve": [vp, C.c_int32],
+    "hc_renderer_set_tuning": [vp, C.c_int32, C.c_int32],
+    "hc_renderer_forward": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp],
+    "hc_renderer_forward_ex": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
+                               vp, vp, vp],
+    "hc_renderer_stats": [vp, vp, c_i64_p, c_i64_p],
+}
+
+_RESTYPES = {"hc_last_error": C.c_char_p, "hc_version": C.c_char_p}
+
+
+class HcError(RuntimeError):
+    """A C-ABI call returned a non-zero hc_status."""
+
+    def __init__(self, fn: str, status: int, msg: str):
+        super().__init__(f"{fn} failed (status {status}): {msg}")
+        self.status = status
+
+
+def lib() -> C.CDLL:
+    """Load libhc.so once; raises if it is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m deepcharacters_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    for name, rt in _RESTYPES.items():
+        getattr(L, name).restype = rt
+        getattr(L, name).argtypes = []
+    for name, args in _SIGS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int32
+    _lib = L
+    return L
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS) + list(_RESTYPES)
+
+
+def call(name: str, *args) -> None:
+    st = getattr(lib(), name)(*args)
+    if st != 0:
+        msg = lib().hc_last_error().decode(errors="replace")
+        raise HcError(name, st, msg)
+
+
+def ptr(t) -> int | None:
+    """Device (or host) address of a tensor / array, None for None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data

@@ -1,0 +1,176 @@
+// Shared state and device helpers of the rasterizer (forward and adjoint).
+//
+// Layout in HBM (V = B*C views, T = tiles per view):
+//   ViewCam   cams[V]             camera set-up, one per view
+//   TriFrame  tri_frame[B*F]      per-frame triangle constants (scaled vertices, plane normal)
+//   TriView   tri_view[V*F]       per-view triangle constants (ray-plane numerator, pixel bbox)
+//   int2      tile_state[V*T]     (binned count, spill slot + 1)
+//   int       bins[V*T*CAP]       triangle ids per tile
+//   int4      spill[S]            (view, tile, triangle) pairs beyond CAP
+//   u64       spill_keys[K*TS*TS] packed (depth_q << 32 | triangle) per spilled tile pixel
+#pragma once
+
+#include "hc_common.cuh"
+#include "hc_math.cuh"
+
+namespace hc {
+
+enum AlbedoMode { kVertexColor = 0, kTextured, kNormal, kLighting, kForegroundMask, kPosition, kDepth, kUV };
+enum ShadingMode { kShaded = 0, kShadeless };
+enum NormalMapMode { kNmOriginal = 0, kNmHitPosition, kNmNone, kNmFace };
+
+struct ViewCam {
+    float invP[16];  // inverse(K * E), row-major 4x4
+    float invE[16];  // inverse(E)
+    float ext[12];   // world -> camera, row-major 3x4
+    float intr[9];   // row-major 3x3
+    float ro[3];     // ray origin (camera centre)
+    float ro_s[3];   // ray origin / 1000
+};
+
+struct TriFrame {    // 48 bytes: s0.xyz n.x | s1.xyz n.y | s2.xyz n.z
+    float4 a, b, c;
+};
+
+struct TriView {     // 16 bytes
+    float num;       // dot(s0, n) - dot(ro_s, n)
+    int x01;         // bbox x0 | x1 << 16
+    int y01;         // bbox y0 | y1 << 16
+    int pad;
+};
+
+struct RasterStats {
+    unsigned long long binned;
+    unsigned long long spilled;
+    int spill_tiles;
+    int overflow;      // bit 0: spill list full, bit 1: spill tile slots exhausted
+};
+
+// Pixel-centre camera ray (reference getRayCuda2 / backprojectPixelCuda,
+// CudaRenderer/cpp/src/Utils/CameraUtil.h:223-258): the pixel centre is lifted
+// to depth 1000 through inv(K*E) and the direction from the camera centre is
+// normalised with rsqrtf.
+__device__ __forceinline__ float3 pixel_ray(const ViewCam& c, int px, int py) {
+    const float u = px + 0.5f;
+    const float v = py + 0.5f;
+    const float4 tp = make_float4(u * 1000.f, v * 1000.f, 1000.f, 1.f);
+    const float4 r0 = make_float4(c.invP[0], c.invP[1], c.invP[2], c.invP[3]);
+    const float4 r1 = make_float4(c.invP[4], c.invP[5], c.invP[6], c.invP[7]);
+    const float4 r2 = make_float4(c.invP[8], c.invP[9], c.invP[10], c.invP[11]);
+    const float3 q = make_float3(dot(r0, tp), dot(r1, tp), dot(r2, tp));
+    return normalize3(q - make_float3(c.ro[0], c.ro[1], c.ro[2]));
+}
+
+struct TriS {
+    float3 s0, s1, s2, n;
+};
+
+__device__ __forceinline__ TriS tri_from(const TriFrame& f) {
+    TriS t;
+    t.s0 = make_float3(f.a.x, f.a.y, f.a.z);
+    t.s1 = make_float3(f.b.x, f.b.y, f.b.z);
+    t.s2 = make_float3(f.c.x, f.c.y, f.c.z);
+    t.n = make_float3(f.a.w, f.b.w, f.c.w);
+    return t;
+}
+
+// Ray / triangle test of the reference (rayTriangleIntersect,
+// CudaRenderer/cpp/src/Utils/RendererUtil.h:26-101) with the per-triangle and
+// per-view terms hoisted: s* = vertices / 1000, n = cross(s1 - s0, s2 - s0),
+// num = dot(s0, n) - dot(origin / 1000, n).  Same operations in the same order
+// per pixel, so hit decisions, t and the barycentrics (a weights s0, b weights
+// s1) match the reference bit for bit.
+__device__ __forceinline__ bool ray_tri(float3 ro_s, float3 dir, const TriS& T, float num,
+                                        float& t, float& a, float& b) {
+    const float ndr = dot(dir, T.n);
+    if (fabsf(ndr) < 0.0000001f) return false;
+    t = num / ndr;
+    if (t < 0.f) return false;
+    const float3 P = ro_s + t * dir;
+    float3 C = cross(T.s1 - T.s0, P - T.s0);
+    if (dot(T.n, C) < 0.f) return false;
+    C = cross(T.s2 - T.s1, P - T.s1);
+    if ((a = dot(T.n, C)) < 0.f) return false;
+    C = cross(T.s0 - T.s2, P - T.s2);
+    if ((b = dot(T.n, C)) < 0.f) return false;
+    const float denom = dot(T.n, T.n);
+    a /= denom;
+    b /= denom;
+    return true;
+}
+
+// Hit accepted by the depth pass: barycentric window of
+// CUDABasedRasterization.cu:243 and the quantised depth int(t * 1e4) of :247-250.
+__device__ __forceinline__ bool raster_hit(float3 ro_s, float3 dir, const TriS& T, float num,
+                                           int& depth_q, float& a, float& b) {
+    float t;
+    if (!ray_tri(ro_s, dir, T, num, t, a, b)) return false;
+    if (!((a >= -0.001f) && (b >= -0.001f) && (a <= 1.001f) && (b <= 1.001f))) return false;
+    depth_q = (int)(t * 10000.f);
+    return true;
+}
+
+// World -> camera -> pixel projection (reference getCamSpacePoint and
+// projectPointFloat3, CudaRenderer/cpp/src/Utils/CameraUtil.h:141-186).
+__device__ __forceinline__ float3 project_point(const float* ext, const float* intr, float3 p) {
+    const float4 h = make_float4(p.x, p.y, p.z, 1.f);
+    const float3 cs = make_float3(dot(make_float4(ext[0], ext[1], ext[2], ext[3]), h),
+                                  dot(make_float4(ext[4], ext[5], ext[6], ext[7]), h),
+                                  dot(make_float4(ext[8], ext[9], ext[10], ext[11]), h));
+    const float3 d1 = cs * make_float3(intr[0], intr[1], intr[2]);
+    const float3 d2 = cs * make_float3(intr[3], intr[4], intr[5]);
+    const float3 d3 = cs * make_float3(intr[6], intr[7], intr[8]);
+    float x = d1.x + d1.y + d1.z;
+    float y = d2.x + d2.y + d2.z;
+    float z = d3.x + d3.y + d3.z;
+    if (z > 0.0000001f) {
+        x /= z;
+        y /= z;
+    } else {
+        z = 0.00001f;
+        x /= z;
+        y /= z;
+    }
+    return make_float3(x, y, z);
+}
+
+// Second-order SH shading of an albedo (reference getShading,
+// CudaRenderer/cpp/src/Utils/RendererUtil.h:135-173), one band set per channel.
+__device__ __forceinline__ float sh_channel(const float* s, float3 d, float3 d2) {
+    float r = s[0];
+    r += s[1] * d.y;
+    r += s[2] * d.z;
+    r += s[3] * d.x;
+    r += s[4] * (d.x * d.y);
+    r += s[5] * (d.z * d.y);
+    r += s[6] * (3.f * d2.z - 1.f);
+    r += s[7] * (d.x * d.z);
+    r += s[8] * (d2.x - d2.y);
+    return r;
+}
+
+__device__ __forceinline__ float3 sh_illum(const float* sh, float3 n) {
+    const float3 n2 = n * n;
+    return make_float3(sh_channel(sh, n, n2), sh_channel(sh + 9, n, n2), sh_channel(sh + 18, n, n2));
+}
+
+struct Topology {
+    int N = 0, F = 0;
+    DevBuf faces;        // int3[F]
+    DevBuf vf;           // int[3F]  vertex -> faces, increasing face id
+    DevBuf vf_id;        // int2[N]  (start, count)
+    DevBuf texcoords;    // float[6F]
+    bool has_texcoords = false;
+};
+
+struct RasterWorkspace {
+    int cap_views = 0;   // views the buffers are sized for
+    int tile = 16;
+    int bin_cap = 512;
+    int tiles_x = 0, tiles_y = 0;
+    long long spill_cap = 0;
+    int spill_tile_cap = 0;
+    DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;
+};
+
+}  // namespace hc

@@ -1,0 +1,627 @@
+// Forward rasterizer: camera set-up, vertex normals, triangle set-up with
+// screen-tile binning, spill-over raster and the per-tile visibility resolve
+// fused with barycentric / face-id / albedo / SH shading output.
+//
+// Reference behaviour (CudaRenderer/cpp/src/Renderer/CUDABasedRasterization.cu):
+// one thread per (view, triangle) loops over the triangle's pixel bbox twice,
+// first an int atomicMin on the quantised depth, then a racy write of every
+// triangle whose depth equals the minimum.  Here each pixel is owned by one
+// thread of its tile's CTA: the triangles binned to the tile are staged in
+// shared memory and every thread keeps the minimum (depth_q, triangle) of its
+// pixel in registers, so the common path has no atomics and the winner among
+// equal depths is deterministic (smallest triangle id).  Triangles beyond the
+// tile's bin capacity go through a spill list resolved with a 64-bit packed
+// atomicMin and merged afterwards.
+#include <algorithm>
+
+#include "renderer.cuh"
+
+namespace hc {
+
+// ---------------------------------------------------------------------------
+// camera set-up: one thread per view (reference initializeCamerasDevice,
+// CUDABasedRasterization.cu:23-67, which runs <<<1,1>>> per frame)
+// ---------------------------------------------------------------------------
+__global__ void k_view_setup(int V, const float* __restrict__ extr, const float* __restrict__ intr,
+                             ViewCam* __restrict__ cams) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const float* e = extr + 12 * (long long)v;
+    const float* k = intr + 9 * (long long)v;
+    M44 E, K;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        E.e[i] = (i % 5 == 0) ? 1.f : 0.f;
+        K.e[i] = (i % 5 == 0) ? 1.f : 0.f;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        K.e[4 * r + 0] = k[3 * r + 0];
+        K.e[4 * r + 1] = k[3 * r + 1];
+        K.e[4 * r + 2] = k[3 * r + 2];
+        K.e[4 * r + 3] = 0.f;
+        E.e[4 * r + 0] = e[4 * r + 0];
+        E.e[4 * r + 1] = e[4 * r + 1];
+        E.e[4 * r + 2] = e[4 * r + 2];
+        E.e[4 * r + 3] = e[4 * r + 3];
+    }
+    const M44 invE = inverse44(E);
+    const M44 invP = inverse44(mul44(K, E));
+    ViewCam& c = cams[v];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        c.invP[i] = invP.e[i];
+        c.invE[i] = invE.e[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 12; ++i) c.ext[i] = e[i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) c.intr[i] = k[i];
+    // camera centre: last column of inv(E), dehomogenised
+    float4 o = make_float4(invE.e[3], invE.e[7], invE.e[11], invE.e[15]);
+    const float w = o.w;
+    o.x /= w;
+    o.y /= w;
+    o.z /= w;
+    c.ro[0] = o.x;
+    c.ro[1] = o.y;
+    c.ro[2] = o.z;
+    c.ro_s[0] = o.x / 1000.f;
+    c.ro_s[1] = o.y / 1000.f;
+    c.ro_s[2] = o.z / 1000.f;
+}
+
+// ---------------------------------------------------------------------------
+// vertex normals: unnormalised sum of incident face normals, in increasing
+// face order (reference renderFaceNormalDevice / renderVertexNormalDevice,
+// CUDABasedRasterization.cu:122-174, computed once per frame and written for
+// every camera of the [B,C,N,3] output)
+// ---------------------------------------------------------------------------
+__global__ void k_vertex_normals(int B, int C, int N, const int3* __restrict__ faces,
+                                 const int* __restrict__ vf, const int2* __restrict__ vf_id,
+                                 const float* __restrict__ verts, float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * N) return;
+    const int b = (int)(i / N);
+    const int v = (int)(i % N);
+    const float* P = verts + (long long)b * N * 3;
+    const int2 r = vf_id[v];
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = r.x; k < r.x + r.y; ++k) {
+        const int3 f = faces[vf[k]];
+        const float3 v0 = ld3(P + 3 * f.x), v1 = ld3(P + 3 * f.y), v2 = ld3(P + 3 * f.z);
+        const float3 fn = cross(v1 - v0, v2 - v0);
+        if (k == r.x) {
+            s = fn;
+        } else {
+            s.x = s.x + fn.x;
+            s.y = s.y + fn.y;
+            s.z = s.z + fn.z;
+        }
+    }
+    for (int c = 0; c < C; ++c) st3(out + (((long long)b * C + c) * N + v) * 3, s);
+}
+
+// ---------------------------------------------------------------------------
+// per-frame triangle constants
+// ---------------------------------------------------------------------------
+__global__ void k_tri_frame(int B, int F, int N, const int3* __restrict__ faces,
+                            const float* __restrict__ verts, TriFrame* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * F) return;
+    const int b = (int)(i / F);
+    const int f = (int)(i % F);
+    const float* P = verts + (long long)b * N * 3;
+    const int3 id = faces[f];
+    const float3 s0 = ld3(P + 3 * id.x) / 1000.f;
+    const float3 s1 = ld3(P + 3 * id.y) / 1000.f;
+    const float3 s2 = ld3(P + 3 * id.z) / 1000.f;
+    const float3 n = cross(s1 - s0, s2 - s0);
+    TriFrame t;
+    t.a = make_float4(s0.x, s0.y, s0.z, n.x);
+    t.b = make_float4(s1.x, s1.y, s1.z, n.y);
+    t.c = make_float4(s2.x, s2.y, s2.z, n.z);
+    out[i] = t;
+}
+
+// ---------------------------------------------------------------------------
+// per-view triangle set-up and screen-tile binning
+//
+// The pixel bbox is the reference's projectFacesDevice (CUDABasedRasterization.cu:
+// 184-208): projected vertex extent +-0.5 px, clamped to the image, truncated to
+// int.  Each (view, triangle) appends itself to every tile its bbox touches.
+// Lanes of a warp that hit the same tile share one atomicAdd on the tile
+// counter (match + ballot + popc); entries beyond the tile's capacity go to
+// the spill list.
+// ---------------------------------------------------------------------------
+__global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tiles_x, int tiles_y, int cap,
+                      const int3* __restrict__ faces, const float* __restrict__ verts,
+                      const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
+                      TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
+                      int4* __restrict__ spill, long long spill_cap, unsigned long long* __restrict__ spill_keys,
+                      int spill_tile_cap, RasterStats* __restrict__ stats) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const bool live = i < (long long)V * F;
+    int view = 0, f = 0;
+    int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
+    if (live) {
+        view = (int)(i / F);
+        f = (int)(i % F);
+        const int b = view / C;
+        const ViewCam& cam = cams[view];
+        const float* P = verts + (long long)b * N * 3;
+        const int3 id = faces[f];
+        const float3 p0 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.x));
+        const float3 p1 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.y));
+        const float3 p2 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.z));
+        x0 = (int)fmaxf(fminf(p0.x, fminf(p1.x, p2.x)) - 0.5f, 0.f);
+        y0 = (int)fmaxf(fminf(p0.y, fminf(p1.y, p2.y)) - 0.5f, 0.f);
+        x1 = (int)fminf(fmaxf(p0.x, fmaxf(p1.x, p2.x)) + 0.5f, (float)(W - 1));
+        y1 = (int)fminf(fmaxf(p0.y, fmaxf(p1.y, p2.y)) + 0.5f, (float)(H - 1));
+        const TriS T = tri_from(tri_frame[(long long)b * F + f]);
+        const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
+        TriView tv;
+        tv.num = dot(T.s0, T.n) - dot(ro_s, T.n);
+        // x1/y1 can be negative for triangles left of / above the image
+        // (empty bbox); store them clamped to -1 so the 16-bit packing keeps
+        // the bbox empty.
+        // x0/y0 beyond the image also mean an empty bbox (x1 <= W-1); clamp
+        // them to W/H so they fit the 16-bit field.
+        const int cx1 = max(x1, -1), cy1 = max(y1, -1);
+        const int cx0 = min(x0, W), cy0 = min(y0, H);
+        tv.x01 = (cx0 & 0xffff) | (cx1 << 16);
+        tv.y01 = (cy0 & 0xffff) | (cy1 << 16);
+        tv.pad = 0;
+        tri_view[i] = tv;
+    }
+    const bool nonempty = live && x1 >= x0 && y1 >= y0;
+    int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
+    if (nonempty) {
+        tx0 = x0 / TS;
+        tx1 = x1 / TS;
+        ty0 = y0 / TS;
+        ty1 = y1 / TS;
+    }
+    const int T = tiles_x * tiles_y;
+    const int ntx = tx1 - tx0 + 1;
+    const int nt = nonempty ? ntx * (ty1 - ty0 + 1) : 0;
+    // lanes walk their tile lists in lock step; same-tile lanes aggregate
+    int maxnt = nt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
+    unsigned long long nbinned = 0;
+    const unsigned lane = threadIdx.x & 31;
+    for (int k = 0; k < maxnt; ++k) {
+        const bool act = k < nt;
+        long long key = -1;
+        if (act) {
+            const int tx = tx0 + k % ntx;
+            const int ty = ty0 + k / ntx;
+            key = (long long)view * T + ty * tiles_x + tx;
+        }
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        if (!act) continue;
+        const int leader = __ffs(same) - 1;
+        const int rank = __popc(same & ((1u << lane) - 1u));
+        int base = 0;
+        if ((int)lane == leader) base = atomicAdd(&tile_state[key].x, __popc(same));
+        base = __shfl_sync(same, base, leader);
+        const int slot = base + rank;
+        if (slot < cap) {
+            bins[key * cap + slot] = f;
+            ++nbinned;
+        } else {
+            if (slot == cap) {
+                // first overflow of this tile: claim a spill key block and clear it
+                const int ks = atomicAdd(&stats->spill_tiles, 1);
+                if (ks < spill_tile_cap) {
+                    unsigned long long* kp = spill_keys + (long long)ks * TS * TS;
+                    for (int p = 0; p < TS * TS; ++p) kp[p] = ~0ull;
+                    tile_state[key].y = ks + 1;
+                } else {
+                    atomicOr(&stats->overflow, 2);
+                }
+            }
+            const unsigned long long si = atomicAdd(&stats->spilled, 1ull);
+            if ((long long)si < spill_cap) {
+                const int tile = (int)(key - (long long)view * T);
+                spill[si] = make_int4(view, tile, f, 0);
+            } else {
+                atomicOr(&stats->overflow, 1);
+            }
+        }
+    }
+    // one counter update per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nbinned += __shfl_xor_sync(0xffffffffu, nbinned, o);
+    if (lane == 0 && nbinned) atomicAdd(&stats->binned, nbinned);
+}
+
+__device__ __forceinline__ void unpack_bbox(const TriView& tv, int& x0, int& x1, int& y0, int& y1) {
+    x0 = tv.x01 & 0xffff;
+    x1 = tv.x01 >> 16;
+    y0 = tv.y01 & 0xffff;
+    y1 = tv.y01 >> 16;
+}
+
+// ---------------------------------------------------------------------------
+// spill raster: (view, tile, triangle) items beyond the bin capacity, one
+// thread each, 64-bit packed atomicMin per pixel of tile x bbox.  With
+// `count_depth` set (diagnostics) the pass instead counts, per pixel, the
+// spilled triangles that reach the final depth.
+// ---------------------------------------------------------------------------
+__global__ void k_spill(int C, int F, int W, int H, int TS, int tiles_x,
+                        const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
+                        const TriView* __restrict__ tri_view, const int2* __restrict__ tile_state,
+                        const int4* __restrict__ spill, long long spill_cap, int spill_tile_cap,
+                        unsigned long long* __restrict__ spill_keys, const RasterStats* __restrict__ stats,
+                        const int* __restrict__ count_depth, int* __restrict__ tie_out, int T) {
+    const long long n = min((long long)stats->spilled, spill_cap);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int4 it = spill[i];
+        const int view = it.x, tile = it.y, f = it.z;
+        const int ks = tile_state[(long long)view * T + tile].y - 1;
+        if (ks < 0 || ks >= spill_tile_cap) continue;
+        const ViewCam& cam = cams[view];
+        const TriView tv = tri_view[(long long)view * F + f];
+        const TriS Tr = tri_from(tri_frame[(long long)(view / C) * F + f]);
+        const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
+        int x0, x1, y0, y1;
+        unpack_bbox(tv, x0, x1, y0, y1);
+        const int tx = tile % tiles_x, ty = tile / tiles_x;
+        const int px0 = max(x0, tx * TS), px1 = min(x1, min(tx * TS + TS - 1, W - 1));
+        const int py0 = max(y0, ty * TS), py1 = min(y1, min(ty * TS + TS - 1, H - 1));
+        for (int py = py0; py <= py1; ++py)
+            for (int px = px0; px <= px1; ++px) {
+                const float3 dir = pixel_ray(cam, px, py);
+                int dq;
+                float a, b;
+                if (!raster_hit(ro_s, dir, Tr, tv.num, dq, a, b)) continue;
+                const int local = (py - ty * TS) * TS + (px - tx * TS);
+                if (count_depth) {
+                    const long long pix = ((long long)view * H + py) * W + px;
+                    if (dq == count_depth[pix]) atomicAdd(&tie_out[pix], 1);
+                } else {
+                    const unsigned long long key = ((unsigned long long)(unsigned)dq << 32) | (unsigned)f;
+                    atomicMin(&spill_keys[(long long)ks * TS * TS + local], key);
+                }
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// tile resolve + shading
+// ---------------------------------------------------------------------------
+struct ShadeArgs {
+    int B, C, N, F, W, H;
+    int albedo, shading;
+    const int3* faces;
+    const float* texcoords;
+    const float* verts;
+    const float* colors;
+    const float* texture;
+    int tex_w, tex_h;
+    const float* sh;
+    const float* vnormal;  // [B,C,N,3]
+    float* bary;
+    int* face;
+    float* render;
+    int* depth_q;
+    int* tie_count;
+};
+
+__device__ __forceinline__ float3 shade_pixel(const ShadeArgs& A, const ViewCam& cam, int view, int b, int f,
+                                              float a, float bb, float3 dir) {
+    const int3 id = A.faces[f];
+    const float* VN = A.vnormal + ((long long)view * A.N) * 3;
+    const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
+    float3 pn = n0 * a + n1 * bb + n2 * (1.f - a - bb);
+    pn = pn / length3(pn);
+    if (dot(pn, dir) > 0.f) pn = -pn;
+    float3 color = make_float3(0.f, 0.f, 0.f);
+    switch (A.albedo) {
+        case kTextured: {
+            const float* tc = A.texcoords + (long long)f * 6;
+            const float2 t0 = make_float2(tc[0], 1.f - tc[1]);
+            const float2 t1 = make_float2(tc[2], 1.f - tc[3]);
+            const float2 t2 = make_float2(tc[4], 1.f - tc[5]);
+            float2 uv = t0 * a + t1 * bb + t2 * (1.f - a - bb);
+            uv.x = uv.x * A.tex_w;
+            uv.y = uv.y * A.tex_h;
+            uv.x = fmaxf(uv.x, 0.f);
+            uv.x = fminf(uv.x, (float)(A.tex_w - 1));
+            uv.y = fmaxf(uv.y, 0.f);
+            uv.y = fminf(uv.y, (float)(A.tex_h - 1));
+            const int lu = (int)(uv.x - 0.5f);
+            const int lv = (int)(uv.y - 0.5f);
+            const float* T = A.texture + (long long)b * A.tex_h * A.tex_w * 3;
+            color = ld3(T + 3LL * A.tex_w * lv + 3 * lu);
+            break;
+        }
+        case kVertexColor: {
+            const float* Cc = A.colors + (long long)b * A.N * 3;
+            const float3 c0 = ld3(Cc + 3 * id.x), c1 = ld3(Cc + 3 * id.y), c2 = ld3(Cc + 3 * id.z);
+            color = make_float3(c0.x * a + c1.x * bb + c2.x * (1.f - a - bb),
+                                c0.y * a + c1.y * bb + c2.y * (1.f - a - bb),
+                                c0.z * a + c1.z * bb + c2.z * (1.f - a - bb));
+            break;
+        }
+        case kNormal:
+            color = make_float3((1.f + pn.x) / 2.f, (1.f + pn.y) / 2.f, (1.f + pn.z) / 2.f);
+            break;
+        case kLighting:
+        case kForegroundMask:
+            color = make_float3(1.f, 1.f, 1.f);
+            break;
+        case kPosition:
+        case kDepth: {
+            const float* P = A.verts + (long long)b * A.N * 3;
+            const float3 p0 = ld3(P + 3 * id.x), p1 = ld3(P + 3 * id.y), p2 = ld3(P + 3 * id.z);
+            const float3 pos = make_float3(p0.x * a + p1.x * bb + p2.x * (1.f - a - bb),
+                                           p0.y * a + p1.y * bb + p2.y * (1.f - a - bb),
+                                           p0.z * a + p1.z * bb + p2.z * (1.f - a - bb));
+            if (A.albedo == kPosition) {
+                color = pos;
+            } else {
+                const float3 o = make_float3(cam.ro[0], cam.ro[1], cam.ro[2]);
+                const float d = length3(o - pos);
+                color = make_float3(d, d, d);
+            }
+            break;
+        }
+        case kUV: {
+            const float* tc = A.texcoords + (long long)f * 6;
+            const float2 t0 = make_float2(tc[0], 1.f - tc[1]);
+            const float2 t1 = make_float2(tc[2], 1.f - tc[3]);
+            const float2 t2 = make_float2(tc[4], 1.f - tc[5]);
+            float2 uv = t0 * a + t1 * bb + t2 * (1.f - a - bb);
+            uv.x = fminf(fmaxf(uv.x, 0.f), 1.f);
+            uv.y = fminf(fmaxf(uv.y, 0.f), 1.f);
+            color = make_float3(uv.x, uv.y, 0.f);
+            break;
+        }
+        default:
+            break;
+    }
+    if ((A.shading == kShaded && A.albedo != kNormal) || A.albedo == kLighting) {
+        const float3 L = sh_illum(A.sh + (long long)view * 27, pn);
+        color = make_float3(L.x * color.x, L.y * color.y, L.z * color.z);
+    }
+    return color;
+}
+
+struct TileTri {
+    float4 a, b, c;  // TriFrame
+    float num;
+    int x01, y01, f;
+};
+
+template <int TS>
+__global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
+                                                   const ViewCam* __restrict__ cams,
+                                                   const TriFrame* __restrict__ tri_frame,
+                                                   const TriView* __restrict__ tri_view,
+                                                   const int2* __restrict__ tile_state,
+                                                   const int* __restrict__ bins,
+                                                   const unsigned long long* __restrict__ spill_keys,
+                                                   int spill_tile_cap) {
+    constexpr int NT = TS * TS;
+    constexpr int CHUNK = NT > 256 ? 256 : NT;  // triangles staged per round
+    __shared__ TileTri s_tri[CHUNK];
+    const int tile = blockIdx.x;
+    const int view = blockIdx.y;
+    const int b = view / A.C;
+    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int lx = threadIdx.x % TS, ly = threadIdx.x / TS;
+    const int px = tx * TS + lx, py = ty * TS + ly;
+    const bool valid = px < A.W && py < A.H;
+    const ViewCam& cam = cams[view];
+    const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
+    const float3 dir = pixel_ray(cam, px, py);
+    const int2 st = tile_state[(long long)view * T + tile];
+    const int n = min(st.x, cap);
+    const int* tb = bins + ((long long)view * T + tile) * cap;
+    unsigned best_d = 0xffffffffu;
+    int best_f = 0x7fffffff;
+    int ties = 0;
+    for (int base = 0; base < n; base += CHUNK) {
+        const int k = base + threadIdx.x;
+        if (threadIdx.x < CHUNK && k < n) {
+            const int f = tb[k];
+            const TriFrame tf = tri_frame[(long long)b * A.F + f];
+            const TriView tv = tri_view[(long long)view * A.F + f];
+            TileTri t;
+            t.a = tf.a;
+            t.b = tf.b;
+            t.c = tf.c;
+            t.num = tv.num;
+            t.x01 = tv.x01;
+            t.y01 = tv.y01;
+            t.f = f;
+            s_tri[threadIdx.x] = t;
+        }
+        __syncthreads();
+        const int m = min(CHUNK, n - base);
+        if (valid) {
+            for (int j = 0; j < m; ++j) {
+                const int x01 = s_tri[j].x01, y01 = s_tri[j].y01;
+                if (px < (x01 & 0xffff) || px > (x01 >> 16) || py < (y01 & 0xffff) || py > (y01 >> 16)) continue;
+                TriFrame tf;
+                tf.a = s_tri[j].a;
+                tf.b = s_tri[j].b;
+                tf.c = s_tri[j].c;
+                int dq;
+                float a, bb;
+                if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].num, dq, a, bb)) continue;
+                const int f = s_tri[j].f;
+                if ((unsigned)dq < best_d) {
+                    best_d = (unsigned)dq;
+                    best_f = f;
+                    ties = 1;
+                } else if ((unsigned)dq == best_d) {
+                    best_f = min(best_f, f);
+                    ++ties;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!valid) return;
+    if (st.x > cap && st.y > 0 && st.y <= spill_tile_cap) {
+        const unsigned long long key = spill_keys[(long long)(st.y - 1) * NT + threadIdx.x];
+        if (key != ~0ull) {
+            const unsigned kd = (unsigned)(key >> 32);
+            const int kf = (int)(key & 0xffffffffu);
+            if (kd < best_d) {
+                best_d = kd;
+                best_f = kf;
+                ties = 0;  // spilled ties are added by the diagnostics pass
+            } else if (kd == best_d) {
+                best_f = min(best_f, kf);
+            }
+        }
+    }
+    const long long pix = ((long long)view * A.H + py) * A.W + px;
+    if (best_d == 0xffffffffu) {
+        A.face[pix] = -1;
+        A.bary[2 * pix + 0] = 0.f;
+        A.bary[2 * pix + 1] = 0.f;
+        A.render[3 * pix + 0] = 0.f;
+        A.render[3 * pix + 1] = 0.f;
+        A.render[3 * pix + 2] = 0.f;
+        if (A.depth_q) A.depth_q[pix] = 0x7fffffff;
+        if (A.tie_count) A.tie_count[pix] = 0;
+        return;
+    }
+    // recompute the winner's barycentrics (same arithmetic as the hit test)
+    const TriS W = tri_from(tri_frame[(long long)b * A.F + best_f]);
+    const TriView wv = tri_view[(long long)view * A.F + best_f];
+    int dq;
+    float a = 0.f, bb = 0.f;
+    raster_hit(ro_s, dir, W, wv.num, dq, a, bb);
+    A.face[pix] = best_f;
+    A.bary[2 * pix + 0] = a;
+    A.bary[2 * pix + 1] = bb;
+    const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
+    A.render[3 * pix + 0] = col.x;
+    A.render[3 * pix + 1] = col.y;
+    A.render[3 * pix + 2] = col.z;
+    if (A.depth_q) A.depth_q[pix] = (int)best_d;
+    if (A.tie_count) A.tie_count[pix] = ties;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H) {
+    const int TS = ws.tile;
+    ws.tiles_x = div_up(W, TS);
+    ws.tiles_y = div_up(H, TS);
+    const long long T = (long long)ws.tiles_x * ws.tiles_y;
+    if (views > ws.cap_views || ws.bins.bytes < (size_t)views * T * ws.bin_cap * sizeof(int)) {
+        HC_TRY(ws.cams.ensure(sizeof(ViewCam) * views));
+        HC_TRY(ws.tri_view.ensure(sizeof(TriView) * (size_t)views * F));
+        HC_TRY(ws.tile_state.ensure(sizeof(int2) * (size_t)views * T));
+        HC_TRY(ws.bins.ensure(sizeof(int) * (size_t)views * T * ws.bin_cap));
+        ws.spill_cap = std::max<long long>(1 << 20, (long long)views * F / 4);
+        HC_TRY(ws.spill.ensure(sizeof(int4) * (size_t)ws.spill_cap));
+        // one key block per spilled tile; every tile can get one while that
+        // stays under 256 MB, beyond it a sixteenth of the tiles
+        const long long all_tiles = views * T;
+        const long long per_tile = (long long)TS * TS * sizeof(unsigned long long);
+        ws.spill_tile_cap = (int)(all_tiles * per_tile <= (256ll << 20) ? all_tiles
+                                                                         : std::max<long long>(256, all_tiles / 16));
+        HC_TRY(ws.spill_keys.ensure(sizeof(unsigned long long) * (size_t)ws.spill_tile_cap * TS * TS));
+        HC_TRY(ws.stats.ensure(sizeof(RasterStats)));
+        ws.cap_views = views;
+    }
+    return HC_OK;
+}
+
+hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int W, int H,
+                         int albedo, int shading, const float* verts, const float* colors, const float* texture,
+                         int tex_h, int tex_w, const float* sh, const float* extr, const float* intr, float* bary,
+                         int* face, float* render, float* vnormal, int* depth_q, int* tie_count) {
+    const int V = B * C;
+    const int N = topo.N, F = topo.F;
+    HC_TRY(raster_reserve(ws, V, F, W, H));
+    HC_TRY(ws.tri_frame.ensure(sizeof(TriFrame) * (size_t)B * F));
+    const int TS = ws.tile;
+    const int T = ws.tiles_x * ws.tiles_y;
+    ViewCam* cams = ws.cams.as<ViewCam>();
+    TriFrame* tf = ws.tri_frame.as<TriFrame>();
+    TriView* tv = ws.tri_view.as<TriView>();
+    int2* tstate = ws.tile_state.as<int2>();
+    RasterStats* stats = ws.stats.as<RasterStats>();
+
+    HC_CUDA(cudaMemsetAsync(tstate, 0, sizeof(int2) * (size_t)V * T, s));
+    HC_CUDA(cudaMemsetAsync(stats, 0, sizeof(RasterStats), s));
+    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, extr, intr, cams);
+    HC_CHECK_LAUNCH();
+    k_vertex_normals<<<div_up((long long)B * N, 256), 256, 0, s>>>(
+        B, C, N, topo.faces.as<int3>(), topo.vf.as<int>(), topo.vf_id.as<int2>(), verts, vnormal);
+    HC_CHECK_LAUNCH();
+    k_tri_frame<<<div_up((long long)B * F, 256), 256, 0, s>>>(B, F, N, topo.faces.as<int3>(), verts, tf);
+    HC_CHECK_LAUNCH();
+    k_bin<<<div_up((long long)V * F, 256), 256, 0, s>>>(
+        V, C, F, N, W, H, TS, ws.tiles_x, ws.tiles_y, ws.bin_cap, topo.faces.as<int3>(), verts, cams, tf, tv, tstate,
+        ws.bins.as<int>(), ws.spill.as<int4>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(),
+        ws.spill_tile_cap, stats);
+    HC_CHECK_LAUNCH();
+    k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
+                                    ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(), stats,
+                                    nullptr, nullptr, T);
+    HC_CHECK_LAUNCH();
+    ShadeArgs A;
+    A.B = B;
+    A.C = C;
+    A.N = N;
+    A.F = F;
+    A.W = W;
+    A.H = H;
+    A.albedo = albedo;
+    A.shading = shading;
+    A.faces = topo.faces.as<int3>();
+    A.texcoords = topo.texcoords.as<float>();
+    A.verts = verts;
+    A.colors = colors;
+    A.texture = texture;
+    A.tex_w = tex_w;
+    A.tex_h = tex_h;
+    A.sh = sh;
+    A.vnormal = vnormal;
+    A.bary = bary;
+    A.face = face;
+    A.render = render;
+    A.depth_q = depth_q;
+    A.tie_count = tie_count;
+    const dim3 grid(T, V);
+    switch (TS) {
+        case 8:
+            k_resolve<8><<<grid, 64, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate, ws.bins.as<int>(),
+                                             ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap);
+            break;
+        case 16:
+            k_resolve<16><<<grid, 256, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate, ws.bins.as<int>(),
+                                               ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap);
+            break;
+        case 32:
+            k_resolve<32><<<grid, 1024, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate,
+                                                ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
+                                                ws.spill_tile_cap);
+            break;
+        default:
+            HC_FAIL(HC_ERR_INVALID, "unsupported tile size %d", TS);
+    }
+    HC_CHECK_LAUNCH();
+    if (tie_count && depth_q) {
+        k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
+                                        ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(),
+                                        stats, depth_q, tie_count, T);
+        HC_CHECK_LAUNCH();
+    }
+    return HC_OK;
+}
+
+}  // namespace hc

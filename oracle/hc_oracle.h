@@ -1,0 +1,50 @@
+/*
+ * CPU restatement of the reference deform-and-render chain -- TEST ORACLE.
+ *
+ * Only the tests, the smoke check and the benchmark's CPU-baseline leg load
+ * this library; the product never does.  Every function follows the
+ * reference lines cited next to it.  Each one exists in two precisions:
+ * the _f64 variant is the FP64 oracle used for error reports and finite
+ * differences, the _f32 variant is the reference arithmetic in float on the
+ * host cores (the CPU baseline).
+ *
+ * Parity pinning: the reference ships no tests, golden vectors or fixtures
+ * for this path; its own CUDA kernels, compiled unmodified from the reference
+ * tree (oracle/_ref), are the second oracle, run on the GPU, and the golden
+ * files under tests/golden were produced by them.
+ */
+#ifndef HC_ORACLE_H_
+#define HC_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Renderer forward (CUDABasedRasterization.cu:23-451 + renderBuffersGPU :553-576).
+ * Shapes as in include/hc.h.  Extra per-pixel outputs (may be NULL):
+ *   depth_q   [B,C,H,W] quantised depth int(t*1e4) of the winner, INT32_MAX if empty
+ *   tie_count [B,C,H,W] triangles reaching the winner's quantised depth
+ *   fragile   [B,C,H,W] 1 where a decision is within rounding of flipping:
+ *             a candidate within 1e-5 (relative) of an edge, or two candidates
+ *             within one depth quantum, or the winner's t*1e4 within 1e-3 of
+ *             an integer (only computed by the f64 variant).
+ * Winner among equal quantised depths: smallest face id.
+ * nthreads <= 0 uses all OpenMP threads. */
+int hco_render_forward_f64(int N, int F, const int32_t* faces, const float* texcoords, int B, int C, int W, int H,
+                           int albedo, int shading, const float* verts, const float* colors, const float* texture,
+                           int TH, int TW, const float* sh, const float* extr, const float* intr, float* bary,
+                           int32_t* face, float* render, float* vnormal, int32_t* depth_q, int32_t* tie_count,
+                           uint8_t* fragile, int nthreads);
+int hco_render_forward_f32(int N, int F, const int32_t* faces, const float* texcoords, int B, int C, int W, int H,
+                           int albedo, int shading, const float* verts, const float* colors, const float* texture,
+                           int TH, int TW, const float* sh, const float* extr, const float* intr, float* bary,
+                           int32_t* face, float* render, float* vnormal, int32_t* depth_q, int32_t* tie_count,
+                           uint8_t* fragile, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
