@@ -28,9 +28,29 @@ _SIGS: dict[str, list] = {
     "hc_renderer_forward_ex": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
                                vp, vp, vp],
     "hc_renderer_stats": [vp, vp, c_i64_p, c_i64_p],
+    "hc_renderer_set_gradient_parity": [vp, C.c_int32],
+    "hc_eg_create": [C.POINTER(vp), C.c_int32, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                     C.c_int32, vp, vp],
+    "hc_eg_destroy": [vp],
+    "hc_eg_reserve": [vp, C.c_int32],
+    "hc_eg_set_full_skinned_gradient": [vp, C.c_int32],
+    "hc_eg_forward": [vp, vp, C.c_int32] + [vp] * 11,
+    "hc_eg_backward": [vp, vp, C.c_int32] + [vp] * 11,
+    "hc_skin_create": [C.POINTER(vp), C.c_int32, vp, vp, vp, vp, vp, C.c_int32, vp, vp, vp, C.c_int32, vp, vp,
+                       C.c_int32, vp, vp, C.c_int32, vp],
+    "hc_skin_destroy": [vp],
+    "hc_skin_reserve": [vp, C.c_int32],
+    "hc_skin_set_parity": [vp, C.c_int32],
+    "hc_dq_skinning_forward": [vp, vp, C.c_int32] + [vp] * 8,
+    "hc_dq_skinning_backward": [vp, vp, C.c_int32] + [vp] * 8,
+    "hc_lb_skinning_forward": [vp, vp, C.c_int32] + [vp] * 9,
+    "hc_lb_skinning_backward": [vp, vp, C.c_int32] + [vp] * 10,
+    "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
+    "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
+                             vp, vp, vp, vp],
 }
 
-_RESTYPES = {"hc_last_error": C.c_char_p, "hc_version": C.c_char_p}
+_RESTYPES = {"hc_last_error": C.c_char_p, "hc_version": C.c_char_p, "hc_kernel_launches": C.c_int64}
 
 
 class HcError(RuntimeError):

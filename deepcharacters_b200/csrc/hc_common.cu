@@ -1,4 +1,6 @@
 // Error reporting for the C ABI.
+#include <atomic>
+
 #include "hc_common.cuh"
 
 namespace hc {
@@ -16,7 +18,11 @@ void set_error(const char* fmt, ...) {
 
 void clear_error() { g_last_error.clear(); }
 
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 }  // namespace hc
 
 extern "C" const char* hc_last_error(void) { return hc::g_last_error.c_str(); }
 extern "C" const char* hc_version(void) { return "hc-b200 0.1 (sm_100a)"; }
+extern "C" int64_t hc_kernel_launches(void) { return hc::g_launches.load(std::memory_order_relaxed); }

@@ -15,6 +15,8 @@ namespace hc {
 
 void set_error(const char* fmt, ...);
 void clear_error();
+// process-wide count of kernel launches issued by this library
+void count_launch();
 
 #define HC_FAIL(code, ...)            \
     do {                              \
@@ -29,7 +31,11 @@ void clear_error();
             HC_FAIL(HC_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
     } while (0)
 
-#define HC_CHECK_LAUNCH() HC_CUDA(cudaGetLastError())
+#define HC_CHECK_LAUNCH()         \
+    do {                          \
+        ::hc::count_launch();     \
+        HC_CUDA(cudaGetLastError()); \
+    } while (0)
 
 #define HC_REQUIRE(cond, ...)                                \
     do {                                                     \

@@ -36,8 +36,19 @@ struct TriView {     // 16 bytes
     float num;       // dot(s0, n) - dot(ro_s, n)
     int x01;         // bbox x0 | x1 << 16
     int y01;         // bbox y0 | y1 << 16
-    int pad;
+    int dqmin;       // lower bound of the quantised depth; bit 31 set = back-facing
 };
+
+// Conservative lower bound of int(t * 1e4) over the triangle: the ray
+// parameter t = num / (dir . n) is at least the plane distance |num| / |n|
+// for a unit direction; the bound is lowered by 1e-4 relative and 2 quanta
+// so float rounding of either side cannot break it.
+__device__ __forceinline__ int depth_lower_bound(float num, float3 n) {
+    const float pd = fabsf(num) / sqrtf(dot(n, n));
+    const float z = pd * 10000.f * (1.f - 1e-4f);
+    if (!(z < 2.0e9f)) return 0x7fffffff;
+    return max((int)z - 2, 0);
+}
 
 struct RasterStats {
     unsigned long long binned;

@@ -13,6 +13,12 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
                          int tex_h, int tex_w, const float* sh, const float* extr, const float* intr, float* bary,
                          int* face, float* render, float* vnormal, int* depth_q, int* tie_count);
 hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H);
+hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
+                          int W, int H, int albedo, int shading, int ifs, int tfs, const float* grad,
+                          const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
+                          const float* sh, const float* target, const float* vnormal, const float* bary,
+                          const int* face, const float* extr, const float* intr, float* vpos_grad,
+                          float* vcol_grad, float* tex_grad, float* sh_grad, int parity);
 
 static int parse_albedo(const char* m) {
     if (!m) return -1;
@@ -95,9 +101,11 @@ hc_status topology_upload(Topology& t, int N, const int32_t* faces, int F, const
 struct hc_renderer_s {
     hc::Topology topo;
     hc::RasterWorkspace ws;
+    hc::DevBuf nrm_grad;  // backward: gradient w.r.t. unnormalised vertex normals
     int C = 0, W = 0, H = 0;
     int albedo = 0, shading = 0, normal_map = hc::kNmNone;
     int image_filter = 2, texture_filter = 2;
+    int grad_parity = 0;  // 1: the reference's barycentric-Jacobian formula
 };
 
 using namespace hc;
@@ -151,7 +159,7 @@ extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, 
 static void release_all(hc_renderer_s* r) {
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
-                      &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats};
+                      &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad};
     for (DevBuf* b : bufs) b->release();
 }
 
@@ -240,5 +248,38 @@ extern "C" hc_status hc_renderer_stats(hc_renderer h, void* stream, int64_t* bin
     if (binned) *binned = (int64_t)st.binned;
     if (spilled) *spilled = (int64_t)st.spilled;
     if (st.overflow) HC_FAIL(HC_ERR_OVERFLOW, "raster spill capacity exceeded (flags %d)", st.overflow);
+    return HC_OK;
+}
+
+extern "C" hc_status hc_renderer_backward(hc_renderer h, void* stream, int32_t batch, const float* render_buffer_grad,
+                                          const float* vertex_pos, const float* vertex_color, const float* texture,
+                                          int32_t texture_height, int32_t texture_width, const float* sh_coeff,
+                                          const float* target_image, const float* vertex_normal,
+                                          const float* barycentric_buffer, const int32_t* face_buffer,
+                                          const float* extrinsics, const float* intrinsics, float* vertex_pos_grad,
+                                          float* vertex_color_grad, float* texture_grad, float* sh_coeff_grad) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    HC_REQUIRE(batch > 0, "batch must be positive (%d)", batch);
+    HC_REQUIRE(h->albedo == kVertexColor || h->albedo == kTextured,
+               "renderer gradients exist only for vertexColor and textured albedo");
+    HC_REQUIRE(render_buffer_grad && vertex_pos && target_image && vertex_normal && barycentric_buffer &&
+                   face_buffer && extrinsics && intrinsics && vertex_pos_grad,
+               "NULL input/output pointer");
+    if (h->albedo == kVertexColor) HC_REQUIRE(vertex_color && vertex_color_grad, "vertexColor mode needs colours");
+    if (h->albedo == kTextured)
+        HC_REQUIRE(texture && texture_grad && texture_width > 0 && texture_height > 0, "textured mode needs a texture");
+    if (h->shading == kShaded) HC_REQUIRE(sh_coeff && sh_coeff_grad, "shaded mode needs sh_coeff");
+    return raster_backward(h->topo, h->ws, h->nrm_grad, (cudaStream_t)stream, batch, h->C, h->W, h->H, h->albedo,
+                           h->shading, h->image_filter, h->texture_filter, render_buffer_grad, vertex_pos,
+                           vertex_color, texture, texture_height, texture_width, sh_coeff, target_image,
+                           vertex_normal, barycentric_buffer, face_buffer, extrinsics, intrinsics, vertex_pos_grad,
+                           vertex_color_grad, texture_grad, sh_coeff_grad, h->grad_parity);
+}
+
+extern "C" hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t parity) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    h->grad_parity = parity ? 1 : 0;
     return HC_OK;
 }

@@ -1,0 +1,518 @@
+// Renderer adjoint (the CudaRendererGradGpu op).
+//
+// Reference: CudaRenderer/cpp/src/Renderer/CUDABasedRasterizationGrad.cu:114-496
+// with the Jacobians of CudaRenderer/cpp/src/Utils/RendererUtil.h:241-914.
+// There, one thread per pixel scatters 9 position + 9 colour + 27 SH float
+// atomics to global memory, and in shaded mode loops over every face around
+// each of its three vertices (another ~160 atomics per pixel).  Here:
+//  * one CTA per 16x16 pixel tile, the target image tile (+ filter halo)
+//    staged in shared memory for the image-gradient taps;
+//  * the barycentric Jacobian is the exact rank-1 form (below) instead of the
+//    reference's 3x9 product (which is kept as the parity mode);
+//  * per-vertex contributions (position, colour, pixel-normal gradients) are
+//    merged inside each warp (lanes matched by vertex id, one leader sums its
+//    group) before one global reduction per vertex per warp;
+//  * SH gradients are reduced over the CTA (warp shuffles) before one atomic
+//    per coefficient;
+//  * the shaded-mode normal chain is split in two: pixels accumulate the
+//    gradient w.r.t. each vertex's unnormalised normal, then a per-vertex
+//    gather over incident faces applies d(face normal)/d(vertex) once per
+//    frame (same sum as the reference's per-pixel loops, reassociated).
+#include <algorithm>
+
+#include "renderer.cuh"
+
+namespace hc {
+
+__global__ void k_view_setup(int V, const float* __restrict__ extr, const float* __restrict__ intr,
+                             ViewCam* __restrict__ cams);
+
+namespace {
+
+constexpr int BT = 16;           // backward tile edge
+constexpr int BNT = BT * BT;     // threads per CTA
+
+struct BwdArgs {
+    int B, C, N, F, W, H;
+    int albedo, shading;
+    int ifs, tfs;
+    int tex_w, tex_h;
+    const int3* faces;
+    const float* texcoords;
+    const float* grad;      // [V,H,W,3]
+    const float* verts;     // [B,N,3]
+    const float* colors;    // [B,N,3]
+    const float* texture;   // [B,TH,TW,3]
+    const float* sh;        // [V,27]
+    const float* target;    // [V,H,W,3]
+    const float* vnormal;   // [V,N,3]
+    const float* bary;      // [V,H,W,2]
+    const int* face;        // [V,H,W]
+    float* vpos_grad;       // [B,N,3]
+    float* vcol_grad;       // [B,N,3]
+    float* tex_grad;        // [B,TH,TW,3]
+    float* sh_grad;         // [V,27]
+    float* nrm_grad;        // [B,N,3] workspace: d loss / d (unnormalised vertex normal)
+};
+
+__device__ __forceinline__ float3 unit3(int k) {
+    return make_float3(k == 0 ? 1.f : 0.f, k == 1 ? 1.f : 0.f, k == 2 ? 1.f : 0.f);
+}
+
+// d(a, b)/d(v0, v1, v2): the barycentric Jacobian of the reference's
+// dJBCDVerpos (RendererUtil.h:670-861) for a = dot(N, C1)/|N|^2 (weight of
+// v0) and b = dot(N, C2)/|N|^2 (weight of v1), in unscaled (mm) coordinates.
+// Returns false (all zero) for grazing rays or degenerate triangles.
+__device__ bool bary_jacobian(float3 o, float3 d, float3 v0, float3 v1, float3 v2, float ja[9], float jb[9]) {
+    const float3 e01 = v1 - v0, e02 = v2 - v0;
+    const float3 N = cross(e01, e02);
+    const float denom = dot(N, N);
+    const float ndr = dot(d, N);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) ja[i] = jb[i] = 0.f;
+    if (fabsf(dot(normalize3(d), normalize3(N))) < 0.001f || fabsf(denom * denom) < 0.001f) return false;
+    const float t = (dot(v0, N) - dot(o, N)) / ndr;
+    const float3 P = o + t * d;
+    const float3 E0 = v2 - v1, E1 = v0 - v2;
+    const float3 vp0 = P - v1, vp1 = P - v2;
+    const float3 C0 = cross(E0, vp0), C1 = cross(E1, vp1);
+    const float tmp0 = dot(N, C0), tmp1 = dot(N, C1);
+    const float3 v0mo = v0 - o;
+    const float v0moN = dot(v0mo, N);
+    const float inv_ndr = 1.f / ndr;
+    const float inv_ndr2 = -1.f / (ndr * ndr);
+    const float inv_den = 1.f / denom;
+    const float inv_den2 = -1.f / (denom * denom);
+#pragma unroll
+    for (int var = 0; var < 9; ++var) {
+        const int vert = var / 3;
+        const float3 ek = unit3(var % 3);
+        const float3 z = make_float3(0.f, 0.f, 0.f);
+        float3 dN;
+        if (vert == 0) dN = cross(-ek, e02) + cross(e01, -ek);
+        else if (vert == 1) dN = cross(ek, e02);
+        else dN = cross(e01, ek);
+        const float3 dv0 = vert == 0 ? ek : z;
+        const float3 dv1 = vert == 1 ? ek : z;
+        const float3 dv2 = vert == 2 ? ek : z;
+        const float dt = inv_ndr2 * dot(dN, d) * v0moN + inv_ndr * (dot(dv0, N) + dot(v0mo, dN));
+        const float3 dE0 = dv2 - dv1, dE1 = dv0 - dv2;
+        const float nd = 2.f * dot(N, dN);
+        const float dtmp0 = dot(dN, C0) + dot(N, cross(dE0, vp0) + cross(E0, dt * d - dv1));
+        const float dtmp1 = dot(dN, C1) + dot(N, cross(dE1, vp1) + cross(E1, dt * d - dv2));
+        ja[var] = dtmp0 * inv_den + tmp0 * inv_den2 * nd;
+        jb[var] = dtmp1 * inv_den + tmp1 * inv_den2 * nd;
+    }
+    return true;
+}
+
+// Sobel-like image gradient of the reference (imageGradient, RendererUtil.h:566-620):
+// weights (x, y)/(x^2+y^2) over a (2k+1)^2 window, normalised by sum |x|/(x^2+y^2);
+// zero near the border.  `x`, `y` are the (possibly fractional) sample position.
+__device__ void image_gradient(const float* img, float x, float y, int w, int h, int fs, float3& du, float3& dv) {
+    du = dv = make_float3(0.f, 0.f, 0.f);
+    if (!(x >= (float)(fs + 1) && y >= (float)(fs + 1) && x < (float)(w - (fs + 1)) && y < (float)(h - (fs + 1))))
+        return;
+    float norm = 0.f;
+    for (int j = -fs; j <= fs; ++j)
+        for (int i = -fs; i <= fs; ++i) {
+            const int idx = (int)((y + j) * w + (x + i));
+            const float3 I = ld3(img + 3LL * idx);
+            const float den = (float)(i * i + j * j);
+            float gu = 0.f, gv = 0.f;
+            if (den != 0.f) {
+                gu = (float)i / den;
+                gv = (float)j / den;
+            }
+            du += I * gu;
+            dv += I * gv;
+            norm += fabsf(gu);
+        }
+    du = du / norm;
+    dv = dv / norm;
+}
+
+// Exact barycentric Jacobian of a ray hit.  With P = o + t d = l0 v0 + l1 v1 +
+// l2 v2 (l2 = 1 - l0 - l1), perturbing vertex i moves (t, l0, l1) by
+// l_i M^-1 dv_i with M = [d, -(v0 - v2), -(v1 - v2)], so
+//   d l0 / d v_i = l_i (d x (v1 - v2)) / (d . N),
+//   d l1 / d v_i = l_i ((v0 - v2) x d) / (d . N),   N = (v1 - v0) x (v2 - v0).
+// Same function as the reference's dJBCDVerpos (RendererUtil.h:670-861) in
+// exact arithmetic, without the intersection point (better conditioned).
+// Returns false for the reference's grazing / degenerate cut-off.
+__device__ __forceinline__ bool bary_rows(float3 d, float3 v0, float3 v1, float3 v2, float3& r0, float3& r1) {
+    const float3 N = cross(v1 - v0, v2 - v0);
+    const float denom = dot(N, N);
+    if (fabsf(dot(normalize3(d), normalize3(N))) < 0.001f || fabsf(denom * denom) < 0.001f) return false;
+    const float inv = 1.f / dot(d, N);
+    r0 = cross(d, v1 - v2) * inv;
+    r1 = cross(v0 - v2, d) * inv;
+    return true;
+}
+
+constexpr int MAXFS = 4;                 // image filter sizes staged in shared memory
+constexpr int TILE_S = BT + 2 * MAXFS;   // staged target tile edge
+
+__global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams,
+                                                     int parity) {
+    __shared__ float s_red[BNT / 32][32][9];
+    __shared__ float s_sh[BNT / 32][27];
+    __shared__ float s_tgt[TILE_S * TILE_S * 3];
+    const int tile = blockIdx.x, view = blockIdx.y;
+    const int b = view / A.C;
+    const bool shaded = A.shading == kShaded;
+    const bool vcol = A.albedo == kVertexColor;
+    const bool textured = A.albedo == kTextured;
+    const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
+    const int px = tx0 + threadIdx.x % BT;
+    const int py = ty0 + threadIdx.x / BT;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const float* tgt = A.target + (long long)view * A.H * A.W * 3;
+    // stage the target tile with the filter halo (clipped to the image)
+    const bool staged = A.ifs <= MAXFS;
+    if (staged) {
+        const int e = BT + 2 * A.ifs;
+        for (int i = threadIdx.x; i < e * e; i += BNT) {
+            const int yy = ty0 - A.ifs + i / e, xx = tx0 - A.ifs + i % e;
+            float3 v = make_float3(0.f, 0.f, 0.f);
+            if (xx >= 0 && yy >= 0 && xx < A.W && yy < A.H) v = ld3(tgt + 3 * ((long long)yy * A.W + xx));
+            st3(s_tgt + 3 * i, v);
+        }
+    }
+    __syncthreads();
+    float shg[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) shg[k] = 0.f;
+    const long long pix = ((long long)view * A.H + py) * A.W + px;
+    const int f = (px < A.W && py < A.H) ? A.face[pix] : -1;
+    int vid[3] = {-1, -1, -1};
+    float bw[3] = {0.f, 0.f, 0.f};
+    float gp[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gp[k] = 0.f;
+    float3 gA = make_float3(0.f, 0.f, 0.f), gnu = make_float3(0.f, 0.f, 0.f);
+    if (f >= 0) {
+        const ViewCam& cam = cams[view];
+        const float3 d = pixel_ray(cam, px, py);
+        const float ba = A.bary[2 * pix], bb = A.bary[2 * pix + 1];
+        const float bc = 1.f - ba - bb;
+        const int3 id = A.faces[f];
+        vid[0] = id.x;
+        vid[1] = id.y;
+        vid[2] = id.z;
+        bw[0] = ba;
+        bw[1] = bb;
+        bw[2] = bc;
+        const float* P = A.verts + (long long)b * A.N * 3;
+        const float3 v0 = ld3(P + 3 * id.x), v1 = ld3(P + 3 * id.y), v2 = ld3(P + 3 * id.z);
+        const float* VN = A.vnormal + (long long)view * A.N * 3;
+        const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
+        const float3 G = ld3(A.grad + 3 * pix);
+        const float3 frag = ba * v0 + bb * v1 + bc * v2;
+        const float3 pnu = ba * n0 + bb * n1 + bc * n2;
+        const float pnv = sqrtf(pnu.x * pnu.x + pnu.y * pnu.y + pnu.z * pnu.z);
+        float3 pn = pnu / pnv;
+        bool flipped = false;
+        if (dot(pn, d) > 0.f) {
+            pn = -pn;
+            flipped = true;
+        }
+        const float* sh = A.sh + (long long)view * 27;
+        float3 alb = make_float3(0.f, 0.f, 0.f);
+        float3 coal = make_float3(1.f, 1.f, 1.f);
+        if (shaded) coal = sh_illum(sh, pn);
+        gA = G * coal;  // d loss / d albedo
+        float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
+        const float* tcp = A.texcoords + (long long)f * 6;
+        if (vcol) {
+            const float* Cc = A.colors + (long long)b * A.N * 3;
+            const float3 c0 = ld3(Cc + 3 * id.x), c1 = ld3(Cc + 3 * id.y), c2 = ld3(Cc + 3 * id.z);
+            alb = ba * c0 + bb * c1 + bc * c2;
+            gbc = make_float3(dot(gA, c0), dot(gA, c1), dot(gA, c2));
+        } else if (textured) {
+            const float2 t0 = make_float2(tcp[0], 1.f - tcp[1]);
+            const float2 t1 = make_float2(tcp[2], 1.f - tcp[3]);
+            const float2 t2 = make_float2(tcp[4], 1.f - tcp[5]);
+            float2 uv = t0 * ba + t1 * bb + t2 * bc;
+            uv.x = uv.x * A.tex_w;
+            uv.y = uv.y * A.tex_h;
+            uv.x = fminf(fmaxf(uv.x, 0.f), (float)(A.tex_w - 1));
+            uv.y = fminf(fmaxf(uv.y, 0.f), (float)(A.tex_h - 1));
+            const float LU = (int)(uv.x - 0.5f) + 0.5f, HU = (int)(uv.x - 0.5f) + 1.5f;
+            const float LV = (int)(uv.y - 0.5f) + 0.5f, HV = (int)(uv.y - 0.5f) + 1.5f;
+            const float* T = A.texture + (long long)b * A.tex_h * A.tex_w * 3;
+            const float3 cLL = ld3(T + 3LL * A.tex_w * (int)LV + 3 * (int)LU);
+            const float3 cLH = ld3(T + 3LL * A.tex_w * (int)HV + 3 * (int)LU);
+            const float3 cHL = ld3(T + 3LL * A.tex_w * (int)LV + 3 * (int)HU);
+            const float3 cHH = ld3(T + 3LL * A.tex_w * (int)HV + 3 * (int)HU);
+            // the reference's bilinear albedo used for the SH terms
+            // (CUDABasedRasterizationGrad.cu:242-243), weight pairs as written there
+            alb = (uv.y - LV) * (((uv.x - LU) * cLL) + ((HU - uv.x) * cHL)) +
+                  (HV - uv.y) * (((uv.x - LU) * cLH) + ((HU - uv.x) * cHH));
+            if (!flipped) {
+                float* tg = A.tex_grad + (long long)b * A.tex_h * A.tex_w * 3 + 3LL * ((int)LV * A.tex_w + (int)LU);
+                atomicAdd(tg + 0, gA.x);
+                atomicAdd(tg + 1, gA.y);
+                atomicAdd(tg + 2, gA.z);
+            }
+            float3 du, dv;
+            image_gradient(T, uv.x, uv.y, A.tex_w, A.tex_h, A.tfs, du, dv);
+            const float gu = dot(gA, du), gv = dot(gA, dv);
+            gbc = make_float3(gu * (t0.x * A.tex_w) + gv * (t0.y * A.tex_h), gu * (t1.x * A.tex_w) + gv * (t1.y * A.tex_h),
+                              gu * (t2.x * A.tex_w) + gv * (t2.y * A.tex_h));
+        }
+        if (shaded) {
+            // SH coefficients: G_r * albedo_r * basis(pn)
+            const float basis[9] = {1.f, pn.y, pn.z, pn.x, pn.x * pn.y, pn.z * pn.y, 3.f * pn.z * pn.z - 1.f,
+                                    pn.x * pn.z, pn.x * pn.x - pn.y * pn.y};
+            const float gl[3] = {G.x * alb.x, G.y * alb.y, G.z * alb.z};
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int k = 0; k < 9; ++k) shg[9 * c + k] = gl[c] * basis[k];
+            // d light / d normal (RendererUtil.h:371-391), then the normalisation Jacobian
+            float3 gno = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float* s = sh + 9 * c;
+                const float3 row = make_float3(s[3] + s[4] * pn.y + s[7] * pn.z + s[8] * 2.f * pn.x,
+                                               s[1] + s[4] * pn.x + s[5] * pn.z + s[8] * -2.f * pn.y,
+                                               s[2] + s[5] * pn.y + s[6] * 6.f * pn.z + s[7] * pn.x);
+                gno += gl[c] * row;
+            }
+            const float v2n = pnv * pnv, v3n = v2n * pnv;
+            const float gu = dot(gno, pnu);
+            gnu = (gno * v2n - pnu * gu) / v3n;
+            gbc += make_float3(dot(gnu, n0), dot(gnu, n1), dot(gnu, n2));
+        }
+        // model -> data: -G^T dTarget/d(u,v) d(u,v)/d(frag) d(frag)/d(v)
+        float3 m = make_float3(0.f, 0.f, 0.f);
+        {
+            const int fs = A.ifs;
+            float gu = 0.f, gv = 0.f;
+            if (px >= fs + 1 && py >= fs + 1 && px < A.W - (fs + 1) && py < A.H - (fs + 1)) {
+                // taps weighted (x, y)/(x^2 + y^2), normalised by sum |x|/(x^2 + y^2)
+                // (imageGradient, RendererUtil.h:566-620), contracted with G
+                float norm = 0.f;
+                const int e = BT + 2 * fs;
+                for (int j = -fs; j <= fs; ++j)
+                    for (int i = -fs; i <= fs; ++i) {
+                        const float den = (float)(i * i + j * j);
+                        if (den == 0.f) continue;
+                        float3 I;
+                        if (staged) {
+                            const int si = (py - ty0 + fs + j) * e + (px - tx0 + fs + i);
+                            I = make_float3(s_tgt[3 * si], s_tgt[3 * si + 1], s_tgt[3 * si + 2]);
+                        } else {
+                            I = ld3(tgt + 3 * ((long long)(py + j) * A.W + (px + i)));
+                        }
+                        const float gi = dot(G, I);
+                        gu += gi * ((float)i / den);
+                        gv += gi * ((float)j / den);
+                        norm += fabsf((float)i / den);
+                    }
+                gu /= norm;
+                gv /= norm;
+            }
+            if (gu != 0.f || gv != 0.f) {
+                const float* e = cam.ext;
+                const float* k = cam.intr;
+                const float3 cs = make_float3(e[0] * frag.x + e[1] * frag.y + e[2] * frag.z + e[3],
+                                              e[4] * frag.x + e[5] * frag.y + e[6] * frag.z + e[7],
+                                              e[8] * frag.x + e[9] * frag.y + e[10] * frag.z + e[11]);
+                const float3 Pp = make_float3(k[0] * cs.x + k[1] * cs.y + k[2] * cs.z,
+                                              k[3] * cs.x + k[4] * cs.y + k[5] * cs.z,
+                                              k[6] * cs.x + k[7] * cs.y + k[8] * cs.z);
+                if (fabsf(Pp.z) > 0.0001f) {
+                    const float iz = 1.f / Pp.z;
+                    const float dx = -Pp.x / (Pp.z * Pp.z), dy = -Pp.y / (Pp.z * Pp.z);
+                    float KE[3][3];
+#pragma unroll
+                    for (int r = 0; r < 3; ++r)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            KE[r][c] = k[3 * r + 0] * e[c] + k[3 * r + 1] * e[4 + c] + k[3 * r + 2] * e[8 + c];
+                    m.x = -(gu * (iz * KE[0][0] + dx * KE[2][0]) + gv * (iz * KE[1][0] + dy * KE[2][0]));
+                    m.y = -(gu * (iz * KE[0][1] + dx * KE[2][1]) + gv * (iz * KE[1][1] + dy * KE[2][1]));
+                    m.z = -(gu * (iz * KE[0][2] + dx * KE[2][2]) + gv * (iz * KE[1][2] + dy * KE[2][2]));
+                }
+            }
+        }
+        // data -> model through the barycentric Jacobian
+        if (parity) {
+            const float3 o = make_float3(cam.ro[0], cam.ro[1], cam.ro[2]);
+            float ja[9], jb[9];
+            bary_jacobian(o, d, v0, v1, v2, ja, jb);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) gp[k] = gbc.x * ja[k] + gbc.y * jb[k] + gbc.z * (-ja[k] - jb[k]);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                gp[3 * i + 0] += m.x * bw[i];
+                gp[3 * i + 1] += m.y * bw[i];
+                gp[3 * i + 2] += m.z * bw[i];
+            }
+        } else {
+            float3 r0, r1;
+            float3 q = m;
+            if (bary_rows(d, v0, v1, v2, r0, r1)) q += (gbc.x - gbc.z) * r0 + (gbc.y - gbc.z) * r1;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                gp[3 * i + 0] = q.x * bw[i];
+                gp[3 * i + 1] = q.y * bw[i];
+                gp[3 * i + 2] = q.z * bw[i];
+            }
+        }
+    }
+    // per-vertex contributions, merged inside the warp: lanes are matched by
+    // vertex id and the lowest lane of each group sums the group's values
+    // from shared memory and issues one reduction per value
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float* row = s_red[warp][lane];
+        row[0] = gp[3 * i];
+        row[1] = gp[3 * i + 1];
+        row[2] = gp[3 * i + 2];
+        row[3] = gA.x * bw[i];
+        row[4] = gA.y * bw[i];
+        row[5] = gA.z * bw[i];
+        row[6] = gnu.x * bw[i];
+        row[7] = gnu.y * bw[i];
+        row[8] = gnu.z * bw[i];
+        __syncwarp();
+        const int key = vid[i];
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (key >= 0 && lane == __ffs(grp) - 1) {
+            float acc[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+            for (unsigned mm = grp; mm; mm &= mm - 1) {
+                const float* r = s_red[warp][__ffs(mm) - 1];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) acc[k] += r[k];
+            }
+            const long long o3 = ((long long)b * A.N + key) * 3;
+            atomicAdd(A.vpos_grad + o3 + 0, acc[0]);
+            atomicAdd(A.vpos_grad + o3 + 1, acc[1]);
+            atomicAdd(A.vpos_grad + o3 + 2, acc[2]);
+            if (vcol) {
+                atomicAdd(A.vcol_grad + o3 + 0, acc[3]);
+                atomicAdd(A.vcol_grad + o3 + 1, acc[4]);
+                atomicAdd(A.vcol_grad + o3 + 2, acc[5]);
+            }
+            if (shaded) {
+                atomicAdd(A.nrm_grad + o3 + 0, acc[6]);
+                atomicAdd(A.nrm_grad + o3 + 1, acc[7]);
+                atomicAdd(A.nrm_grad + o3 + 2, acc[8]);
+            }
+        }
+        __syncwarp();
+    }
+    // SH: reduce over the CTA, one atomic per coefficient
+    if (shaded) {
+#pragma unroll
+        for (int k = 0; k < 27; ++k) {
+            float v = shg[k];
+#pragma unroll
+            for (int o2 = 16; o2 > 0; o2 >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o2);
+            if (lane == 0) s_sh[warp][k] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 27) {
+            float v = 0.f;
+            for (int w = 0; w < BNT / 32; ++w) v += s_sh[w][threadIdx.x];
+            if (v != 0.f) atomicAdd(A.sh_grad + (long long)view * 27 + threadIdx.x, v);
+        }
+    }
+}
+
+// Normal chain, per (frame, vertex): for every incident face g = (x, y, z)
+// with unnormalised normal N_g = (y - x) x (z - x), the gradient reaching N_g
+// is the sum of the three vertex-normal gradients; d N_g / d vertex gives
+//   x: g x (z - y),  y: (z - x) x g,  z: g x (y - x).
+__global__ void k_normal_chain(int B, int N, const int3* __restrict__ faces, const int* __restrict__ vf,
+                               const int2* __restrict__ vf_id, const float* __restrict__ verts,
+                               const float* __restrict__ nrm_grad, float* __restrict__ vpos_grad) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * N) return;
+    const int b = (int)(i / N), v = (int)(i % N);
+    const float* P = verts + (long long)b * N * 3;
+    const float* Gn = nrm_grad + (long long)b * N * 3;
+    const int2 r = vf_id[v];
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    for (int k = r.x; k < r.x + r.y; ++k) {
+        const int3 f = faces[vf[k]];
+        const float3 g = ld3(Gn + 3 * f.x) + ld3(Gn + 3 * f.y) + ld3(Gn + 3 * f.z);
+        const float3 x = ld3(P + 3 * f.x), y = ld3(P + 3 * f.y), z = ld3(P + 3 * f.z);
+        if (v == f.x) acc += cross(g, z - y);
+        else if (v == f.y) acc += cross(z - x, g);
+        else acc += cross(g, y - x);
+    }
+    float* o = vpos_grad + i * 3;
+    o[0] += acc.x;
+    o[1] += acc.y;
+    o[2] += acc.z;
+}
+
+}  // namespace
+
+hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
+                          int W, int H, int albedo, int shading, int ifs, int tfs, const float* grad,
+                          const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
+                          const float* sh, const float* target, const float* vnormal, const float* bary,
+                          const int* face, const float* extr, const float* intr, float* vpos_grad,
+                          float* vcol_grad, float* tex_grad, float* sh_grad, int parity) {
+    const int V = B * C, N = topo.N;
+    HC_TRY(ws.cams.ensure(sizeof(ViewCam) * (size_t)std::max(V, ws.cap_views)));
+    const bool shaded = shading == kShaded;
+    if (shaded) HC_TRY(nrm_ws.ensure(sizeof(float) * 3 * (size_t)B * N));
+    if (vpos_grad) HC_CUDA(cudaMemsetAsync(vpos_grad, 0, sizeof(float) * 3 * (size_t)B * N, s));
+    if (vcol_grad) HC_CUDA(cudaMemsetAsync(vcol_grad, 0, sizeof(float) * 3 * (size_t)B * N, s));
+    if (tex_grad && tex_h > 0 && tex_w > 0)
+        HC_CUDA(cudaMemsetAsync(tex_grad, 0, sizeof(float) * 3 * (size_t)B * tex_h * tex_w, s));
+    if (sh_grad) HC_CUDA(cudaMemsetAsync(sh_grad, 0, sizeof(float) * 27 * (size_t)V, s));
+    if (shaded) HC_CUDA(cudaMemsetAsync(nrm_ws.ptr, 0, sizeof(float) * 3 * (size_t)B * N, s));
+    ViewCam* cams = ws.cams.as<ViewCam>();
+    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, extr, intr, cams);
+    HC_CHECK_LAUNCH();
+    BwdArgs A;
+    A.B = B;
+    A.C = C;
+    A.N = N;
+    A.F = topo.F;
+    A.W = W;
+    A.H = H;
+    A.albedo = albedo;
+    A.shading = shading;
+    A.ifs = ifs;
+    A.tfs = tfs;
+    A.tex_w = tex_w;
+    A.tex_h = tex_h;
+    A.faces = topo.faces.as<int3>();
+    A.texcoords = topo.texcoords.as<float>();
+    A.grad = grad;
+    A.verts = verts;
+    A.colors = colors;
+    A.texture = texture;
+    A.sh = sh;
+    A.target = target;
+    A.vnormal = vnormal;
+    A.bary = bary;
+    A.face = face;
+    A.vpos_grad = vpos_grad;
+    A.vcol_grad = vcol_grad;
+    A.tex_grad = tex_grad;
+    A.sh_grad = sh_grad;
+    A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
+    const int tiles_x = div_up(W, BT), tiles_y = div_up(H, BT);
+    k_render_grad<<<dim3(tiles_x * tiles_y, V), BNT, 0, s>>>(A, tiles_x, cams, parity);
+    HC_CHECK_LAUNCH();
+    if (shaded) {
+        k_normal_chain<<<div_up((long long)B * N, 256), 256, 0, s>>>(B, N, topo.faces.as<int3>(), topo.vf.as<int>(),
+                                                                     topo.vf_id.as<int2>(), verts, nrm_ws.as<float>(),
+                                                                     vpos_grad);
+        HC_CHECK_LAUNCH();
+    }
+    return HC_OK;
+}
+
+}  // namespace hc

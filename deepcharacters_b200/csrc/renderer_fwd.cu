@@ -171,7 +171,8 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         const int cx0 = min(x0, W), cy0 = min(y0, H);
         tv.x01 = (cx0 & 0xffff) | (cx1 << 16);
         tv.y01 = (cy0 & 0xffff) | (cy1 << 16);
-        tv.pad = 0;
+        // front-facing: the plane normal points towards the camera (num < 0)
+        tv.dqmin = depth_lower_bound(tv.num, T.n) | (tv.num < 0.f ? 0 : (int)0x80000000);
         tri_view[i] = tv;
     }
     const bool nonempty = live && x1 >= x0 && y1 >= y0;
@@ -395,6 +396,8 @@ struct TileTri {
     float4 a, b, c;  // TriFrame
     float num;
     int x01, y01, f;
+    int dqmin;       // depth lower bound | back-facing flag (bit 31)
+    int pad[3];
 };
 
 template <int TS>
@@ -425,47 +428,61 @@ __global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, in
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
-    for (int base = 0; base < n; base += CHUNK) {
-        const int k = base + threadIdx.x;
-        if (threadIdx.x < CHUNK && k < n) {
-            const int f = tb[k];
-            const TriFrame tf = tri_frame[(long long)b * A.F + f];
-            const TriView tv = tri_view[(long long)view * A.F + f];
-            TileTri t;
-            t.a = tf.a;
-            t.b = tf.b;
-            t.c = tf.c;
-            t.num = tv.num;
-            t.x01 = tv.x01;
-            t.y01 = tv.y01;
-            t.f = f;
-            s_tri[threadIdx.x] = t;
-        }
-        __syncthreads();
-        const int m = min(CHUNK, n - base);
-        if (valid) {
-            for (int j = 0; j < m; ++j) {
-                const int x01 = s_tri[j].x01, y01 = s_tri[j].y01;
-                if (px < (x01 & 0xffff) || px > (x01 >> 16) || py < (y01 & 0xffff) || py > (y01 >> 16)) continue;
-                TriFrame tf;
-                tf.a = s_tri[j].a;
-                tf.b = s_tri[j].b;
-                tf.c = s_tri[j].c;
-                int dq;
-                float a, bb;
-                if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].num, dq, a, bb)) continue;
-                const int f = s_tri[j].f;
-                if ((unsigned)dq < best_d) {
-                    best_d = (unsigned)dq;
-                    best_f = f;
-                    ties = 1;
-                } else if ((unsigned)dq == best_d) {
-                    best_f = min(best_f, f);
-                    ++ties;
+    // Two passes over the tile's triangles: front-facing first, then
+    // back-facing.  A triangle whose depth lower bound exceeds the pixel's
+    // current best depth can neither win nor tie, so once the front surface
+    // is resolved most back faces are rejected without a ray test.  The
+    // result is the same minimum (depth, id) as one unordered pass.
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int base = 0; base < n; base += CHUNK) {
+            if (pass == 0 || n > CHUNK) {
+                const int k = base + threadIdx.x;
+                __syncthreads();
+                if (threadIdx.x < CHUNK && k < n) {
+                    const int f = tb[k];
+                    const TriFrame tf = tri_frame[(long long)b * A.F + f];
+                    const TriView tv = tri_view[(long long)view * A.F + f];
+                    TileTri t;
+                    t.a = tf.a;
+                    t.b = tf.b;
+                    t.c = tf.c;
+                    t.num = tv.num;
+                    t.x01 = tv.x01;
+                    t.y01 = tv.y01;
+                    t.f = f;
+                    t.dqmin = tv.dqmin;
+                    s_tri[threadIdx.x] = t;
+                }
+                __syncthreads();
+            }
+            const int m = min(CHUNK, n - base);
+            if (valid) {
+                for (int j = 0; j < m; ++j) {
+                    const int dm = s_tri[j].dqmin;
+                    if ((dm < 0) != (pass == 1)) continue;          // wrong facing for this pass
+                    if ((unsigned)(dm & 0x7fffffff) > best_d) continue;  // cannot reach the best depth
+                    const int x01 = s_tri[j].x01, y01 = s_tri[j].y01;
+                    if (px < (x01 & 0xffff) || px > (x01 >> 16) || py < (y01 & 0xffff) || py > (y01 >> 16))
+                        continue;
+                    TriFrame tf;
+                    tf.a = s_tri[j].a;
+                    tf.b = s_tri[j].b;
+                    tf.c = s_tri[j].c;
+                    int dq;
+                    float a, bb;
+                    if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].num, dq, a, bb)) continue;
+                    const int f = s_tri[j].f;
+                    if ((unsigned)dq < best_d) {
+                        best_d = (unsigned)dq;
+                        best_f = f;
+                        ties = 1;
+                    } else if ((unsigned)dq == best_d) {
+                        best_f = min(best_f, f);
+                        ++ties;
+                    }
                 }
             }
         }
-        __syncthreads();
     }
     if (!valid) return;
     if (st.x > cap && st.y > 0 && st.y <= spill_tile_cap) {

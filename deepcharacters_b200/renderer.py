@@ -80,6 +80,10 @@ class RendererEngine:
     def set_tuning(self, tile: int, bin_capacity: int):
         _lib.call("hc_renderer_set_tuning", self._h, int(tile), int(bin_capacity))
 
+    def set_gradient_parity(self, parity: bool):
+        """True: the reference's barycentric-Jacobian formula; False (default): exact closed form."""
+        _lib.call("hc_renderer_set_gradient_parity", self._h, int(bool(parity)))
+
     def stats(self) -> tuple[int, int]:
         b = C.c_int64()
         s = C.c_int64()
@@ -170,10 +174,35 @@ class _RenderFn(torch.autograd.Function):
                 torch.zeros_like(extrinsics), torch.zeros_like(intrinsics))
 
 
-def renderer_backward(engine, render_buffer_grad, vertex_pos, vertex_color, texture, sh_coeff, target_image,
-                      vertex_normal, barycentric_buffer, face_buffer, extrinsics, intrinsics):
-    """``CudaRendererGradGpu``: gradients w.r.t. vertex_pos, vertex_color, texture, sh_coeff."""
-    raise NotImplementedError("renderer backward is provided by hc_renderer_backward")
+def renderer_backward(engine: RendererEngine, render_buffer_grad, vertex_pos, vertex_color, texture, sh_coeff,
+                      target_image, vertex_normal, barycentric_buffer, face_buffer, extrinsics, intrinsics,
+                      batch: int | None = None):
+    """``CudaRendererGradGpu``: gradients w.r.t. vertex_pos, vertex_color, texture, sh_coeff.
+
+    The batch size comes from ``vertex_pos`` (CudaRendererGrad.cpp:184)."""
+    vp = _f32(vertex_pos, "vertex_pos")
+    B = int(batch if batch is not None else vp.shape[0])
+    dev = vp.device
+    g = _f32(render_buffer_grad, "render_buffer_grad")
+    vc = _f32(vertex_color, "vertex_color")
+    tex = _f32(texture, "texture")
+    sh = _f32(sh_coeff, "sh_coeff")
+    tgt = _f32(target_image, "target_image")
+    vn = _f32(vertex_normal, "vertex_normal")
+    bary = _f32(barycentric_buffer, "barycentric_buffer")
+    face = face_buffer.detach().to(torch.int32).contiguous()
+    ex = _f32(extrinsics, "extrinsics")
+    it = _f32(intrinsics, "intrinsics")
+    TH = int(tex.shape[1]) if tex is not None and tex.dim() == 4 else 0
+    TW = int(tex.shape[2]) if tex is not None and tex.dim() == 4 else 0
+    gpos = torch.empty((B, engine.N, 3), device=dev, dtype=torch.float32)
+    gcol = torch.zeros((B, engine.N, 3), device=dev, dtype=torch.float32)
+    gtex = torch.zeros((B, max(TH, 1), max(TW, 1), 3), device=dev, dtype=torch.float32)
+    gsh = torch.zeros((B, engine.C, 27), device=dev, dtype=torch.float32)
+    P = _lib.ptr
+    _lib.call("hc_renderer_backward", engine.handle, _stream(), B, P(g), P(vp), P(vc), P(tex), TH, TW, P(sh), P(tgt),
+              P(vn), P(bary), P(face), P(ex), P(it), P(gpos), P(gcol), P(gtex) if TH > 0 else None, P(gsh))
+    return gpos, gcol, gtex, gsh
 
 
 class CudaRendererGpu:

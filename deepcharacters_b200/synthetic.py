@@ -405,3 +405,23 @@ def render_scene(subdiv: int, batch: int, views: int, width: int, height: int, s
                 extr=np.tile(ex[None], (batch, 1)), intr=np.tile(it[None], (batch, 1)),
                 texcoords=spherical_uvs(verts[0], faces), target=target,
                 N=N, F=faces.shape[0], B=batch, C=views, W=width, H=height)
+
+
+def eg_scene(subdiv: int, n_nodes: int, batch: int, seed: int, k: int = 4, n_markers: int = 8,
+             delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, skinned_rot_std: float = 0.1,
+             skinned_t_std: float = 0.02 * MM, disp_std: float = 0.001 * MM):
+    """Embedded-graph inputs on a jittered icosphere: the graph (farthest-point
+    nodes, K nearest nodes per vertex, inverse-distance weights), markers on
+    random node vertices, and per-frame node rotations (Euler, rad) /
+    translations (mm) and vertex displacements."""
+    rng = rng_for(seed)
+    verts, faces = sphere_mesh(subdiv, rng)
+    g = embedded_graph(verts, n_nodes, k, rng)
+    mk_nodes = rng.choice(n_nodes, size=n_markers, replace=False).astype(np.int32) if n_markers else None
+    markers = (verts[g.node_vertex[mk_nodes]] + rng.normal(0, 5.0, (n_markers, 3))).astype(np.float32) \
+        if n_markers else None
+    f = lambda std, shape: rng.normal(0.0, std, size=shape).astype(np.float32)  # noqa: E731
+    return dict(verts=verts, faces=faces, graph=g, markers=markers, marker_node=mk_nodes,
+                dT=f(delta_t_std, (batch, n_nodes, 3)), dA=f(delta_rot_std, (batch, n_nodes, 3)),
+                sT=f(skinned_t_std, (batch, n_nodes, 3)), sA=f(skinned_rot_std, (batch, n_nodes, 3)),
+                disp=f(disp_std, (batch, verts.shape[0], 3)))

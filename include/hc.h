@@ -41,6 +41,9 @@ enum {
 const char* hc_last_error(void);
 /* Library version string. */
 const char* hc_version(void);
+/* Number of kernel launches this library has issued in this process
+ * (launches recorded into a CUDA graph count once, at capture). */
+int64_t hc_kernel_launches(void);
 
 /* ------------------------------------------------------------------------ */
 /* Rasterizer / renderer                                                     */
@@ -116,11 +119,190 @@ hc_status hc_renderer_forward_ex(hc_renderer h, void* stream, int32_t batch,
                                  int32_t* depth_q, int32_t* tie_count);
 
 /*
+ * Adjoint of the forward render (CudaRendererGradGpu).
+ * Replaces CudaRendererGrad::Compute
+ * (CudaRenderer/cpp/src/TensorflowOperators/CudaRenderer/CudaRendererGrad.cpp:6-34,241-274)
+ * and renderBuffersGradGPU (CudaRenderer/cpp/src/Renderer/CUDABasedRasterizationGrad.cu:503-514).
+ * Inputs in the op's order: render_buffer_grad [B,C,H,W,3], vertex_pos,
+ * vertex_color, texture, sh_coeff, target_image [B,C,H,W,3], vertex_normal
+ * [B,C,N,3], barycentric_buffer, face_buffer (the forward's saved outputs),
+ * extrinsics, intrinsics.  Outputs (overwritten): vertex_pos_grad [B,N,3],
+ * vertex_color_grad [B,N,3], texture_grad [B,TH,TW,3], sh_coeff_grad [B,C,27].
+ * Only vertexColor and textured albedo carry gradients (the reference
+ * registers zeros for the other modes, CudaRendererGPU.py:229-237).
+ */
+hc_status hc_renderer_backward(hc_renderer h, void* stream, int32_t batch,
+                               const float* render_buffer_grad, const float* vertex_pos,
+                               const float* vertex_color, const float* texture,
+                               int32_t texture_height, int32_t texture_width, const float* sh_coeff,
+                               const float* target_image, const float* vertex_normal,
+                               const float* barycentric_buffer, const int32_t* face_buffer,
+                               const float* extrinsics, const float* intrinsics,
+                               float* vertex_pos_grad, float* vertex_color_grad, float* texture_grad,
+                               float* sh_coeff_grad);
+
+/*
+ * Barycentric Jacobian of the adjoint.  0 (default): the exact derivative of
+ * the ray-hit barycentrics in closed form (rank 1 per vertex); 1: the
+ * reference's 3x9 formula (dJBCDVerpos, RendererUtil.h:670-861) evaluated as
+ * written.  Both are the same function; they differ by float rounding, which
+ * for the reference formula is ~1e-4 relative at millimetre scale.
+ */
+hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t parity);
+
+/*
  * Raster statistics of the last forward on this handle: triangle/tile pairs
  * binned and pairs that overflowed a tile bin and took the atomic spill path.
  * Synchronises `stream`; host output pointers, either may be NULL.
  */
 hc_status hc_renderer_stats(hc_renderer h, void* stream, int64_t* binned, int64_t* spilled);
+
+/* ------------------------------------------------------------------------ */
+/* Embedded-graph deformation                                                */
+/* ------------------------------------------------------------------------ */
+
+typedef struct hc_eg_s* hc_eg;
+
+/*
+ * Create an embedded graph over a base mesh (host arrays).  Replaces the
+ * EmbeddedGraphGpu op construction (CustomTensorFlowCPPOperators/src/
+ * CustomGPUOperators/EmbeddedGraphOperator/EmbeddedGraphGPUOp.cpp:6-25,30-120),
+ * which reads the same arrays from the character / graph files
+ * (Skeletool/Mesh/EmbeddedGraph.cpp:379-548): base vertices [N,3], faces
+ * [F,3], node -> base-vertex index [M], the vertex -> node CSR (offsets,
+ * sizes, indices, weights) and the node -> vertex CSR with the same weights,
+ * optional markers [Mk,3] with their node [Mk].
+ */
+hc_status hc_eg_create(hc_eg* out, int32_t n_vertices, const float* base_vertices, const int32_t* faces,
+                       int32_t n_faces, int32_t n_nodes, const int32_t* node_to_base_vertex,
+                       const int32_t* v2n_offsets, const int32_t* v2n_sizes, const int32_t* v2n_indices,
+                       const float* v2n_weights, const int32_t* n2v_offsets, const int32_t* n2v_sizes,
+                       const int32_t* n2v_indices, const float* n2v_weights, int32_t n_markers,
+                       const float* base_markers, const int32_t* marker_to_node);
+hc_status hc_eg_destroy(hc_eg h);
+hc_status hc_eg_reserve(hc_eg h, int32_t batch);
+/* 0 (default): skinned-rotation/translation gradients are zero, as in the
+ * reference (EmbeddedGraphGPUOpGrad.cu:136-142); 1: return them. */
+hc_status hc_eg_set_full_skinned_gradient(hc_eg h, int32_t enable);
+
+/*
+ * Forward (EmbeddedGraphGpu; EmbeddedGraphGPUOp.cu:229-240).  Inputs
+ * [B,M,3]: nodes_delta_translation, nodes_delta_rotation (Euler, rad),
+ * nodes_skinned_translation, nodes_skinned_rotation; vertex_displacements
+ * [B,N,3].  Outputs: deformed_vertices [B,N,3], deformed_normals [B,N,3]
+ * (may be NULL), deformed_markers [B,Mk,3], deformed_graph [B,M,3] (may be
+ * NULL), d_delta_rotation / d_skinned_rotation [B,M,3] (copies of the angle
+ * inputs for the gradient op; may be NULL).
+ */
+hc_status hc_eg_forward(hc_eg h, void* stream, int32_t batch, const float* nodes_delta_translation,
+                        const float* nodes_delta_rotation, const float* nodes_skinned_translation,
+                        const float* nodes_skinned_rotation, const float* vertex_displacements,
+                        float* deformed_vertices, float* deformed_normals, float* deformed_markers,
+                        float* deformed_graph, float* d_delta_rotation, float* d_skinned_rotation);
+
+/*
+ * Adjoint (EmbeddedGraphGpuGrad; EmbeddedGraphGPUOpGrad.cu:204-213):
+ * deformed_vertices_grad [B,N,3], deformed_markers_grad [B,Mk,3] (may be NULL),
+ * d_delta_a / d_skinned_a [B,M,3] -> nodes_t_grad, nodes_r_grad,
+ * nodes_skinned_t_grad, nodes_skinned_r_grad [B,M,3], vertex_displacements_grad
+ * [B,N,3].  nodes_delta_translation and vertex_displacements (the forward
+ * inputs) are only read with the full skinned gradient enabled (else NULL).
+ */
+hc_status hc_eg_backward(hc_eg h, void* stream, int32_t batch, const float* deformed_vertices_grad,
+                         const float* deformed_markers_grad, const float* d_delta_a, const float* d_skinned_a,
+                         float* nodes_t_grad, float* nodes_r_grad, float* nodes_skinned_t_grad,
+                         float* nodes_skinned_r_grad, float* vertex_displacements_grad,
+                         const float* nodes_delta_translation, const float* vertex_displacements);
+
+/* ------------------------------------------------------------------------ */
+/* Forward kinematics + dual-quaternion / linear-blend skinning              */
+/* ------------------------------------------------------------------------ */
+
+typedef struct hc_skin_s* hc_skin;
+
+/*
+ * Create a skinned character from host arrays (what the reference reads from
+ * its .character / .skeleton / .skin files, Skeletool/Character/
+ * skinnedcharacter.cpp:425-559, skeleton.cpp).  Replaces the DqSkinningGpu /
+ * LbSkinningGpu op construction (DQSkinningGPUOp.cpp:5-15,18-120;
+ * LBSkinningGPUOp.cpp:5-16).
+ *   joints: parent [J] (-1 = root, parents before children), joint_type [J]
+ *   (0 revolute, 1 prismatic), offset [J,3] (local, mm), axis [J,3] (local
+ *   unit axis), joint_scale [J] (NULL = 1);
+ *   dofs: CSR dof_offsets [D+1] over (dof_joint, dof_weight) entries; a dof
+ *   adds weight * value to each joint's parameter (dof.cpp:9-17);
+ *   skinning joints: skin_joint [S] and skin_scale [S] (NULL = 1), whose
+ *   transform is joint * scale * inverse(rest joint);
+ *   mesh: base_vertices / base_normals [N,3], skin_index [N,K] (skinning joint
+ *   per weight slot).
+ */
+hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_t* parent, const int32_t* joint_type,
+                         const float* offset, const float* axis, const float* joint_scale, int32_t n_dofs,
+                         const int32_t* dof_offsets, const int32_t* dof_joint, const float* dof_weight,
+                         int32_t n_skin, const int32_t* skin_joint, const float* skin_scale, int32_t n_vertices,
+                         const float* base_vertices, const float* base_normals, int32_t k,
+                         const int32_t* skin_index);
+hc_status hc_skin_destroy(hc_skin h);
+hc_status hc_skin_reserve(hc_skin h, int32_t batch);
+/* 1 (default): gradients reproduce the reference's formulas, including the
+ * weight-Jacobian indexing slips (DQHelper.h:121-174,
+ * LBSkinningGPUOpGrad.cu:22-32,65-74); 0: exact weight gradients. */
+hc_status hc_skin_set_parity(hc_skin h, int32_t parity);
+
+/* DqSkinningGpu forward (DQSkinningGPUOp.cpp:351-389 + DQSkinningGPUOp.cu:56-137),
+ * forward kinematics on the device: dofs [B,D], skinning_weights [B,N,K] ->
+ * skinned_vertex_positions / normals [B,N,3], global_joint_position /
+ * axis [B,J,3], dual_quaternions [B,S,8] (rotation x,y,z,w then translation
+ * x,y,z,w), output_skinning_weights [B,N,K] (copy; may be NULL). */
+hc_status hc_dq_skinning_forward(hc_skin h, void* stream, int32_t batch, const float* dofs,
+                                 const float* skinning_weights, float* skinned_vertex_positions,
+                                 float* skinned_vertex_normals, float* global_joint_position,
+                                 float* global_joint_axis, float* dual_quaternions,
+                                 float* output_skinning_weights);
+/* DqSkinningGpuGrad (DQSkinningGPUOpGrad.cu:12-217): dofs_grad [B,D] (the
+ * reference's linearised rotation-about-axis derivative), skinning_weights_grad
+ * [B,N,K]. */
+hc_status hc_dq_skinning_backward(hc_skin h, void* stream, int32_t batch,
+                                  const float* skinned_vertex_positions_grad,
+                                  const float* skinned_vertex_positions, const float* global_joint_position,
+                                  const float* global_joint_axis, const float* dual_quaternions,
+                                  const float* skinning_weights, float* dofs_grad, float* skinning_weights_grad);
+/* LbSkinningGpu forward (LBSkinningGPUOp.cu:49-113): + displacement [B,N,3];
+ * transformation [B,S,12] (rotation row-major 9, translation 3). */
+hc_status hc_lb_skinning_forward(hc_skin h, void* stream, int32_t batch, const float* dofs,
+                                 const float* skinning_weights, const float* displacement,
+                                 float* skinned_vertex_positions, float* skinned_vertex_normals,
+                                 float* global_joint_position, float* global_joint_axis, float* transformation,
+                                 float* output_skinning_weights);
+/* LbSkinningGpuGrad (LBSkinningGPUOpGrad.cu:11-168): dofs_grad [B,D],
+ * skinning_weights_grad [B,N,K], displacement_grad [B,N,3].  displacement is
+ * only read in the exact mode (parity 0). */
+hc_status hc_lb_skinning_backward(hc_skin h, void* stream, int32_t batch,
+                                  const float* skinned_vertex_positions_grad,
+                                  const float* skinned_vertex_positions, const float* global_joint_position,
+                                  const float* global_joint_axis, const float* transformation,
+                                  const float* skinning_weights, const float* displacement, float* dofs_grad,
+                                  float* skinning_weights_grad, float* displacement_grad);
+
+/* ------------------------------------------------------------------------ */
+/* Losses                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Masked L1 image loss of the training step and its gradient.
+ * Replaces the TF graph of Projects/HoloportedCharacters/HPCMeshDL.py:669-688:
+ * difference = 255 (render - target) * mask * (face >= 0),
+ * loss = sum |difference| / count_nonzero(difference),
+ * render_buffer_grad = 255 sign(difference) * mask * (face >= 0) / count.
+ * n_pixels = B*C*H*W; render/target are [n_pixels,3]; face_buffer [n_pixels];
+ * foreground_mask [n_pixels] uint8 (NULL = all ones); loss is one device
+ * float; workspace is device scratch of at least 16 bytes (its contents on
+ * entry are ignored).
+ */
+hc_status hc_image_l1_loss(void* stream, int64_t n_pixels, const float* render_buffer,
+                           const float* target_image, const int32_t* face_buffer,
+                           const uint8_t* foreground_mask, void* workspace, float* loss,
+                           float* render_buffer_grad);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,44 @@ int hco_render_forward_f32(int N, int F, const int32_t* faces, const float* texc
                            int32_t* face, float* render, float* vnormal, int32_t* depth_q, int32_t* tie_count,
                            uint8_t* fragile, int nthreads);
 
+/* Renderer adjoint (CUDABasedRasterizationGrad.cu:114-514), shapes as
+ * hc_renderer_backward in include/hc.h; outputs are overwritten. */
+int hco_render_backward_f64(int N, int F, const int32_t* faces, const float* texcoords, int B, int C, int W, int H,
+                            int albedo, int shading, int ifs, int tfs, const float* grad, const float* verts,
+                            const float* colors, const float* texture, int TH, int TW, const float* sh,
+                            const float* target, const float* vnormal, const float* bary, const int32_t* face,
+                            const float* extr, const float* intr, float* vpos_grad, float* vcol_grad,
+                            float* tex_grad, float* sh_grad, int nthreads);
+int hco_render_backward_f32(int N, int F, const int32_t* faces, const float* texcoords, int B, int C, int W, int H,
+                            int albedo, int shading, int ifs, int tfs, const float* grad, const float* verts,
+                            const float* colors, const float* texture, int TH, int TW, const float* sh,
+                            const float* target, const float* vnormal, const float* bary, const int32_t* face,
+                            const float* extr, const float* intr, float* vpos_grad, float* vcol_grad,
+                            float* tex_grad, float* sh_grad, int nthreads);
+
+/* Embedded-graph forward / adjoint (EmbeddedGraphGPUOp.cu:11-225,
+ * EmbeddedGraphGPUOpGrad.cu:9-201); full = 1 adds the skinned gradients. */
+#define HCO_EG_DECL(P)                                                                                          \
+    int hco_eg_forward_##P(int B, int N, int M, int Mk, int F, const float* base, const int32_t* faces,        \
+                           const int32_t* node_vertex, const int32_t* v2n_off, const int32_t* v2n_size,         \
+                           const int32_t* v2n_idx, const float* v2n_w, const float* markers, const int32_t* m2n, \
+                           const float* dT, const float* dA, const float* sT, const float* sA, const float* disp, \
+                           float* out_v, float* out_n, float* out_m, float* out_g);                              \
+    int hco_eg_backward_##P(int B, int N, int M, int Mk, const float* base, const int32_t* node_vertex,        \
+                            const int32_t* v2n_off, const int32_t* v2n_size, const int32_t* v2n_idx,           \
+                            const float* v2n_w, const int32_t* n2v_off, const int32_t* n2v_size,                \
+                            const int32_t* n2v_idx, const float* n2v_w, const int32_t* n2m, const float* markers, \
+                            const float* gv, const float* gm, const float* dT, const float* dA, const float* sA, \
+                            const float* disp, int full, float* gT, float* gA, float* gsT, float* gsA, float* gdisp);
+HCO_EG_DECL(f64)
+HCO_EG_DECL(f32)
+/* FP64 forward with double outputs (finite differences) */
+int hco_eg_forward_f64d(int B, int N, int M, int Mk, int F, const float* base, const int32_t* faces,
+                        const int32_t* node_vertex, const int32_t* v2n_off, const int32_t* v2n_size,
+                        const int32_t* v2n_idx, const float* v2n_w, const float* markers, const int32_t* m2n,
+                        const float* dT, const float* dA, const float* sT, const float* sA, const float* disp,
+                        double* out_v, double* out_n, double* out_m, double* out_g);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,7 +34,9 @@ def oracle_lib() -> C.CDLL:
         if not os.path.exists(ORACLE_LIB):
             raise RuntimeError(f"{ORACLE_LIB} missing: run `make -C oracle`")
         _olib = C.CDLL(ORACLE_LIB)
-        for name in ("hco_render_forward_f64", "hco_render_forward_f32"):
+        for name in ("hco_render_forward_f64", "hco_render_forward_f32", "hco_render_backward_f64",
+                     "hco_render_backward_f32", "hco_eg_forward_f64", "hco_eg_forward_f32", "hco_eg_backward_f64",
+                     "hco_eg_backward_f32", "hco_eg_forward_f64d"):
             getattr(_olib, name).restype = C.c_int
     return _olib
 
@@ -58,7 +60,7 @@ def ref_lib() -> C.CDLL:
             [C.c_void_p] * 3 + [C.c_void_p] * 7 + [C.c_int]
         _rlib.hcref_render_backward.restype = C.c_int
         _rlib.hcref_render_backward.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 4 + [C.c_int, C.c_int] + \
-            [C.c_void_p] * 12
+            [C.c_void_p] * 11
     return _rlib
 
 
@@ -105,6 +107,35 @@ def render_forward(faces, texcoords, B, C_, W, H, albedo, shading, verts, colors
             C.c_int(nthreads))
     if st != 0:
         raise RuntimeError("oracle render failed")
+    return out
+
+
+def render_backward(faces, texcoords, B, C_, W, H, albedo, shading, grad, verts, colors, texture, sh, target,
+                    vnormal, bary, face, extr, intr, ifs=2, tfs=2, precision="f64", nthreads=0):
+    """CPU oracle adjoint.  Returns dict of numpy gradient arrays."""
+    faces = _c(faces, np.int32).reshape(-1)
+    F = faces.size // 3
+    verts = _c(verts, np.float32)
+    N = verts.reshape(B, -1, 3).shape[1]
+    texture = _c(texture, np.float32)
+    TH, TW = (texture.shape[1], texture.shape[2]) if texture is not None and texture.ndim == 4 else (0, 0)
+    tc = _c(texcoords, np.float32) if texcoords is not None else np.zeros(6 * F, np.float32)
+    arrs = [_c(a, np.float32) for a in (grad, colors, sh, target, vnormal, bary, extr, intr)]
+    grad, colors, sh, target, vnormal, bary, extr, intr = arrs
+    face = _c(face, np.int32)
+    out = {"vertex_pos_grad": np.zeros((B, N, 3), np.float32), "vertex_color_grad": np.zeros((B, N, 3), np.float32),
+           "texture_grad": np.zeros((B, max(TH, 1), max(TW, 1), 3), np.float32),
+           "sh_coeff_grad": np.zeros((B, C_, 27), np.float32)}
+    fn = getattr(oracle_lib(), f"hco_render_backward_{precision}")
+    vp_ = C.c_void_p
+    st = fn(C.c_int(N), C.c_int(F), vp_(_p(faces)), vp_(_p(tc)), C.c_int(B), C.c_int(C_), C.c_int(W), C.c_int(H),
+            C.c_int(ALBEDO[albedo]), C.c_int(SHADING[shading]), C.c_int(ifs), C.c_int(tfs), vp_(_p(grad)),
+            vp_(_p(verts)), vp_(_p(colors)), vp_(_p(texture)), C.c_int(TH), C.c_int(TW), vp_(_p(sh)),
+            vp_(_p(target)), vp_(_p(vnormal)), vp_(_p(bary)), vp_(_p(face)), vp_(_p(extr)), vp_(_p(intr)),
+            vp_(_p(out["vertex_pos_grad"])), vp_(_p(out["vertex_color_grad"])),
+            vp_(_p(out["texture_grad"]) if TH > 0 else None), vp_(_p(out["sh_coeff_grad"])), C.c_int(nthreads))
+    if st != 0:
+        raise RuntimeError("oracle render backward failed")
     return out
 
 
@@ -167,4 +198,125 @@ class RefRenderer:
                                              _p(o["texture_grad"]), _p(o["sh_coeff_grad"]))
         if st != 0:
             raise RuntimeError(f"reference backward failed: cuda error {st}")
+        return o
+
+
+# ---------------------------------------------------------------------------
+# embedded graph
+# ---------------------------------------------------------------------------
+def _eg_arrays(d):
+    i32 = lambda a: _c(a, np.int32)  # noqa: E731
+    f32 = lambda a: _c(a, np.float32)  # noqa: E731
+    return dict(base=f32(d.base_vertices), faces=i32(d.faces), nv=i32(d.node_vertex), v2n_off=i32(d.v2n_offsets),
+                v2n_size=i32(d.v2n_sizes), v2n_idx=i32(d.v2n_indices), v2n_w=f32(d.v2n_weights),
+                n2v_off=i32(d.n2v_offsets), n2v_size=i32(d.n2v_sizes), n2v_idx=i32(d.n2v_indices),
+                n2v_w=f32(d.n2v_weights),
+                markers=f32(d.markers) if d.markers is not None else np.zeros((1, 3), np.float32),
+                m2n=i32(d.marker_node) if d.marker_node is not None else np.zeros(1, np.int32),
+                Mk=0 if d.markers is None else len(d.markers))
+
+
+def eg_forward(d, dT, dA, sT, sA, disp, precision="f64"):
+    """CPU oracle EG forward; d is an EGData.  numpy in / out."""
+    a = _eg_arrays(d)
+    B = dT.shape[0]
+    N, M, F, Mk = a["base"].shape[0], a["nv"].shape[0], a["faces"].size // 3, a["Mk"]
+    ins = [_c(x, np.float32) for x in (dT, dA, sT, sA, disp)]
+    odt = np.float64 if precision == "f64d" else np.float32
+    out = {"vertices": np.zeros((B, N, 3), odt), "normals": np.zeros((B, N, 3), odt),
+           "markers": np.zeros((B, max(Mk, 1), 3), odt), "graph": np.zeros((B, M, 3), odt)}
+    fn = getattr(oracle_lib(), f"hco_eg_forward_{precision}")
+    vp_ = C.c_void_p
+    st = fn(B, N, M, Mk, F, vp_(_p(a["base"])), vp_(_p(a["faces"])), vp_(_p(a["nv"])), vp_(_p(a["v2n_off"])),
+            vp_(_p(a["v2n_size"])), vp_(_p(a["v2n_idx"])), vp_(_p(a["v2n_w"])), vp_(_p(a["markers"])),
+            vp_(_p(a["m2n"])), *(vp_(_p(x)) for x in ins), vp_(_p(out["vertices"])), vp_(_p(out["normals"])),
+            vp_(_p(out["markers"])), vp_(_p(out["graph"])))
+    if st != 0:
+        raise RuntimeError("oracle eg forward failed")
+    return out
+
+
+def eg_backward(d, gv, gm, dT, dA, sA, disp, full=False, precision="f64"):
+    a = _eg_arrays(d)
+    B = gv.shape[0]
+    N, M, Mk = a["base"].shape[0], a["nv"].shape[0], a["Mk"]
+    n2m = np.full(M, -1, np.int32)
+    if Mk:
+        n2m[a["m2n"]] = np.arange(Mk, dtype=np.int32)
+    gv, dT, dA, sA, disp = (_c(x, np.float32) for x in (gv, dT, dA, sA, disp))
+    gm = _c(gm, np.float32) if (gm is not None and Mk) else None
+    out = {k: np.zeros((B, M, 3), np.float32) for k in ("t", "r", "st", "sr")}
+    out["disp"] = np.zeros((B, N, 3), np.float32)
+    fn = getattr(oracle_lib(), f"hco_eg_backward_{precision}")
+    vp_ = C.c_void_p
+    st = fn(B, N, M, Mk, vp_(_p(a["base"])), vp_(_p(a["nv"])), vp_(_p(a["v2n_off"])), vp_(_p(a["v2n_size"])),
+            vp_(_p(a["v2n_idx"])), vp_(_p(a["v2n_w"])), vp_(_p(a["n2v_off"])), vp_(_p(a["n2v_size"])),
+            vp_(_p(a["n2v_idx"])), vp_(_p(a["n2v_w"])), vp_(_p(n2m)), vp_(_p(a["markers"])), vp_(_p(gv)),
+            vp_(_p(gm)), vp_(_p(dT)), vp_(_p(dA)), vp_(_p(sA)), vp_(_p(disp)), int(full), vp_(_p(out["t"])),
+            vp_(_p(out["r"])), vp_(_p(out["st"])), vp_(_p(out["sr"])), vp_(_p(out["disp"])))
+    if st != 0:
+        raise RuntimeError("oracle eg backward failed")
+    return out
+
+
+class RefEG:
+    """The reference embedded-graph kernels (GPU), on torch CUDA tensors."""
+
+    def __init__(self, d, device):
+        import torch
+        a = _eg_arrays(d)
+        self.N, self.M, self.F, self.Mk = a["base"].shape[0], a["nv"].shape[0], a["faces"].size // 3, a["Mk"]
+        # vertex -> face lists in the reference's order
+        faces = a["faces"].reshape(-1, 3)
+        lists = [[] for _ in range(self.N)]
+        for f, (x, y, z) in enumerate(faces):
+            for v in dict.fromkeys((int(x), int(y), int(z))):
+                lists[v].append(f)
+        vf = np.array([f for L in lists for f in L], np.int32)
+        starts = np.cumsum([0] + [len(L) for L in lists[:-1]]).astype(np.int32)
+        vfid = np.stack([starts, np.array([len(L) for L in lists], np.int32)], 1)
+        n2m = np.full(self.M, -1, np.int32)
+        if self.Mk:
+            n2m[a["m2n"]] = np.arange(self.Mk, dtype=np.int32)
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(device)  # noqa: E731
+        self.d = {k: t(v) for k, v in a.items() if k != "Mk"}
+        self.d["vf"], self.d["vfid"], self.d["n2m"] = t(vf), t(vfid), t(n2m)
+        L = ref_lib()
+        L.hcref_eg_forward.restype = C.c_int
+        L.hcref_eg_forward.argtypes = [C.c_int] * 5 + [C.c_void_p] * 22
+        L.hcref_eg_backward.restype = C.c_int
+        L.hcref_eg_backward.argtypes = [C.c_int] * 4 + [C.c_void_p] * 21
+
+    def forward(self, dT, dA, sT, sA, disp):
+        import torch
+        B, dev = dT.shape[0], dT.device
+        o = {"vertices": torch.zeros((B, self.N, 3), device=dev), "normals": torch.zeros((B, self.N, 3), device=dev),
+             "markers": torch.zeros((B, max(self.Mk, 1), 3), device=dev),
+             "graph": torch.zeros((B, self.M, 3), device=dev), "da": torch.zeros((B, self.M, 3), device=dev),
+             "sa": torch.zeros((B, self.M, 3), device=dev)}
+        d = self.d
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_eg_forward(B, self.N, self.M, self.Mk, self.F, _p(d["base"]), _p(d["faces"]), _p(d["vf"]),
+                                        _p(d["vfid"]), _p(d["nv"]), _p(d["v2n_off"]), _p(d["v2n_size"]),
+                                        _p(d["v2n_idx"]), _p(d["v2n_w"]), _p(d["m2n"]), _p(d["markers"]), _p(dT),
+                                        _p(dA), _p(sT), _p(sA), _p(disp), _p(o["vertices"]), _p(o["normals"]),
+                                        _p(o["markers"]), _p(o["graph"]), _p(o["da"]), _p(o["sa"]))
+        if st != 0:
+            raise RuntimeError(f"reference eg forward failed: {st}")
+        return o
+
+    def backward(self, gv, gm, dA, sA):
+        import torch
+        B, dev = gv.shape[0], gv.device
+        o = {k: torch.zeros((B, self.M, 3), device=dev) for k in ("t", "r", "st", "sr")}
+        o["disp"] = torch.zeros((B, self.N, 3), device=dev)
+        d = self.d
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_eg_backward(B, self.N, self.M, self.Mk, _p(d["base"]), _p(d["nv"]), _p(d["v2n_off"]),
+                                         _p(d["v2n_size"]), _p(d["v2n_idx"]), _p(d["v2n_w"]), _p(d["n2v_off"]),
+                                         _p(d["n2v_size"]), _p(d["n2v_idx"]), _p(d["n2v_w"]), _p(d["n2m"]),
+                                         _p(d["markers"]), _p(gv), _p(gm), _p(dA), _p(sA), _p(o["t"]), _p(o["r"]),
+                                         _p(o["st"]), _p(o["sr"]), _p(o["disp"]))
+        if st != 0:
+            raise RuntimeError(f"reference eg backward failed: {st}")
         return o
