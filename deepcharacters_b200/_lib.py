@@ -45,6 +45,14 @@ _SIGS: dict[str, list] = {
     "hc_dq_skinning_backward": [vp, vp, C.c_int32] + [vp] * 8,
     "hc_lb_skinning_forward": [vp, vp, C.c_int32] + [vp] * 9,
     "hc_lb_skinning_backward": [vp, vp, C.c_int32] + [vp] * 10,
+    "hc_camera_projection_forward": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_int32, vp],
+    "hc_camera_projection_backward": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_int32, vp],
+    "hc_projected_mesh_boundary": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp],
+    "hc_silhouette_create": [C.POINTER(vp)],
+    "hc_silhouette_destroy": [vp],
+    "hc_silhouette_reserve": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
+    "hc_silhouette_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 9,
+    "hc_silhouette_backward": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 6,
     "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
     "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
                              vp, vp, vp, vp],

@@ -39,16 +39,8 @@ struct TriView {     // 16 bytes
     int dqmin;       // lower bound of the quantised depth; bit 31 set = back-facing
 };
 
-// Conservative lower bound of int(t * 1e4) over the triangle: the ray
-// parameter t = num / (dir . n) is at least the plane distance |num| / |n|
-// for a unit direction; the bound is lowered by 1e-4 relative and 2 quanta
-// so float rounding of either side cannot break it.
-__device__ __forceinline__ int depth_lower_bound(float num, float3 n) {
-    const float pd = fabsf(num) / sqrtf(dot(n, n));
-    const float z = pd * 10000.f * (1.f - 1e-4f);
-    if (!(z < 2.0e9f)) return 0x7fffffff;
-    return max((int)z - 2, 0);
-}
+struct TriS;
+
 
 struct RasterStats {
     unsigned long long binned;
@@ -83,6 +75,23 @@ __device__ __forceinline__ TriS tri_from(const TriFrame& f) {
     t.s2 = make_float3(f.c.x, f.c.y, f.c.z);
     t.n = make_float3(f.a.w, f.b.w, f.c.w);
     return t;
+}
+
+// Conservative lower bound of int(t * 1e4) over the triangle.  For a unit
+// ray direction t is the distance from the camera centre to the hit point,
+// which is at least (a) the distance to the triangle's plane, |num| / |n|,
+// and (b) the distance to the nearest vertex minus the longest edge (every
+// point of a triangle lies within its longest edge of some vertex).  The
+// larger of the two is lowered by 1e-4 relative and 2 quanta so float
+// rounding of either side cannot break it.
+__device__ __forceinline__ int depth_lower_bound(float num, float3 n, const TriS& T, float3 o) {
+    const float pd = fabsf(num) / sqrtf(dot(n, n));
+    const float d0 = length3(T.s0 - o), d1 = length3(T.s1 - o), d2 = length3(T.s2 - o);
+    const float e = fmaxf(length3(T.s1 - T.s0), fmaxf(length3(T.s2 - T.s1), length3(T.s0 - T.s2)));
+    const float vd = fminf(d0, fminf(d1, d2)) - e;
+    const float z = fmaxf(pd, vd) * 10000.f * (1.f - 1e-4f);
+    if (!(z < 2.0e9f)) return 0x7fffffff;
+    return max((int)z - 2, 0);
 }
 
 // Ray / triangle test of the reference (rayTriangleIntersect,

@@ -172,7 +172,7 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         tv.x01 = (cx0 & 0xffff) | (cx1 << 16);
         tv.y01 = (cy0 & 0xffff) | (cy1 << 16);
         // front-facing: the plane normal points towards the camera (num < 0)
-        tv.dqmin = depth_lower_bound(tv.num, T.n) | (tv.num < 0.f ? 0 : (int)0x80000000);
+        tv.dqmin = depth_lower_bound(tv.num, T.n, T, ro_s) | (tv.num < 0.f ? 0 : (int)0x80000000);
         tri_view[i] = tv;
     }
     const bool nonempty = live && x1 >= x0 && y1 >= y0;
@@ -393,11 +393,9 @@ __device__ __forceinline__ float3 shade_pixel(const ShadeArgs& A, const ViewCam&
 }
 
 struct TileTri {
+    int4 hdr;        // x01, y01, dqmin (depth lower bound | back-facing bit 31), face id
     float4 a, b, c;  // TriFrame
-    float num;
-    int x01, y01, f;
-    int dqmin;       // depth lower bound | back-facing flag (bit 31)
-    int pad[3];
+    float4 nm;       // ray-plane numerator
 };
 
 template <int TS>
@@ -443,14 +441,11 @@ __global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, in
                     const TriFrame tf = tri_frame[(long long)b * A.F + f];
                     const TriView tv = tri_view[(long long)view * A.F + f];
                     TileTri t;
+                    t.hdr = make_int4(tv.x01, tv.y01, tv.dqmin, f);
                     t.a = tf.a;
                     t.b = tf.b;
                     t.c = tf.c;
-                    t.num = tv.num;
-                    t.x01 = tv.x01;
-                    t.y01 = tv.y01;
-                    t.f = f;
-                    t.dqmin = tv.dqmin;
+                    t.nm = make_float4(tv.num, 0.f, 0.f, 0.f);
                     s_tri[threadIdx.x] = t;
                 }
                 __syncthreads();
@@ -458,20 +453,19 @@ __global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, in
             const int m = min(CHUNK, n - base);
             if (valid) {
                 for (int j = 0; j < m; ++j) {
-                    const int dm = s_tri[j].dqmin;
-                    if ((dm < 0) != (pass == 1)) continue;          // wrong facing for this pass
-                    if ((unsigned)(dm & 0x7fffffff) > best_d) continue;  // cannot reach the best depth
-                    const int x01 = s_tri[j].x01, y01 = s_tri[j].y01;
-                    if (px < (x01 & 0xffff) || px > (x01 >> 16) || py < (y01 & 0xffff) || py > (y01 >> 16))
-                        continue;
+                    // one 16-byte header load decides whether the ray test runs
+                    const int4 h = s_tri[j].hdr;
+                    if ((h.z < 0) != (pass == 1)) continue;             // wrong facing for this pass
+                    if ((unsigned)(h.z & 0x7fffffff) > best_d) continue;  // cannot reach the best depth
+                    if (px < (h.x & 0xffff) || px > (h.x >> 16) || py < (h.y & 0xffff) || py > (h.y >> 16)) continue;
                     TriFrame tf;
                     tf.a = s_tri[j].a;
                     tf.b = s_tri[j].b;
                     tf.c = s_tri[j].c;
                     int dq;
                     float a, bb;
-                    if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].num, dq, a, bb)) continue;
-                    const int f = s_tri[j].f;
+                    if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].nm.x, dq, a, bb)) continue;
+                    const int f = h.w;
                     if ((unsigned)dq < best_d) {
                         best_d = (unsigned)dq;
                         best_f = f;

@@ -1,0 +1,489 @@
+// Camera projection, projected-mesh boundary and the multi-view silhouette
+// distance-transform loss (CameraProjectionGpu, MultiViewSilhouetteLossGpu and
+// their gradient ops).
+//
+// References: CustomTensorFlowCPPOperators/src/CustomGPUOperators/
+//   CameraProjectionOperator/CameraProjectionGPUOp{,Grad}.cu,
+//   MultiViewSilhouetteLossOperator/MultiViewSilhouetteLossGPUOp{,Grad}.cu,
+//   Skeletool/Mesh/CUDABasedRasterization.cu:168-200 (boundary test).
+//
+// The reference's data -> model term scans every vertex for every boundary
+// pixel of the distance image (MultiViewSilhouetteLossGPUOp.cu:195-212).
+// Here the boundary vertices of each view are binned into a grid whose cell
+// edge is the search radius (30 * crop scale px), so a pixel only scans the
+// 3x3 cells around it; the candidate with the smallest distance and, among
+// equal distances, the smallest vertex id is the reference's first-strictly-
+// smaller winner.
+#include "hc_common.cuh"
+#include "hc_math.cuh"
+
+namespace hc {
+namespace {
+
+__device__ __forceinline__ float3 cam_point(const float* e, float3 p) {
+    const float4 h = make_float4(p.x, p.y, p.z, 1.f);
+    return make_float3(dot(make_float4(e[0], e[1], e[2], e[3]), h), dot(make_float4(e[4], e[5], e[6], e[7]), h),
+                       dot(make_float4(e[8], e[9], e[10], e[11]), h));
+}
+
+__device__ __forceinline__ float3 cam_vector(const float* e, float3 p) {
+    const float4 h = make_float4(p.x, p.y, p.z, 0.f);
+    return make_float3(dot(make_float4(e[0], e[1], e[2], e[3]), h), dot(make_float4(e[4], e[5], e[6], e[7]), h),
+                       dot(make_float4(e[8], e[9], e[10], e[11]), h));
+}
+
+// projectPointFloat (CameraUtil.h:108-137 of the custom-op utilities)
+__device__ __forceinline__ float2 project2(const float* k, float3 p) {
+    const float3 d1 = p * make_float3(k[0], k[1], k[2]);
+    const float3 d2 = p * make_float3(k[3], k[4], k[5]);
+    const float3 d3 = p * make_float3(k[6], k[7], k[8]);
+    float x = d1.x + d1.y + d1.z;
+    float y = d2.x + d2.y + d2.z;
+    float z = d3.x + d3.y + d3.z;
+    if (z > 0.0000001f) {
+        x /= z;
+        y /= z;
+    } else {
+        z = 0.00001f;
+        x /= z;
+        y /= z;
+    }
+    return make_float2(x, y);
+}
+
+__global__ void k_project(int B, int C, int N, const float* __restrict__ pts, const float* __restrict__ vecs,
+                          const float* __restrict__ extr, const float* __restrict__ intr, int is_point,
+                          float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N) return;
+    const int p = (int)(i % N);
+    const int c = (int)((i / N) % C);
+    const int b = (int)(i / ((long long)N * C));
+    const float* e = extr + ((long long)b * C + c) * 12;
+    const float* k = intr + ((long long)b * C + c) * 9;
+    const float3 P = ld3(pts + ((long long)b * N + p) * 3);
+    float2 r;
+    if (is_point) {
+        r = project2(k, cam_point(e, P));
+    } else {
+        const float3 cp = cam_point(e, P);
+        const float3 np = cp + cam_vector(e, ld3(vecs + ((long long)b * N + p) * 3));
+        const float2 a = project2(k, cp), bb = project2(k, np);
+        float2 dvec = make_float2(bb.x - a.x, bb.y - a.y);
+        const float inv = rsqrtf(dvec.x * dvec.x + dvec.y * dvec.y);
+        r = make_float2(dvec.x * inv, dvec.y * inv);
+    }
+    out[2 * i] = r.x;
+    out[2 * i + 1] = r.y;
+}
+
+// d(image point)/d(world point), summed over the cameras
+// (CameraProjectionGPUOpGrad.cu:12-79; the normals get a zero gradient, :83-98)
+__global__ void k_project_grad(int B, int C, int N, const float* __restrict__ gimg, const float* __restrict__ pts,
+                               const float* __restrict__ extr, const float* __restrict__ intr, int is_point,
+                               float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * N) return;
+    const int p = (int)(i % N), b = (int)(i / N);
+    float3 g = make_float3(0.f, 0.f, 0.f);
+    if (is_point) {
+        const float3 P = ld3(pts + i * 3);
+        for (int c = 0; c < C; ++c) {
+            const float* e = extr + ((long long)b * C + c) * 12;
+            const float* k = intr + ((long long)b * C + c) * 9;
+            const float3 cs = cam_point(e, P);
+            const float ax = k[0], ay = k[4], gm = k[1];
+            const float a00 = ax / cs.z, a01 = gm / cs.z, a02 = (-ax * cs.x - gm * cs.y) / (cs.z * cs.z);
+            const float a11 = ay / cs.z, a12 = (-ay * cs.y) / (cs.z * cs.z);
+            const float2 gi = make_float2(gimg[(((long long)b * C + c) * N + p) * 2],
+                                          gimg[(((long long)b * C + c) * N + p) * 2 + 1]);
+            // rows of dI/dv * dE/dv
+            const float3 r0 = make_float3(a00 * e[0] + a01 * e[4] + a02 * e[8], a00 * e[1] + a01 * e[5] + a02 * e[9],
+                                          a00 * e[2] + a01 * e[6] + a02 * e[10]);
+            const float3 r1 = make_float3(a11 * e[4] + a12 * e[8], a11 * e[5] + a12 * e[9], a11 * e[6] + a12 * e[10]);
+            g += r0 * gi.x + r1 * gi.y;
+        }
+    }
+    st3(out + i * 3, g);
+}
+
+// Boundary vertices of the projected mesh: a vertex is on the boundary of a
+// view if a pixel of the 3x3 window around its (truncated) projection is not
+// covered (Skeletool/Mesh/CUDABasedRasterization.cu:168-200).  Coverage is the
+// renderer's face buffer.
+__global__ void k_boundary(int B, int C, int N, int W, int H, const float* __restrict__ p2d,
+                           const int* __restrict__ face, unsigned char* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N) return;
+    const long long view = i / N;
+    const int u = (int)p2d[2 * i], v = (int)p2d[2 * i + 1];
+    unsigned char r = 0;
+    if (u - 1 >= 0 && u + 1 < W && v - 1 >= 0 && v + 1 < H) {
+        const int* F = face + view * H * W;
+        for (int c = u - 1; c <= u + 1; ++c)
+            for (int rr = v - 1; rr <= v + 1; ++rr)
+                if (F[(long long)rr * W + c] < 0) r = 1;
+    }
+    out[i] = r;
+}
+
+__device__ __forceinline__ float dt_decode(unsigned char x) {
+    float v = (int)x;
+    if (v >= 127) v = (v - 127) * 2;
+    return v;
+}
+
+// model -> data term per (frame, view, vertex) (MultiViewSilhouetteLossGPUOp.cu:11-138)
+__global__ void k_sil_points(int B, int C, int N, int U, int V, const float* __restrict__ p2d,
+                             const float* __restrict__ n2d, const unsigned char* __restrict__ isb,
+                             const unsigned char* __restrict__ dt, const float* __restrict__ crops,
+                             float* __restrict__ residual, float* __restrict__ dtgrad) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N) return;
+    const long long view = i / N;
+    const float* cr = crops + view * 7;
+    const float2 border = make_float2(cr[0], cr[1]);
+    const float scale = cr[2];
+    const float2 cmin = make_float2(cr[3], cr[4]), cmax = make_float2(cr[5], cr[6]);
+    const float pu = p2d[2 * i], pv = p2d[2 * i + 1];
+    const bool in_view = pu - 2 > cmin.x && pu + 2 < cmax.x && pv - 2 > cmin.y && pv + 2 < cmax.y;
+    if (!in_view) {
+        dtgrad[2 * i] = 0.f;
+        dtgrad[2 * i + 1] = 0.f;
+        residual[i] = 0.f;
+        return;
+    }
+    const float fx = (pu - cmin.x) / scale + border.x, fy = (pv - cmin.y) / scale + border.y;
+    const int x = (int)fx, y = (int)fy;
+    const unsigned char* D = dt + view * (long long)U * V;
+    float val = dt_decode(D[(long long)y * U + x]);
+    const float f00 = dt_decode(D[(long long)(y - 1) * U + (x - 1)]), f01 = dt_decode(D[(long long)(y - 1) * U + x]);
+    const float f02 = dt_decode(D[(long long)(y - 1) * U + (x + 1)]), f10 = dt_decode(D[(long long)y * U + (x - 1)]);
+    const float f12 = dt_decode(D[(long long)y * U + (x + 1)]), f20 = dt_decode(D[(long long)(y + 1) * U + (x - 1)]);
+    const float f21 = dt_decode(D[(long long)(y + 1) * U + x]), f22 = dt_decode(D[(long long)(y + 1) * U + (x + 1)]);
+    const float du = (1.f / 8.f) * ((-1.f) * f00 + (+1.f) * f02 + (-2.f) * f10 + (+2.f) * f12 + (-1.f) * f20 + (+1.f) * f22);
+    const float dv = (1.f / 8.f) * ((-1.f) * f00 + (-2.f) * f01 + (-1.f) * f02 + (+1.f) * f20 + (+2.f) * f21 + (+1.f) * f22);
+    float2 dn = make_float2(du, dv), dnu = make_float2(du, dv);
+    const bool inside = (int)D[(long long)y * U + x] <= 127;
+    const float nonvanishing = (float)(int)(dn.x != 0 || dn.y != 0);
+    const float boundary = (float)(int)(isb[i] != 0);
+    if (inside) dn = make_float2(-dn.x, -dn.y);
+    const float dn_dot = dn.x * n2d[2 * i] + dn.y * n2d[2 * i + 1];
+    if (!(dn_dot >= 0.f) && inside) dnu = make_float2(-dnu.x, -dnu.y);
+    val *= boundary;
+    val *= nonvanishing;
+    dnu = make_float2(dnu.x * boundary * nonvanishing, dnu.y * boundary * nonvanishing);
+    dtgrad[2 * i] = dnu.x * (1.f / (255.f));
+    dtgrad[2 * i + 1] = dnu.y * (1.f / (255.f));
+    residual[i] = val * (1.f / (255.f));
+}
+
+// grid of boundary vertices per view: cell edge = search radius 30 * scale
+struct SilGrid {
+    int gx, gy;       // cells per view
+    int* count;       // [views * cells]
+    int* start;       // [views * cells + 1] per view prefix
+    int* cursor;      // [views * cells]
+    int* items;       // [views * N]
+};
+
+__device__ __forceinline__ bool grid_cell(const float* cr, int U, int V, int gx, int gy, float px, float py, int& cx,
+                                          int& cy) {
+    // image-space box of the distance image, extended by one radius
+    const float scale = cr[2], R = 30.f * scale;
+    const float x0 = (0.f - cr[0]) * scale + cr[3] - R, y0 = (0.f - cr[1]) * scale + cr[4] - R;
+    const float fx = floorf((px - x0) / R), fy = floorf((py - y0) / R);
+    if (!(fx >= 0.f && fy >= 0.f && fx < (float)gx && fy < (float)gy)) return false;
+    cx = (int)fx;
+    cy = (int)fy;
+    return true;
+}
+
+__global__ void k_grid_count(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
+                             const unsigned char* __restrict__ isb, const float* __restrict__ crops) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N || !isb[i]) return;
+    const long long view = i / N;
+    int cx, cy;
+    if (!grid_cell(crops + view * 7, U, V, g.gx, g.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
+    atomicAdd(&g.count[view * g.gx * g.gy + cy * g.gx + cx], 1);
+}
+
+// exclusive scan of the cell counts, one CTA per view
+__global__ void k_grid_scan(SilGrid g) {
+    const int view = blockIdx.x;
+    const int cells = g.gx * g.gy;
+    __shared__ int s_part[1024];
+    const int* cnt = g.count + (long long)view * cells;
+    int* st = g.start + (long long)view * cells;
+    // each thread scans a contiguous chunk
+    const int per = (cells + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * per, hi = min(cells, lo + per);
+    int sum = 0;
+    for (int c = lo; c < hi; ++c) sum += cnt[c];
+    s_part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+        const int v = threadIdx.x >= (unsigned)off ? s_part[threadIdx.x - off] : 0;
+        __syncthreads();
+        s_part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    int run = s_part[threadIdx.x] - sum;
+    for (int c = lo; c < hi; ++c) {
+        st[c] = run;
+        g.cursor[(long long)view * cells + c] = run;
+        run += cnt[c];
+    }
+}
+
+__global__ void k_grid_fill(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
+                            const unsigned char* __restrict__ isb, const float* __restrict__ crops) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N || !isb[i]) return;
+    const long long view = i / N;
+    int cx, cy;
+    if (!grid_cell(crops + view * 7, U, V, g.gx, g.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
+    const int slot = atomicAdd(&g.cursor[view * g.gx * g.gy + cy * g.gx + cx], 1);
+    g.items[view * (long long)N + slot] = (int)(i % N);
+}
+
+// data -> model term per distance-image pixel (MultiViewSilhouetteLossGPUOp.cu:142-240)
+__global__ void k_sil_pixels(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
+                             const unsigned char* __restrict__ dt, const float* __restrict__ crops,
+                             float* __restrict__ residual1, float* __restrict__ closest) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * U * V) return;
+    const long long view = i / ((long long)U * V);
+    const int vid = (int)((i / U) % V), uid = (int)(i % U);
+    const unsigned char* D = dt + view * (long long)U * V;
+    int best = -1;
+    float2 imgpos = make_float2(0.f, 0.f);
+    float scale = 1.f;
+    if ((int)D[(long long)vid * U + uid] == 127) {
+        int nb = 0;
+        for (int j = -2; j <= 2; ++j)
+            for (int k = -2; k <= 2; ++k) {
+                const int yy = vid + j, xx = uid + k;
+                if (yy >= 0 && yy < V && xx >= 0 && xx < U && (int)D[(long long)yy * U + xx] == 127) ++nb;
+            }
+        if (nb >= 4) {
+            const float* cr = crops + view * 7;
+            scale = cr[2];
+            imgpos = make_float2(((float)uid - cr[0]) * scale + cr[3], ((float)vid - cr[1]) * scale + cr[4]);
+            float bestd = 30.f * scale;
+            int cx, cy;
+            const int cells = g.gx * g.gy;
+            if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
+                for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.gy - 1); ++yy)
+                    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, g.gx - 1); ++xx) {
+                        const int cell = yy * g.gx + xx;
+                        const int s0 = g.start[view * cells + cell];
+                        const int n = g.count[view * cells + cell];
+                        for (int q = 0; q < n; ++q) {
+                            const int v = g.items[view * (long long)N + s0 + q];
+                            const float* pp = p2d + (view * (long long)N + v) * 2;
+                            const float2 dlt = make_float2(pp[0] - imgpos.x, pp[1] - imgpos.y);
+                            const float dist = sqrtf(dlt.x * dlt.x + dlt.y * dlt.y);
+                            if (dist < bestd || (dist == bestd && best >= 0 && v < best)) {
+                                bestd = dist;
+                                best = v;
+                            }
+                        }
+                    }
+            }
+        }
+    }
+    if (best >= 0) {
+        const float* pp = p2d + (view * (long long)N + best) * 2;
+        residual1[2 * i] = (pp[0] - imgpos.x) / (30.f * scale);
+        residual1[2 * i + 1] = (pp[1] - imgpos.y) / (30.f * scale);
+        closest[i] = (float)best;
+    } else {
+        residual1[2 * i] = 0.f;
+        residual1[2 * i + 1] = 0.f;
+        closest[i] = -1.f;
+    }
+}
+
+__global__ void k_sil_grad_points(long long n, const float* __restrict__ dtgrad, const float* __restrict__ g,
+                                  float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[2 * i] = dtgrad[2 * i] * g[i];
+    out[2 * i + 1] = dtgrad[2 * i + 1] * g[i];
+}
+
+__global__ void k_sil_grad_pixels(int B, int C, int N, int U, int V, const float* __restrict__ g1,
+                                  const float* __restrict__ closest, const float* __restrict__ crops,
+                                  float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * U * V) return;
+    const int cv = (int)closest[i];
+    if (cv < 0) return;
+    const long long view = i / ((long long)U * V);
+    const float scale = crops[view * 7 + 2];
+    float* o = out + (view * N + cv) * 2;
+    atomicAdd(o, g1[2 * i] / (30.f * scale));
+    atomicAdd(o + 1, g1[2 * i + 1] / (30.f * scale));
+}
+
+}  // namespace
+}  // namespace hc
+
+using namespace hc;
+
+extern "C" hc_status hc_camera_projection_forward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                  const float* points_global_space, const float* vectors_global_space,
+                                                  const float* extrinsics, const float* intrinsics,
+                                                  int32_t is_point, float* points_image_space) {
+    clear_error();
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points >= 0, "bad sizes");
+    HC_REQUIRE(points_global_space && extrinsics && intrinsics && points_image_space, "NULL pointer");
+    HC_REQUIRE(is_point || vectors_global_space, "vector mode needs vectors_global_space");
+    const long long n = (long long)batch * n_cameras * n_points;
+    if (n == 0) return HC_OK;
+    k_project<<<div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(batch, n_cameras, n_points, points_global_space,
+                                                                vectors_global_space, extrinsics, intrinsics,
+                                                                is_point, points_image_space);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_camera_projection_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                   const float* points_image_space_grad,
+                                                   const float* points_global_space, const float* extrinsics,
+                                                   const float* intrinsics, int32_t is_point,
+                                                   float* points_global_space_grad) {
+    clear_error();
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points >= 0, "bad sizes");
+    HC_REQUIRE(points_image_space_grad && points_global_space && extrinsics && intrinsics && points_global_space_grad,
+               "NULL pointer");
+    const long long n = (long long)batch * n_points;
+    if (n == 0) return HC_OK;
+    k_project_grad<<<div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(batch, n_cameras, n_points,
+                                                                     points_image_space_grad, points_global_space,
+                                                                     extrinsics, intrinsics, is_point,
+                                                                     points_global_space_grad);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                int32_t width, int32_t height, const float* points_image_space,
+                                                const int32_t* face_buffer, uint8_t* is_boundary) {
+    clear_error();
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points >= 0 && width > 2 && height > 2, "bad sizes");
+    HC_REQUIRE(points_image_space && face_buffer && is_boundary, "NULL pointer");
+    const long long n = (long long)batch * n_cameras * n_points;
+    if (n == 0) return HC_OK;
+    k_boundary<<<div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(batch, n_cameras, n_points, width, height,
+                                                                 points_image_space, face_buffer, is_boundary);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+struct hc_silhouette_s {
+    DevBuf grid;
+    size_t need = 0;
+};
+
+static size_t grid_bytes(long long views, int gx, int gy, int N) {
+    const long long cells = views * gx * gy;
+    return sizeof(int) * (size_t)(3 * cells + 1 + views * (long long)N);
+}
+
+extern "C" hc_status hc_silhouette_create(hc_silhouette* out) {
+    clear_error();
+    HC_REQUIRE(out, "out is NULL");
+    *out = new hc_silhouette_s();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_silhouette_destroy(hc_silhouette h) {
+    clear_error();
+    if (!h) return HC_OK;
+    h->grid.release();
+    delete h;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_silhouette_reserve(hc_silhouette h, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                           int32_t resolution_u, int32_t resolution_v) {
+    clear_error();
+    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 0 && resolution_v > 0, "bad sizes");
+    const int gx = div_up(resolution_u, 30) + 3, gy = div_up(resolution_v, 30) + 3;
+    HC_TRY(h->grid.ensure(grid_bytes((long long)batch * n_cameras, gx, gy, n_points)));
+    return HC_OK;
+}
+
+extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
+                                           int32_t n_points, int32_t resolution_u, int32_t resolution_v,
+                                           const float* points_image_space, const float* normals_image_space,
+                                           const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                           const float* multi_view_crops, float* mv_dt_residual,
+                                           float* mv_dt_residual_1, float* dt_image_gradient,
+                                           float* closest_vertex_id) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 2 && resolution_v > 2, "bad sizes");
+    HC_REQUIRE(points_image_space && normals_image_space && is_boundary && distance_transform_image &&
+                   multi_view_crops && mv_dt_residual && mv_dt_residual_1 && dt_image_gradient && closest_vertex_id,
+               "NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int U = resolution_u, V = resolution_v, N = n_points;
+    const long long views = (long long)batch * n_cameras;
+    SilGrid g;
+    g.gx = div_up(U, 30) + 3;
+    g.gy = div_up(V, 30) + 3;
+    HC_REQUIRE(g.gx * g.gy <= 1024 * 64, "distance image too large for the boundary grid");
+    HC_TRY(h->grid.ensure(grid_bytes(views, g.gx, g.gy, N)));
+    const long long cells = views * g.gx * g.gy;
+    int* base = h->grid.as<int>();
+    g.count = base;
+    g.start = base + cells;
+    g.cursor = base + 2 * cells + 1;
+    g.items = base + 3 * cells + 1;
+    HC_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)cells, s));
+    const long long np = views * N;
+    k_sil_points<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, points_image_space, normals_image_space,
+                                                 is_boundary, distance_transform_image, multi_view_crops,
+                                                 mv_dt_residual, dt_image_gradient);
+    HC_CHECK_LAUNCH();
+    k_grid_count<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+                                                 multi_view_crops);
+    HC_CHECK_LAUNCH();
+    k_grid_scan<<<(unsigned)views, 1024, 0, s>>>(g);
+    HC_CHECK_LAUNCH();
+    k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+                                                multi_view_crops);
+    HC_CHECK_LAUNCH();
+    const long long npx = views * U * V;
+    k_sil_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space,
+                                                  distance_transform_image, multi_view_crops, mv_dt_residual_1,
+                                                  closest_vertex_id);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                            int32_t resolution_u, int32_t resolution_v, const float* mv_dt_grad,
+                                            const float* mv_dt_grad_1, const float* dt_image_grad,
+                                            const float* closest_vertex_id, const float* multi_view_crops,
+                                            float* points_image_space_grad) {
+    clear_error();
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 0 && resolution_v > 0, "bad sizes");
+    HC_REQUIRE(mv_dt_grad && mv_dt_grad_1 && dt_image_grad && closest_vertex_id && multi_view_crops &&
+                   points_image_space_grad,
+               "NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long np = (long long)batch * n_cameras * n_points;
+    k_sil_grad_points<<<div_up(np, 256), 256, 0, s>>>(np, dt_image_grad, mv_dt_grad, points_image_space_grad);
+    HC_CHECK_LAUNCH();
+    const long long npx = (long long)batch * n_cameras * resolution_u * resolution_v;
+    k_sil_grad_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, n_points, resolution_u, resolution_v,
+                                                       mv_dt_grad_1, closest_vertex_id, multi_view_crops,
+                                                       points_image_space_grad);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}

@@ -425,3 +425,41 @@ def eg_scene(subdiv: int, n_nodes: int, batch: int, seed: int, k: int = 4, n_mar
                 dT=f(delta_t_std, (batch, n_nodes, 3)), dA=f(delta_rot_std, (batch, n_nodes, 3)),
                 sT=f(skinned_t_std, (batch, n_nodes, 3)), sA=f(skinned_rot_std, (batch, n_nodes, 3)),
                 disp=f(disp_std, (batch, verts.shape[0], 3)))
+
+
+def skinning_scene(subdiv: int, n_skel: int, batch: int, seed: int, k: int = 4, pose_amplitude: float = 0.5):
+    """Skinned-character inputs: jittered icosphere, random revolute tree
+    (three joints per skeletal joint), K nearest skinning joints per vertex
+    with Dirichlet weights, per-frame poses U(-a, a) and small displacements."""
+    rng = rng_for(seed)
+    verts, faces = sphere_mesh(subdiv, rng)
+    sk = random_skeleton(n_skel, rng)
+    idx, w = skinning_weights(verts, sk, k, rng)
+    dofs = np.stack([random_pose(sk, rng_for(seed, b), pose_amplitude) for b in range(batch)])
+    return dict(verts=verts, faces=faces, skeleton=sk, skin_index=idx, weights=np.tile(w[None], (batch, 1, 1)),
+                dofs=dofs, disp=rng.normal(0.0, 1.0, size=(batch, verts.shape[0], 3)).astype(np.float32))
+
+
+def silhouette_masks(batch: int, views: int, width: int, height: int, seed: int, scale: float = 1.0) -> np.ndarray:
+    """uint8 distance-transform images [B,C,H,W] of seeded random ellipses
+    (centre +-64 px, semi-axes U[80,200] px at 512 px, scaled by ``scale``)."""
+    out = np.empty((batch, views, height, width), np.uint8)
+    for b in range(batch):
+        for c in range(views):
+            r = rng_for(seed, 100 * b + c)
+            cx = width / 2 + r.uniform(-64, 64) * scale
+            cy = height / 2 + r.uniform(-64, 64) * scale
+            a, bb = r.uniform(80, 200) * scale, r.uniform(80, 200) * scale
+            th = r.uniform(0, np.pi)
+            yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
+            x, y = xx + 0.5 - cx, yy + 0.5 - cy
+            u = (math.cos(th) * x + math.sin(th) * y) / a
+            v = (-math.sin(th) * x + math.cos(th) * y) / bb
+            out[b, c] = encode_dt((u * u + v * v) <= 1.0)
+    return out
+
+
+def identity_crops(batch: int, views: int, width: int, height: int) -> np.ndarray:
+    """Multi-view crops (border u, border v, scale, min u, min v, max u, max v) of uncropped images."""
+    c = np.array([0, 0, 1, 0, 0, width, height], np.float32)
+    return np.tile(c, (batch, views, 1))

@@ -285,6 +285,60 @@ hc_status hc_lb_skinning_backward(hc_skin h, void* stream, int32_t batch,
                                   float* skinning_weights_grad, float* displacement_grad);
 
 /* ------------------------------------------------------------------------ */
+/* Camera projection, projected-mesh boundary, silhouette DT loss            */
+/* ------------------------------------------------------------------------ */
+
+/* CameraProjectionGpu (CameraProjectionGPUOp.cu:12-102): points [B,N,3] (and
+ * vectors [B,N,3] when is_point = 0), extrinsics [B,C*12], intrinsics [B,C*9]
+ * -> points_image_space [B,C,N,2] (image points, or unit image-space
+ * directions of the vectors). */
+hc_status hc_camera_projection_forward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                       const float* points_global_space, const float* vectors_global_space,
+                                       const float* extrinsics, const float* intrinsics, int32_t is_point,
+                                       float* points_image_space);
+/* CameraProjectionGpuGrad (CameraProjectionGPUOpGrad.cu:12-111): [B,C,N,2]
+ * gradient -> points_global_space_grad [B,N,3] (zero in vector mode, as the
+ * reference registers for normals). */
+hc_status hc_camera_projection_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                        const float* points_image_space_grad, const float* points_global_space,
+                                        const float* extrinsics, const float* intrinsics, int32_t is_point,
+                                        float* points_global_space_grad);
+/* ProjectedMeshBoundaryGpu (Skeletool/Mesh/CUDABasedRasterization.cu:168-200):
+ * a vertex is a boundary vertex of a view when a pixel of the 3x3 window
+ * around its truncated projection is uncovered; coverage is a renderer face
+ * buffer [B,C,H,W] (-1 = empty).  is_boundary [B,C,N] uint8. */
+hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                     int32_t width, int32_t height, const float* points_image_space,
+                                     const int32_t* face_buffer, uint8_t* is_boundary);
+
+typedef struct hc_silhouette_s* hc_silhouette;
+hc_status hc_silhouette_create(hc_silhouette* out);
+hc_status hc_silhouette_destroy(hc_silhouette h);
+hc_status hc_silhouette_reserve(hc_silhouette h, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                int32_t resolution_u, int32_t resolution_v);
+/*
+ * MultiViewSilhouetteLossGpu (MultiViewSilhouetteLossGPUOp.cu:11-251):
+ * points / normals_image_space [B,C,N,2], is_boundary [B,C,N] uint8,
+ * distance_transform_image [B,C,U,V] uint8 stored with rows of U values (the
+ * reference's indexing), multi_view_crops [B,C,7] -> mv_dt_residual [B,C,N],
+ * mv_dt_residual_1 [B,C,V,U,2], dt_image_gradient [B,C,N,2],
+ * closest_vertex_id [B,C,V,U] (float, -1 = none).
+ */
+hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                int32_t resolution_u, int32_t resolution_v, const float* points_image_space,
+                                const float* normals_image_space, const uint8_t* is_boundary,
+                                const uint8_t* distance_transform_image, const float* multi_view_crops,
+                                float* mv_dt_residual, float* mv_dt_residual_1, float* dt_image_gradient,
+                                float* closest_vertex_id);
+/* MultiViewSilhouetteLossGpuGrad (MultiViewSilhouetteLossGPUOpGrad.cu:11-72)
+ * -> points_image_space_grad [B,C,N,2] (overwritten). */
+hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                 int32_t resolution_u, int32_t resolution_v, const float* mv_dt_grad,
+                                 const float* mv_dt_grad_1, const float* dt_image_grad,
+                                 const float* closest_vertex_id, const float* multi_view_crops,
+                                 float* points_image_space_grad);
+
+/* ------------------------------------------------------------------------ */
 /* Losses                                                                    */
 /* ------------------------------------------------------------------------ */
 

@@ -320,3 +320,150 @@ class RefEG:
         if st != 0:
             raise RuntimeError(f"reference eg backward failed: {st}")
         return o
+
+
+# ---------------------------------------------------------------------------
+# skinning (reference GPU kernels, fed with given dual quaternions / transforms)
+# ---------------------------------------------------------------------------
+class RefSkin:
+    def __init__(self, ch):
+        L = ref_lib()
+        L.hcref_dq_forward.restype = C.c_int
+        L.hcref_dq_forward.argtypes = [C.c_int] * 6 + [C.c_void_p] * 9
+        L.hcref_dq_backward.restype = C.c_int
+        L.hcref_dq_backward.argtypes = [C.c_int] * 6 + [C.c_void_p] * 16
+        L.hcref_lbs_forward.restype = C.c_int
+        L.hcref_lbs_forward.argtypes = [C.c_int] * 6 + [C.c_void_p] * 10
+        L.hcref_lbs_backward.restype = C.c_int
+        L.hcref_lbs_backward.argtypes = [C.c_int] * 6 + [C.c_void_p] * 17
+        self.ch = ch
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+        f32 = lambda a: np.ascontiguousarray(a, np.float32)  # noqa: E731
+        self.h = dict(parent=i32(ch.parent), type=i32(ch.joint_type), doff=i32(ch.dof_offsets), dj=i32(ch.dof_joint),
+                      sj=i32(ch.skin_joint), si=i32(ch.skin_index), bv=f32(ch.base_vertices),
+                      bn=f32(ch.base_normals))
+        self.N, self.K = ch.skin_index.shape
+        self.S, self.J, self.D = ch.n_skin, ch.n_joints, ch.n_dofs
+
+    def dq_forward(self, dq, weights):
+        import torch
+        B, dev = dq.shape[0], dq.device
+        o = [torch.zeros((B, self.N, 3), device=dev), torch.zeros((B, self.N, 3), device=dev),
+             torch.zeros((B, self.S, 8), device=dev), torch.zeros((B, self.N, self.K), device=dev)]
+        torch.cuda.synchronize()
+        h = self.h
+        st = ref_lib().hcref_dq_forward(B, self.N, self.S, self.K, self.J, self.D, _p(h["si"]), _p(h["bv"]),
+                                        _p(h["bn"]), _p(weights), _p(dq), *(_p(t) for t in o))
+        if st != 0:
+            raise RuntimeError(f"reference dq forward failed: {st}")
+        return o
+
+    def dq_backward(self, gv, vpos, gpos, gaxis, dq, weights, file_weights):
+        import torch
+        B, dev = gv.shape[0], gv.device
+        gd = torch.zeros((B, self.D), device=dev)
+        gw = torch.zeros((B, self.N, self.K), device=dev)
+        fw = np.ascontiguousarray(file_weights, np.float32)
+        h = self.h
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_dq_backward(B, self.N, self.S, self.K, self.J, self.D, _p(h["parent"]), _p(h["type"]),
+                                         _p(h["doff"]), _p(h["dj"]), _p(h["sj"]), _p(h["si"]), _p(fw), _p(h["bv"]),
+                                         _p(gv), _p(vpos), _p(gpos), _p(gaxis), _p(dq), _p(weights), _p(gd), _p(gw))
+        if st != 0:
+            raise RuntimeError(f"reference dq backward failed: {st}")
+        return gd, gw
+
+    def lbs_forward(self, xf12_host, weights, disp):
+        import torch
+        B, dev = weights.shape[0], weights.device
+        o = [torch.zeros((B, self.N, 3), device=dev), torch.zeros((B, self.N, 3), device=dev),
+             torch.zeros((B, self.S, 12), device=dev), torch.zeros((B, self.N, self.K), device=dev)]
+        xf = np.ascontiguousarray(xf12_host, np.float32)
+        h = self.h
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_lbs_forward(B, self.N, self.S, self.K, self.J, self.D, _p(h["si"]), _p(h["bv"]),
+                                         _p(h["bn"]), _p(weights), _p(disp), _p(xf), *(_p(t) for t in o))
+        if st != 0:
+            raise RuntimeError(f"reference lbs forward failed: {st}")
+        return o
+
+    def lbs_backward(self, gv, vpos, gpos, gaxis, xf12_dev, weights, file_weights):
+        import torch
+        B, dev = gv.shape[0], gv.device
+        gd = torch.zeros((B, self.D), device=dev)
+        gw = torch.zeros((B, self.N, self.K), device=dev)
+        gdisp = torch.zeros((B, self.N, 3), device=dev)
+        fw = np.ascontiguousarray(file_weights, np.float32)
+        h = self.h
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_lbs_backward(B, self.N, self.S, self.K, self.J, self.D, _p(h["parent"]), _p(h["type"]),
+                                          _p(h["doff"]), _p(h["dj"]), _p(h["sj"]), _p(h["si"]), _p(fw), _p(h["bv"]),
+                                          _p(gv), _p(vpos), _p(gpos), _p(gaxis), _p(xf12_dev), _p(weights), _p(gd),
+                                          _p(gw), _p(gdisp))
+        if st != 0:
+            raise RuntimeError(f"reference lbs backward failed: {st}")
+        return gd, gw, gdisp
+
+
+# ---------------------------------------------------------------------------
+# camera projection / silhouette (reference GPU kernels)
+# ---------------------------------------------------------------------------
+class RefSilhouette:
+    def __init__(self):
+        L = ref_lib()
+        L.hcref_projection_forward.restype = C.c_int
+        L.hcref_projection_forward.argtypes = [C.c_int] * 3 + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+        L.hcref_projection_backward.restype = C.c_int
+        L.hcref_projection_backward.argtypes = [C.c_int] * 3 + [C.c_void_p] * 4 + [C.c_int, C.c_void_p]
+        L.hcref_silhouette_forward.restype = C.c_int
+        L.hcref_silhouette_forward.argtypes = [C.c_int] * 5 + [C.c_void_p] * 9
+        L.hcref_silhouette_backward.restype = C.c_int
+        L.hcref_silhouette_backward.argtypes = [C.c_int] * 5 + [C.c_void_p] * 6
+
+    def project(self, pts, vecs, extr, intr, is_point):
+        import torch
+        B, N = pts.shape[:2]
+        Cn = extr.reshape(B, -1).shape[1] // 12
+        out = torch.zeros((B, Cn, N, 2), device=pts.device)
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_projection_forward(B, Cn, N, _p(pts), _p(vecs), _p(extr), _p(intr), int(is_point),
+                                                _p(out))
+        if st != 0:
+            raise RuntimeError(f"reference projection failed: {st}")
+        return out
+
+    def project_grad(self, g, pts, extr, intr, is_point):
+        import torch
+        B, Cn, N = g.shape[:3]
+        out = torch.zeros((B, N, 3), device=g.device)
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_projection_backward(B, Cn, N, _p(g), _p(pts), _p(extr), _p(intr), int(is_point), _p(out))
+        if st != 0:
+            raise RuntimeError(f"reference projection grad failed: {st}")
+        return out
+
+    def forward(self, p2d, n2d, isb, dt, crops):
+        import torch
+        B, Cn, N = p2d.shape[:3]
+        U, V = dt.shape[2], dt.shape[3]
+        dev = p2d.device
+        o = [torch.zeros((B, Cn, N), device=dev), torch.zeros((B, Cn, V, U, 2), device=dev),
+             torch.zeros((B, Cn, N, 2), device=dev), torch.zeros((B, Cn, V, U), device=dev)]
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_silhouette_forward(B, Cn, N, U, V, _p(p2d), _p(n2d), _p(isb), _p(dt), _p(crops),
+                                                *(_p(t) for t in o))
+        if st != 0:
+            raise RuntimeError(f"reference silhouette failed: {st}")
+        return o
+
+    def backward(self, g, g1, dtg, closest, crops):
+        import torch
+        B, Cn, N = g.shape
+        V, U = closest.shape[2], closest.shape[3]
+        out = torch.zeros((B, Cn, N, 2), device=g.device)
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_silhouette_backward(B, Cn, N, U, V, _p(g), _p(g1), _p(dtg), _p(closest), _p(crops),
+                                                 _p(out))
+        if st != 0:
+            raise RuntimeError(f"reference silhouette grad failed: {st}")
+        return out

@@ -36,10 +36,12 @@ def test_forward_matches_reference_kernels(scene):
     ours = EmbeddedGraphEngine(d).forward(*ins)
     ref = O.RefEG(d, DEV).forward(*ins)
     torch.cuda.synchronize()
-    assert torch.equal(ours[0], ref["vertices"]), nrel(ours[0], ref["vertices"])
+    # per-node rotations are evaluated once per node instead of inline per
+    # (vertex, node); sin/cos may then round 1 ulp apart
+    assert nrel(ours[0], ref["vertices"]) < 1e-7
     assert nrel(ours[1], ref["normals"]) < 1e-6
-    assert torch.equal(ours[2], ref["markers"][:, :6])
-    assert torch.equal(ours[3], ref["graph"])
+    assert nrel(ours[2], ref["markers"][:, :6]) < 1e-7
+    assert nrel(ours[3], ref["graph"]) < 1e-7
     assert torch.equal(ours[4], ref["da"]) and torch.equal(ours[5], ref["sa"])
 
 

@@ -1,0 +1,105 @@
+"""Camera projection, projected-mesh boundary and the multi-view silhouette
+loss on the GPU against the reference kernels and the FP64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+from deepcharacters_b200 import synthetic as S
+from deepcharacters_b200.renderer import RendererEngine
+from deepcharacters_b200.silhouette import (SilhouetteEngine, camera_projection_backward, camera_projection_forward,
+                                            projected_mesh_boundary, silhouette_backward)
+from oracle import oracle as O
+from oracle import silhouette_oracle as SO
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference kernels (oracle/_ref) not built")
+RES = 192
+
+
+def _t(a, dt=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV, dt)
+
+
+def nrel(a, b):
+    a = torch.as_tensor(a).double().cpu()
+    b = torch.as_tensor(b).double().cpu()
+    return float((a - b).norm() / max(b.norm().item(), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def scene():
+    sc = S.render_scene(4, batch=2, views=3, width=RES, height=RES, seed=31)
+    verts = _t(sc["verts"])
+    v = sc["verts"].astype(np.float64)
+    normals = v / np.linalg.norm(v, axis=2, keepdims=True)
+    eng = RendererEngine(sc["faces"], sc["texcoords"], sc["N"], 3, RES, RES, "foregroundMask", "shadeless", 2, 2)
+    face = eng.forward(verts, None, None, None, _t(sc["extr"]), _t(sc["intr"]))[1]
+    dt = S.silhouette_masks(2, 3, RES, RES, seed=5, scale=RES / 512)
+    crops = S.identity_crops(2, 3, RES, RES)
+    return dict(sc=sc, verts=verts, normals=_t(normals.astype(np.float32)), face=face, dt=dt, crops=crops)
+
+
+@needs_ref
+def test_projection_matches_reference_kernels(scene):
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    ref = O.RefSilhouette()
+    for is_point in (1, 0):
+        ours = camera_projection_forward(scene["verts"], scene["normals"], ex, it, is_point)
+        theirs = ref.project(scene["verts"], scene["normals"], ex, it, is_point)
+        torch.cuda.synchronize()
+        assert torch.equal(ours, theirs), (is_point, nrel(ours, theirs))
+    g = torch.randn((2, 3, sc["N"], 2), device=DEV, generator=torch.Generator(DEV).manual_seed(1))
+    ours = camera_projection_backward(g, scene["verts"], ex, it, 1)
+    theirs = ref.project_grad(g, scene["verts"], ex, it, 1)
+    assert nrel(ours, theirs) < 1e-6
+
+
+def test_projection_matches_fp64_oracle(scene):
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    p = camera_projection_forward(scene["verts"], None, ex, it, 1)
+    po = SO.project(sc["verts"], None, sc["extr"], sc["intr"], True)
+    assert nrel(p, po) < 1e-6
+    g = np.random.default_rng(2).normal(size=(2, 3, sc["N"], 2))
+    gp = camera_projection_backward(_t(g), scene["verts"], ex, it, 1)
+    assert nrel(gp, SO.project_grad(g, sc["verts"], sc["extr"], sc["intr"])) < 1e-5
+
+
+def _sil_inputs(scene):
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    p2d = camera_projection_forward(scene["verts"], None, ex, it, 1)
+    n2d = camera_projection_forward(scene["verts"], scene["normals"], ex, it, 0)
+    isb = projected_mesh_boundary(p2d, scene["face"], RES, RES)
+    return p2d, n2d, isb, _t(scene["dt"], torch.uint8), _t(scene["crops"])
+
+
+@needs_ref
+def test_silhouette_matches_reference_kernels(scene):
+    p2d, n2d, isb, dt, crops = _sil_inputs(scene)
+    assert int(isb.sum()) > 0
+    eng = SilhouetteEngine()
+    ours = eng.forward(p2d, n2d, isb, dt, crops)
+    ref = O.RefSilhouette().forward(p2d, n2d, isb, dt, crops)
+    torch.cuda.synchronize()
+    names = ("mv_dt_residual", "mv_dt_residual_1", "dt_image_gradient", "closest_vertex_id")
+    for a, b, n in zip(ours, ref, names):
+        assert torch.equal(a, b), (n, nrel(a, b))
+    assert int((ours[3] >= 0).sum()) > 0
+    g = torch.randn(ours[0].shape, device=DEV, generator=torch.Generator(DEV).manual_seed(3))
+    g1 = torch.randn(ours[1].shape, device=DEV, generator=torch.Generator(DEV).manual_seed(4))
+    gp = silhouette_backward(g, g1, ours[2], ours[3], crops)
+    rgp = O.RefSilhouette().backward(g, g1, ref[2], ref[3], crops)
+    assert nrel(gp, rgp) < 1e-6
+
+
+def test_silhouette_matches_fp64_oracle(scene):
+    p2d, n2d, isb, dt, crops = _sil_inputs(scene)
+    ours = SilhouetteEngine().forward(p2d, n2d, isb, dt, crops)
+    ora = SO.silhouette_forward(p2d.cpu().numpy(), n2d.cpu().numpy(), isb.cpu().numpy(), scene["dt"],
+                                scene["crops"])
+    assert np.array_equal(ours[3].cpu().numpy(), ora[3])
+    for a, b in zip(ours[:3], ora[:3]):
+        assert nrel(a, b) < 1e-6

@@ -1,0 +1,123 @@
+"""Device forward kinematics + DQ / LBS skinning against the FP64 oracle and
+the reference skinning kernels (fed with the same dual quaternions /
+transforms, since the reference computes those on the host with Eigen)."""
+import numpy as np
+import pytest
+import torch
+
+from deepcharacters_b200 import synthetic as S
+from deepcharacters_b200.skinning import Character, SkinningEngine, dq_skinning_gpu, lb_skinning_gpu
+from oracle import oracle as O
+from oracle import skinning_oracle as K
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="reference kernels (oracle/_ref) not built")
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).to(DEV)
+
+
+def nrel(a, b):
+    a = torch.as_tensor(a).double().cpu()
+    b = torch.as_tensor(b).double().cpu()
+    return float((a - b).norm() / max(b.norm().item(), 1e-30))
+
+
+@pytest.fixture(scope="module")
+def scene():
+    sc = S.skinning_scene(4, 24, batch=3, seed=17)
+    ch = Character.from_synthetic(sc["skeleton"], sc["verts"], sc["faces"], sc["skin_index"])
+    return sc, ch
+
+
+def test_fk_and_dq_match_fp64_oracle(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    v, n, gp, ga, dq, w = eng.dq_forward(_t(sc["dofs"]), _t(sc["weights"]))
+    _, _, gpos, gaxis = K.fk(ch, sc["dofs"])
+    assert nrel(gp, gpos) < 1e-5 and nrel(ga, gaxis) < 1e-5
+    dq_o = K.dual_quaternions(ch, sc["dofs"])
+    assert np.abs(dq.cpu().numpy() - dq_o).max() < 1e-4
+    vo, no = K.dq_skin(ch, dq_o, sc["weights"])
+    assert nrel(v, vo) < 1e-5 and nrel(n, no) < 1e-5
+    assert torch.equal(w, _t(sc["weights"]))
+
+
+@needs_ref
+def test_dq_skinning_matches_reference_kernels(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    w = _t(sc["weights"])
+    v, n, gp, ga, dq, _ = eng.dq_forward(_t(sc["dofs"]), w)
+    ref = O.RefSkin(ch)
+    rv, rn, rdq, rw = ref.dq_forward(dq, w)
+    torch.cuda.synchronize()
+    assert torch.equal(v, rv) and torch.equal(n, rn) and torch.equal(dq, rdq)
+    g = torch.randn(v.shape, device=DEV, generator=torch.Generator(DEV).manual_seed(1))
+    gd, gw = eng.dq_backward(g, v, gp, ga, dq, w)
+    rgd, rgw = ref.dq_backward(g, v, gp, ga, dq, w, sc["weights"][0])
+    assert nrel(gd, rgd) < 1e-5, nrel(gd, rgd)
+    assert nrel(gw, rgw) < 1e-5, nrel(gw, rgw)
+
+
+@needs_ref
+def test_lbs_skinning_matches_reference_kernels(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    w, disp = _t(sc["weights"]), _t(sc["disp"])
+    v, n, gp, ga, xf, _ = eng.lbs_forward(_t(sc["dofs"]), w, disp)
+    ref = O.RefSkin(ch)
+    rv, rn, rxf, _ = ref.lbs_forward(xf.cpu().numpy(), w, disp)
+    torch.cuda.synchronize()
+    assert torch.equal(xf, rxf)
+    assert nrel(v, rv) < 1e-6 and nrel(n, rn) < 1e-6
+    g = torch.randn(v.shape, device=DEV, generator=torch.Generator(DEV).manual_seed(2))
+    gd, gw, gdisp = eng.lbs_backward(g, v, gp, ga, xf, w)
+    rgd, rgw, rgdisp = ref.lbs_backward(g, v, gp, ga, xf, w, sc["weights"][0])
+    assert nrel(gd, rgd) < 1e-5
+    assert nrel(gw, rgw) < 1e-5
+    assert nrel(gdisp, rgdisp) < 1e-5
+
+
+def test_exact_weight_and_displacement_gradients_match_finite_differences(scene):
+    """With parity off, the weight / displacement gradients are the true derivatives."""
+    sc, ch = scene
+    eng = SkinningEngine(ch, parity=False)
+    B = 1
+    dofs, w, disp = sc["dofs"][:B], sc["weights"][:B].astype(np.float64), sc["disp"][:B].astype(np.float64)
+    g = np.random.default_rng(3).normal(size=(B, ch.base_vertices.shape[0], 3))
+    v, n, gp, ga, dq, _ = eng.dq_forward(_t(dofs), _t(w))
+    _, gw = eng.dq_backward(_t(g), v, gp, ga, dq, _t(w))
+    vl, nl, gpl, gal, xf, _ = eng.lbs_forward(_t(dofs), _t(w), _t(disp))
+    _, lgw, lgd = eng.lbs_backward(_t(g), vl, gpl, gal, xf, _t(w), _t(disp))
+    dq_o = K.dual_quaternions(ch, dofs)
+    Rs, ts = K.skin_transforms(ch, dofs)
+    rng = np.random.default_rng(4)
+    h = 1e-6
+    for _ in range(6):
+        vi, k = int(rng.integers(0, ch.base_vertices.shape[0])), int(rng.integers(0, 4))
+        wp, wm = w.copy(), w.copy()
+        wp[0, vi, k] += h
+        wm[0, vi, k] -= h
+        fd = ((K.dq_skin(ch, dq_o, wp)[0] - K.dq_skin(ch, dq_o, wm)[0])[0, vi] @ g[0, vi]) / (2 * h)
+        assert abs(fd - float(gw[0, vi, k])) <= 1e-3 * max(1.0, abs(fd)), ("dq", fd, float(gw[0, vi, k]))
+        fl = ((K.lbs_skin(ch, Rs, ts, wp, disp)[0] - K.lbs_skin(ch, Rs, ts, wm, disp)[0])[0, vi] @ g[0, vi]) / (2 * h)
+        assert abs(fl - float(lgw[0, vi, k])) <= 1e-3 * max(1.0, abs(fl)), ("lbs", fl, float(lgw[0, vi, k]))
+    Rb = np.einsum("vk,vkij->vij", w[0], Rs[0, ch.skin_index])
+    np.testing.assert_allclose(lgd[0].cpu().numpy(), np.einsum("vji,vj->vi", Rb, g[0]), rtol=1e-4, atol=1e-4)
+
+
+def test_autograd_wrappers(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    dofs = _t(sc["dofs"]).requires_grad_(True)
+    w = _t(sc["weights"]).requires_grad_(True)
+    disp = _t(sc["disp"]).requires_grad_(True)
+    out = dq_skinning_gpu(eng, dofs, w)
+    out[0].sum().backward()
+    assert dofs.grad is not None and w.grad is not None
+    out = lb_skinning_gpu(eng, dofs, w, disp)
+    out[0].square().sum().backward()
+    assert disp.grad is not None and float(disp.grad.abs().sum()) > 0
