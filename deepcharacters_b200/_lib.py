@@ -52,6 +52,7 @@ _SIGS: dict[str, list] = {
     "hc_silhouette_destroy": [vp],
     "hc_silhouette_reserve": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
     "hc_silhouette_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 9,
+    "hc_silhouette_forward_static": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 9,
     "hc_silhouette_backward": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 6,
     "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
     "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,

@@ -14,6 +14,9 @@
 // 3x3 cells around it; the candidate with the smallest distance and, among
 // equal distances, the smallest vertex id is the reference's first-strictly-
 // smaller winner.
+#include <mutex>
+#include <vector>
+
 #include "hc_common.cuh"
 #include "hc_math.cuh"
 
@@ -484,6 +487,95 @@ extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t
     k_sil_grad_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, n_points, resolution_u, resolution_v,
                                                        mv_dt_grad_1, closest_vertex_id, multi_view_crops,
                                                        points_image_space_grad);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// No-allocation variant of the silhouette forward.
+//
+// Some callers cannot call cudaMalloc: a TensorFlow custom op has to take its
+// memory from TF's allocator (which already owns most of the device), and
+// hosts that pre-allocate everything at start-up forbid allocation on their
+// hot path.  This entry point keeps the boundary-vertex grid in a fixed
+// file-scope device array instead of the handle's workspace.  The array is
+// part of the module image, so every GPU that loads the library holds it
+// until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kSilStaticBytes = 8u << 20;  // 8 MiB
+static __device__ __align__(256) int g_sil_static[kSilStaticBytes / sizeof(int)];
+
+// The host-side name g_sil_static is not a device address: resolve it once per
+// device, with that device current.
+hc_status sil_static_base(int** out) {
+    static std::mutex mu;
+    static std::vector<int*> per_device;
+    int dev = 0;
+    HC_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if ((int)per_device.size() <= dev) per_device.resize(dev + 1, nullptr);
+    if (!per_device[dev]) {
+        void* p = nullptr;
+        HC_CUDA(cudaGetSymbolAddress(&p, g_sil_static));
+        per_device[dev] = static_cast<int*>(p);
+    }
+    *out = per_device[dev];
+    return HC_OK;
+}
+
+}  // namespace
+
+extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                  int32_t resolution_u, int32_t resolution_v,
+                                                  const float* points_image_space, const float* normals_image_space,
+                                                  const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                                  const float* multi_view_crops, float* mv_dt_residual,
+                                                  float* mv_dt_residual_1, float* dt_image_gradient,
+                                                  float* closest_vertex_id) {
+    clear_error();
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 2 && resolution_v > 2, "bad sizes");
+    HC_REQUIRE(points_image_space && normals_image_space && is_boundary && distance_transform_image &&
+                   multi_view_crops && mv_dt_residual && mv_dt_residual_1 && dt_image_gradient && closest_vertex_id,
+               "NULL pointer");
+    const int U = resolution_u, V = resolution_v, N = n_points;
+    const long long views = (long long)batch * n_cameras;
+    SilGrid g;
+    g.gx = div_up(U, 30) + 3;
+    g.gy = div_up(V, 30) + 3;
+    const size_t need = grid_bytes(views, g.gx, g.gy, N);
+    HC_REQUIRE(need <= kSilStaticBytes,
+               "hc_silhouette_forward_static: %lld views x %d points at %dx%d need %zu bytes of grid scratch; the "
+               "static scratch holds %zu bytes (use hc_silhouette_forward)",
+               views, N, U, V, need, kSilStaticBytes);
+    int* base = nullptr;
+    HC_TRY(sil_static_base(&base));
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long cells = views * g.gx * g.gy;
+    g.count = base;
+    g.start = base + cells;
+    g.cursor = base + 2 * cells + 1;
+    g.items = base + 3 * cells + 1;
+    // the array keeps the previous call's contents; the cell counts must start at zero
+    HC_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)cells, s));
+    const long long np = views * N;
+    k_sil_points<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, points_image_space, normals_image_space,
+                                                 is_boundary, distance_transform_image, multi_view_crops,
+                                                 mv_dt_residual, dt_image_gradient);
+    HC_CHECK_LAUNCH();
+    k_grid_count<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+                                                 multi_view_crops);
+    HC_CHECK_LAUNCH();
+    k_grid_scan<<<(unsigned)views, 1024, 0, s>>>(g);
+    HC_CHECK_LAUNCH();
+    k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+                                                multi_view_crops);
+    HC_CHECK_LAUNCH();
+    const long long npx = views * U * V;
+    k_sil_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space,
+                                                  distance_transform_image, multi_view_crops, mv_dt_residual_1,
+                                                  closest_vertex_id);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }

@@ -338,6 +338,28 @@ hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras,
                                  const float* closest_vertex_id, const float* multi_view_crops,
                                  float* points_image_space_grad);
 
+/*
+ * hc_silhouette_forward without allocation.  No counterpart in the reference.
+ * For callers that cannot allocate device memory themselves: a TensorFlow
+ * custom op must take its memory from TF's allocator, and hosts that reserve
+ * everything at start-up forbid cudaMalloc on their hot path.  Same arguments
+ * and results as hc_silhouette_forward minus the handle: the boundary-vertex
+ * grid lives in a fixed 8 MiB device array inside the library (held by every
+ * GPU that loads it, until the process exits), which limits a call to
+ *   4 * (B*C * (3 * (ceil(U/30)+3) * (ceil(V/30)+3) + N) + 1) <= 8 MiB,
+ * e.g. 8 views of 1024x1024 with N = 40,962; larger calls return
+ * HC_ERR_INVALID.  The first call on a device resolves the array's device
+ * address with that device current.  All calls on a device share the one array and it keeps the last call's contents: calls
+ * whose kernels overlap on the GPU (e.g. issued on different streams) race,
+ * so order them on one stream.
+ */
+hc_status hc_silhouette_forward_static(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                       int32_t resolution_u, int32_t resolution_v, const float* points_image_space,
+                                       const float* normals_image_space, const uint8_t* is_boundary,
+                                       const uint8_t* distance_transform_image, const float* multi_view_crops,
+                                       float* mv_dt_residual, float* mv_dt_residual_1, float* dt_image_gradient,
+                                       float* closest_vertex_id);
+
 /* ------------------------------------------------------------------------ */
 /* Losses                                                                    */
 /* ------------------------------------------------------------------------ */

@@ -1,0 +1,65 @@
+"""hc_silhouette_forward_static: the silhouette forward for callers that
+cannot allocate device memory (a TensorFlow op must take its memory from TF's
+allocator; some hosts reserve everything at start-up).  Its scratch is a
+fixed 8 MiB array inside libhc.so.  Checked through the C ABI against the
+handle-based hc_silhouette_forward on two calls in a row (the array keeps
+the previous call's contents, so the second call proves it is reset).
+
+This file is named to be collected last."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from deepcharacters_b200 import _lib
+
+
+def _static_call(B, C, N, U, V, ptrs, stream=None):
+    return _lib.lib().hc_silhouette_forward_static(stream, B, C, N, U, V, *ptrs)
+
+
+def test_rejects_calls_larger_than_the_static_scratch():
+    """128 views of 1024x1024 with 40,962 points need ~23 MB of grid: refused
+    before any device work (no GPU needed)."""
+    dummy = [ctypes.c_void_p(16)] * 9
+    st = _static_call(16, 8, 40962, 1024, 1024, dummy)
+    assert st == 1
+    assert b"static scratch holds 8388608 bytes" in _lib.lib().hc_last_error()
+
+
+@pytest.mark.gpu
+def test_static_scratch_matches_allocating_entry_point_twice():
+    import torch
+
+    from deepcharacters_b200 import synthetic as S
+    from deepcharacters_b200.renderer import RendererEngine
+    from deepcharacters_b200.silhouette import SilhouetteEngine, camera_projection_forward, projected_mesh_boundary
+
+    dev = "cuda:0"
+    res = 160
+    t = lambda a, dt=torch.float32: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
+    P = _lib.ptr
+    eng = SilhouetteEngine()
+    for call, seed in enumerate((41, 42)):
+        sc = S.render_scene(3, batch=2, views=3, width=res, height=res, seed=seed)
+        verts = t(sc["verts"])
+        v = sc["verts"].astype(np.float64)
+        normals = t((v / np.linalg.norm(v, axis=2, keepdims=True)).astype(np.float32))
+        ex, it = t(sc["extr"]), t(sc["intr"])
+        r = RendererEngine(sc["faces"], sc["texcoords"], sc["N"], 3, res, res, "foregroundMask", "shadeless", 2, 2)
+        face = r.forward(verts, None, None, None, ex, it)[1]
+        p2d = camera_projection_forward(verts, None, ex, it, 1)
+        n2d = camera_projection_forward(verts, normals, ex, it, 0)
+        isb = projected_mesh_boundary(p2d, face, res, res)
+        dt = t(S.silhouette_masks(2, 3, res, res, seed=seed, scale=res / 512), torch.uint8)
+        crops = t(S.identity_crops(2, 3, res, res))
+        ref = eng.forward(p2d, n2d, isb, dt, crops)
+        B, Cn, N = p2d.shape[:3]
+        out = [torch.full_like(x, 7.0) for x in ref]
+        st = _static_call(B, Cn, N, res, res, [P(p2d), P(n2d), P(isb), P(dt), P(crops)] + [P(x) for x in out],
+                          torch.cuda.current_stream().cuda_stream)
+        assert st == 0, _lib.lib().hc_last_error()
+        torch.cuda.synchronize()
+        assert int((ref[3] >= 0).sum()) > 0
+        for a, b in zip(out, ref):
+            assert torch.equal(a, b), f"call {call}"
