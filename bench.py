@@ -1,12 +1,15 @@
 #!/usr/bin/env python
 """Benchmark of the deform-and-render chain: fwd+bwd views/s at 81,920 triangles, 1024x1024.
 
-Workload (one "step"): 16 frames x 8 views of an icosphere subdivision-6 mesh
-(40,962 vertices / 81,920 triangles, radius 1 m = 1000 units, 1 cm vertex
-jitter), cameras on a 3 m ring (fx = fy = 1200), vertex-colour rasterization,
-the masked L1 image loss against seeded target images, and the renderer
-adjoint (gradients w.r.t. vertex positions and vertex colours).  Synthetic
-data; inputs larger than L2 (1.6 GB of target images per step).
+Workload (one "step"): the deform-and-render chain on 16 frames x 8 views of
+a character built on an icosphere subdivision-6 mesh (40,962 vertices /
+81,920 triangles, radius 1 m = 1000 units, 1 cm vertex jitter): node skinning
+of a 1000-node embedded graph by a 24-joint tree (3 revolute dofs each),
+embedded-graph deformation, vertex-colour rasterization at 1024x1024 from
+cameras on a 3 m ring (fx = fy = 1200), the masked L1 image loss, camera
+projection + projected-mesh boundary + the silhouette distance-transform loss,
+and the adjoints back to node rotations / translations and vertex colours.
+Synthetic data; inputs larger than L2 (1.6 GB of target images per step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -15,8 +18,9 @@ ours:       the chain through libhc.so, captured once in a CUDA graph and
             same step through the public Python API with every step's inputs
             copied from pinned host memory and the loss read back.
 reference:  the reference's own CUDA kernels (compiled unmodified for sm_100a
-            into oracle/_ref) driven per frame like its TF ops, the plain
-            per-view per-op path, with the L1 loss as elementwise torch ops.
+            into oracle/_ref) driven op by op like its TF ops (the renderer
+            per frame), node skinning on the host as the reference's CPU op,
+            the losses as elementwise torch ops: the plain per-op path.
 Under torchrun every rank runs its own 16 frames (weak scaling); the
 gradient of the shared vertex colours is all-reduced over NCCL each step.
 """
@@ -136,100 +140,77 @@ def max_over_ranks(x: float, world: int) -> float:
 # --------------------------------------------------------------------------
 # workload
 # --------------------------------------------------------------------------
+N_NODES, N_SKEL, FX = 1000, 24, 1200.0
+W_SIL, W_SIL1 = 1e-3, 1e-3  # weights of the two silhouette residual terms
+
+
 def make_workload(rank: int):
     from deepcharacters_b200 import synthetic as S
-    sc = S.render_scene(SUBDIV, batch=FRAMES, views=VIEWS, width=RES, height=RES, seed=2 + 100 * rank, fx=1200.0,
-                        texture_size=16)
-    # the foreground mask of the data term: inside of a seeded ellipse per view
-    return sc
+    return S.chain_scene(SUBDIV, N_NODES, N_SKEL, FRAMES, VIEWS, RES, RES, seed=2 + 100 * rank, fx=FX)
 
 
 def cpu_baseline(sc, frames=1, views=2):
-    """The oracle restatement in float on the host cores (bounded sample)."""
+    """The oracle restatement on the host cores (bounded sample): node
+    skinning + EG forward, raster + L1 + raster adjoint + EG adjoint in float."""
+    from deepcharacters_b200.chain import character, eg_data
     from oracle import oracle as O
-    sub = {k: sc[k] for k in ("faces", "texcoords")}
+    from oracle import skinning_oracle as K
     B, C = frames, views
-    verts = sc["verts"][:B]
-    colors = sc["colors"][:B]
+    d = eg_data(sc)
+    ch = character(sc)
+    cores = os.cpu_count() or 1
     extr = sc["extr"][:B, :12 * C]
     intr = sc["intr"][:B, :9 * C]
-    sh = sc["sh"][:B, :C]
-    target = sc["target"][:B, :C]
-    tex = sc["texture"][:B]
-    cores = os.cpu_count() or 1
     t0 = time.perf_counter()
-    fw = O.render_forward(sub["faces"], sub["texcoords"], B, C, RES, RES, "vertexColor", "shadeless", verts, colors,
-                          tex, sh, extr, intr, precision="f32", nthreads=cores, fragile=False)
+    sT, sA, _ = K.pose2eg(ch, sc["dofs"][:B], sc["graph"].node_vertex, sc["skin_weights"])
+    eg = O.eg_forward(d, sc["dT"][:B], sc["dA"][:B], sT.astype(np.float32), sA.astype(np.float32), sc["disp"][:B],
+                      precision="f32")
+    verts = eg["vertices"]
+    fw = O.render_forward(sc["faces"], sc["texcoords"], B, C, RES, RES, "vertexColor", "shadeless", verts,
+                          sc["colors"][:B], sc["texture"][:B], sc["sh"][:B, :C], extr, intr, precision="f32",
+                          nthreads=cores, fragile=False)
     m = (fw["face"] >= 0)[..., None]
-    diff = 255.0 * (fw["render"] - target) * m
+    diff = 255.0 * (fw["render"] - sc["target"][:B, :C]) * m
     cnt = max(int(np.count_nonzero(diff)), 1)
     g = (255.0 * np.sign(diff) / cnt).astype(np.float32)
-    O.render_backward(sub["faces"], sub["texcoords"], B, C, RES, RES, "vertexColor", "shadeless", g, verts, colors,
-                      tex, sh, target, fw["vnormal"], fw["bary"], fw["face"], extr, intr, precision="f32",
-                      nthreads=cores)
+    bw = O.render_backward(sc["faces"], sc["texcoords"], B, C, RES, RES, "vertexColor", "shadeless", g, verts,
+                           sc["colors"][:B], sc["texture"][:B], sc["sh"][:B, :C], sc["target"][:B, :C], fw["vnormal"],
+                           fw["bary"], fw["face"], extr, intr, precision="f32", nthreads=cores)
+    O.eg_backward(d, bw["vertex_pos_grad"], np.zeros((B, 8, 3), np.float32), sc["dT"][:B], sc["dA"][:B],
+                  sA.astype(np.float32), sc["disp"][:B], precision="f32")
     dt = time.perf_counter() - t0
     return {"value": B * C / dt, "unit": "views/s", "cores": cores, "kind": "port",
-            "sample": f"{B} frame x {C} views of the same workload (fwd + L1 + bwd, float oracle, OpenMP)"}
+            "sample": f"{B} frame x {C} views of the same workload: node skinning + EG fwd, raster + L1 + raster "
+                      "adjoint + EG adjoint (float oracle, OpenMP; silhouette terms not in the sample)"}
 
 
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
-class Chain:
-    """One fwd + loss + bwd step through libhc.so on device-resident buffers."""
-
-    def __init__(self, sc, dev):
-        from deepcharacters_b200.renderer import RendererEngine
-        self.eng = RendererEngine(sc["faces"], sc["texcoords"], sc["N"], VIEWS, RES, RES, "vertexColor", "shadeless",
-                                  2, 2)
-        self.eng.set_tuning(8, 256)
-        self.eng.reserve(FRAMES)
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-        self.inp = {k: t(sc[k]) for k in ("verts", "colors", "texture", "sh", "extr", "intr", "target")}
-        B, C, H, W, N = FRAMES, VIEWS, RES, RES, sc["N"]
-        self.out = dict(bary=torch.empty((B, C, H, W, 2), device=dev), face=torch.empty((B, C, H, W), device=dev,
-                                                                                         dtype=torch.int32),
-                        render=torch.empty((B, C, H, W, 3), device=dev), vnormal=torch.empty((B, C, N, 3), device=dev))
-        self.grad_img = torch.empty((B, C, H, W, 3), device=dev)
-        self.loss = torch.zeros((1,), device=dev)
-        self.ws = torch.zeros((4,), device=dev, dtype=torch.float64)
-        self.gpos = torch.empty((B, N, 3), device=dev)
-        self.gcol = torch.empty((B, N, 3), device=dev)
-        self.gsh = torch.empty((B, C, 27), device=dev)
-        self.n_px = B * C * H * W
-
-    def forward(self):
-        i = self.inp
-        self.eng.forward(i["verts"], i["colors"], i["texture"], i["sh"], i["extr"], i["intr"], out=self.out)
-
-    def loss_grad(self):
-        from deepcharacters_b200 import _lib
-        from deepcharacters_b200.renderer import _stream
-        P = _lib.ptr
-        _lib.call("hc_image_l1_loss", _stream(), self.n_px, P(self.out["render"]), P(self.inp["target"]),
-                  P(self.out["face"]), None, P(self.ws), P(self.loss), P(self.grad_img))
-
-    def backward(self):
-        from deepcharacters_b200 import _lib
-        from deepcharacters_b200.renderer import _stream
-        P = _lib.ptr
-        i, o = self.inp, self.out
-        _lib.call("hc_renderer_backward", self.eng.handle, _stream(), FRAMES, P(self.grad_img), P(i["verts"]),
-                  P(i["colors"]), P(i["texture"]), 16, 16, P(i["sh"]), P(i["target"]), P(o["vnormal"]),
-                  P(o["bary"]), P(o["face"]), P(i["extr"]), P(i["intr"]), P(self.gpos), P(self.gcol), None,
-                  P(self.gsh))
-
-    def step(self):
-        self.forward()
-        self.loss_grad()
-        self.backward()
+def stage_bytes(sc):
+    """Algorithmic bytes per call of each stage (compulsory traffic of what
+    the stage must read and write once)."""
+    B, C, P, N, F, M = FRAMES, VIEWS, RES * RES, sc["N"], sc["F"], sc["M"]
+    K = 4
+    eg = B * (12 * N * 2 + 8 * K * N + 24 * M) + 12 * N  # read base / write verts + normals, CSR, node params
+    return {
+        # EG + raster: verts read, bary 8 + face 4 + render 12 written per pixel; L1 reads render + target,
+        # writes the image gradient
+        "deform_render_forward": eg + B * C * (24 * P + 12 * N) + B * C * (12 + 12 + 4 + 12) * P,
+        # projection, coverage + boundary, per-pixel silhouette residual (dt 1, res1 8, closest 4), squared loss
+        "silhouette_forward": B * C * (16 * N + 1 * P + 1 * P + 12 * P + 8 * P + 8 * 3 * N),
+        "silhouette_backward": B * C * (8 * P + 4 * P + 24 * N) + B * 24 * N,
+        # bwd raster reads grad image 12 + bary 8 + face 4 per pixel, writes vertex grads; EG adjoint
+        "render_eg_backward": B * C * 24 * P + B * (36 * N + 24 * N) + eg,
+    }
 
 
 def run_ours(args, world, rank, local):
     from deepcharacters_b200 import _lib
     dev = torch.device("cuda", local)
+    from deepcharacters_b200.chain import DeformRenderChain
     sc = make_workload(rank)
-    ch = Chain(sc, dev)
+    ch = DeformRenderChain(sc, dev, FRAMES, VIEWS, RES, RES, W_SIL, W_SIL1)
     views_per_step = FRAMES * VIEWS
     # eager warm-up (allocates every workspace), then capture one step
     for _ in range(2):
@@ -248,7 +229,7 @@ def run_ours(args, world, rank, local):
 
     def allreduce():
         if world > 1:
-            torch.distributed.all_reduce(ch.gcol)
+            torch.distributed.all_reduce(ch.buf["gcol"])
 
     for _ in range(args.warmup):
         g.replay()
@@ -272,8 +253,7 @@ def run_ours(args, world, rank, local):
 
     # per-stage device time (eager, same inputs) for the roofline of the dominant call
     stage_ms = {}
-    for name, fn in (("render_forward", ch.forward), ("image_l1_loss", ch.loss_grad),
-                     ("render_backward", ch.backward)):
+    for name, fn in ch.stages():
         fn()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -283,13 +263,8 @@ def run_ours(args, world, rank, local):
         b.record()
         torch.cuda.synchronize()
         stage_ms[name] = a.elapsed_time(b) / 3
+    sbytes = stage_bytes(sc)
     N, F = sc["N"], sc["F"]
-    P = RES * RES
-    stage_bytes = {  # algorithmic bytes per call
-        "render_forward": views_per_step * 24 * P + FRAMES * (24 * N + 12 * F),
-        "image_l1_loss": views_per_step * (12 + 12 + 4 + 12) * P,
-        "render_backward": views_per_step * (4 + 8 + 12 + 12) * P + FRAMES * (24 * N + 12 * F + 24 * N),
-    }
     dom = max(stage_ms, key=stage_ms.get)
     peaks = {}
     try:
@@ -297,22 +272,27 @@ def run_ours(args, world, rank, local):
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    ach = stage_bytes[dom] / (stage_ms[dom] / 1e3) / 1e9
+    ach = sbytes[dom] / (stage_ms[dom] / 1e3) / 1e9
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = None
     if os.path.exists(traffic_path):
         traffic = json.load(open(traffic_path)).get(dom)
 
-    # e2e: public API, pinned host inputs copied every step, loss read back
+    # e2e: public API, pinned host inputs copied every step, losses read back
     e2e = None if args.no_e2e else run_e2e(ch, sc, dev, args, world)
 
     line = {
         "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded icosphere, ring cameras, random targets)",
-        "config": {"workload": "icosphere subdiv-6 (40,962 verts / 81,920 tris) x 16 frames x 8 views 1024x1024, "
-                               "vertexColor shadeless raster + masked L1 + adjoint, CUDA graph",
-                   "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES], "triangles": F,
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded icosphere character, random pose / node deltas, ring cameras, random targets, "
+                "ellipse silhouettes)",
+        "config": {"workload": "deform-and-render chain fwd+bwd: icosphere subdiv-6 (40,962 verts / 81,920 tris), "
+                               "1000-node embedded graph (K=4) skinned by a 24-joint tree (node DQ), 16 frames x 8 "
+                               "views 1024x1024, vertexColor raster + masked L1 + silhouette DT loss, gradients to "
+                               "node rotations / translations and vertex colours, one CUDA graph per step",
+                   "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES], "triangles": F, "vertices": N,
+                   "nodes": N_NODES, "joints": 3 * N_SKEL,
                    "parallelism": f"frames sharded, {world} rank(s)",
                    "l2": "inputs larger than L2 (1.6 GB of target images per step)",
                    "raster_tile": 8, "bin_capacity": 256},
@@ -321,7 +301,7 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
-                     "stage_ms": stage_ms,
+                     "stage_ms": stage_ms, "stage_bytes": sbytes,
                      "chain_bytes_per_view": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS),
                      "chain_frac": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS) * value / world / 1e9 / peak},
         "clocks": clocks,
@@ -332,16 +312,19 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+E2E_KEYS = ("dofs", "dT", "dA", "colors", "sh", "extr", "intr", "target", "dt")
+
+
 def run_e2e(ch, sc, dev, args, world):
-    """Same step through the public API with host inputs: per step H2D of
-    vertex positions, colours, cameras, SH and target images from pinned
-    memory (double-buffered on a copy stream) and D2H of the loss."""
-    keys = ("verts", "colors", "sh", "extr", "intr", "target")
-    host = {k: torch.from_numpy(np.ascontiguousarray(sc[k])).pin_memory() for k in keys}
-    bufs = [{k: torch.empty_like(ch.inp[k]) for k in keys} for _ in range(2)]
+    """Same step through the C ABI with host inputs: per step H2D of the pose,
+    node deltas, vertex colours, cameras, SH, target images and distance
+    images from pinned memory (double-buffered on a copy stream) and D2H of
+    the three loss values."""
+    host = {k: torch.from_numpy(np.ascontiguousarray(sc[k])).pin_memory() for k in E2E_KEYS}
+    bufs = [{k: torch.empty_like(ch.inp[k]) for k in E2E_KEYS} for _ in range(2)]
     h2d = sum(v.numel() * v.element_size() for v in host.values())
     copy = torch.cuda.Stream()
-    loss_host = torch.zeros((1,), dtype=torch.float32).pin_memory()
+    loss_host = torch.zeros((3,), dtype=torch.float32).pin_memory()
     ready = [torch.cuda.Event() for _ in range(2)]
     done = [torch.cuda.Event() for _ in range(2)]
     saved = dict(ch.inp)
@@ -349,7 +332,7 @@ def run_e2e(ch, sc, dev, args, world):
     def upload(slot):
         with torch.cuda.stream(copy):
             copy.wait_event(done[slot])
-            for k in keys:
+            for k in E2E_KEYS:
                 bufs[slot][k].copy_(host[k], non_blocking=True)
             ready[slot].record(copy)
 
@@ -362,11 +345,11 @@ def run_e2e(ch, sc, dev, args, world):
             torch.cuda.current_stream().wait_event(ready[slot])
             if i + 1 < n:
                 upload((i + 1) % 2)
-            for k in keys:
+            for k in E2E_KEYS:
                 ch.inp[k] = bufs[slot][k]
             ch.step()
             if world > 1:
-                torch.distributed.all_reduce(ch.gcol)
+                torch.distributed.all_reduce(ch.buf["gcol"])
             done[slot].record()
             loss_host.copy_(ch.loss, non_blocking=True)
         torch.cuda.synchronize()
@@ -379,8 +362,8 @@ def run_e2e(ch, sc, dev, args, world):
     dt = max_over_ranks(time.perf_counter() - t0, world)
     ch.inp.update(saved)
     return {"value": FRAMES * VIEWS * world * args.steps / dt, "unit": "views/s", "h2d_bytes_per_step": h2d,
-            "d2h_bytes_per_step": 4, "ms_per_step": dt / args.steps * 1e3,
-            "path": "RendererEngine.forward + hc_image_l1_loss + hc_renderer_backward, eager, pinned double buffer"}
+            "d2h_bytes_per_step": 12, "ms_per_step": dt / args.steps * 1e3,
+            "path": "the same C-ABI calls issued eagerly per step, inputs from pinned host memory (double buffer)"}
 
 
 # --------------------------------------------------------------------------
@@ -390,24 +373,16 @@ def run_reference(args, world, rank, local):
     if rank != 0:
         return
     from oracle import oracle as O
-    if not O.ref_available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhcref.so was not built"}))
+    if not (O.ref_available() and os.path.exists(O.REF_MB_LIB)):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference kernels were not built"}))
         return
+    from oracle.chain_ref import RefChain
     dev = torch.device("cuda", local)
     sc = make_workload(0)
-    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-    inp = {k: t(sc[k]) for k in ("verts", "colors", "texture", "sh", "extr", "intr", "target")}
-    ref = O.RefRenderer(sc["faces"], sc["texcoords"], sc["N"], VIEWS, RES, RES, "vertexColor", "shadeless", "none", 2,
-                        2)
+    ref = RefChain(sc, dev, FRAMES, VIEWS, RES, RES, W_SIL, W_SIL1)
 
     def step():
-        fw = ref.forward(FRAMES, inp["verts"], inp["colors"], inp["texture"], inp["sh"], inp["extr"], inp["intr"],
-                         depth=False, sync_each=0)
-        diff = 255.0 * (fw["render"] - inp["target"]) * (fw["face"] >= 0).unsqueeze(-1)
-        cnt = torch.count_nonzero(diff).clamp_min(1)
-        g = 255.0 * torch.sign(diff) / cnt
-        ref.backward(FRAMES, g.contiguous(), inp["verts"], inp["colors"], inp["texture"], inp["sh"], inp["target"],
-                     fw["vnormal"], fw["bary"], fw["face"], inp["extr"], inp["intr"])
+        ref.step()
 
     for _ in range(args.warmup):
         step()
@@ -425,12 +400,16 @@ def run_reference(args, world, rank, local):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "icosphere subdiv-6 (40,962 verts / 81,920 tris) x 16 frames x 8 views 1024x1024, "
-                               "vertexColor shadeless raster + masked L1 + adjoint",
+        "config": {"workload": "deform-and-render chain fwd+bwd: icosphere subdiv-6 (40,962 verts / 81,920 tris), "
+                               "1000-node embedded graph (K=4) skinned by a 24-joint tree (node DQ), 16 frames x 8 "
+                               "views 1024x1024, vertexColor raster + masked L1 + silhouette DT loss, gradients to "
+                               "node rotations / translations and vertex colours",
                    "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES]},
         "cpu_baseline": {"value": value, "unit": "views/s", "kind": "reference", "cores": 1,
-                         "sample": "full step; the reference's own CUDA kernels (CUDABasedRasterization{,Grad}.cu, "
-                                   "unmodified, sm_100a) launched per frame from one host thread like its TF ops"},
+                         "sample": "full step; the reference's own CUDA kernels (renderer, EG, camera projection, "
+                                   "mesh boundary, silhouette loss; unmodified, sm_100a) launched per op like its TF "
+                                   "ops (renderer per frame), Pose2EG on the host (numpy restatement of the C++ op), "
+                                   "losses as torch elementwise ops"},
         "e2e": {"value": value, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "clocks": clocks,
     }

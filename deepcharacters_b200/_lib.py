@@ -54,6 +54,15 @@ _SIGS: dict[str, list] = {
     "hc_silhouette_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 9,
     "hc_silhouette_forward_static": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 9,
     "hc_silhouette_backward": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32] + [vp] * 6,
+    "hc_pose2eg_forward": [vp, vp, C.c_int32, vp, C.c_int32, vp, vp, vp, vp, vp],
+    "hc_pose2eg_backward": [vp, vp, C.c_int32, vp, C.c_int32, vp, vp, vp, vp, vp],
+    "hc_mesh_boundary_create": [vp, vp, C.c_int32, C.c_int32],
+    "hc_mesh_boundary_destroy": [vp],
+    "hc_mesh_boundary_reserve": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
+    "hc_mesh_boundary_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp],
+    "hc_sum_squares_loss": [vp, C.c_int64, vp, C.c_float, vp, vp, vp],
+    "hc_add_inplace": [vp, C.c_int64, vp, vp],
+    "hc_gaussian_smooth": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, vp, vp],
     "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
     "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
                              vp, vp, vp, vp],

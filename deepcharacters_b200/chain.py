@@ -1,0 +1,162 @@
+"""The deform-and-render training step as one object: the composition of
+the reference ops that Projects/HoloportedCharacters/HPCMeshDL.py builds in
+TF (Pose2EmbeddedGraphCpu -> EmbeddedGraphGpu -> CudaRendererGpu with the L1
+image loss, and CameraProjectionGpu -> ProjectedMeshBoundaryGpu ->
+MultiViewSilhouetteLossGpu with a sum-of-squares loss on its residuals),
+with their registered gradients, issued as C-ABI calls on preallocated
+device buffers so that a whole step can be captured in one CUDA graph.
+
+Scene dictionary keys (see ``synthetic.chain_scene``): verts [N,3], faces
+[F,3], graph (EmbeddedGraph), markers [8,3], marker_node [8], skeleton,
+skin_index / skin_weights [N,K], texcoords, and per-frame dofs [B,D], dT / dA
+[B,M,3], disp [B,N,3], colors [B,N,3], texture, sh [B,C,27], extr [B,12C],
+intr [B,9C], target [B,C,H,W,3], dt [B,C,H,W] uint8, crops [B,C,7].
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .embedded_graph import EGData, EmbeddedGraphEngine
+from .renderer import RendererEngine, _stream
+from .silhouette import MeshBoundaryEngine, SilhouetteEngine
+from .skinning import Character, SkinningEngine
+
+
+def character(sc) -> Character:
+    return Character.from_synthetic(sc["skeleton"], sc["verts"], sc["faces"], sc["skin_index"])
+
+
+def eg_data(sc) -> EGData:
+    return EGData.from_synthetic(sc["verts"], sc["faces"], sc["graph"], sc["markers"], sc["marker_node"])
+
+
+class DeformRenderChain:
+    """One fwd + loss + bwd step of the deform-and-render chain through
+    libhc.so on device-resident buffers:
+
+      dofs -> node skinning (Pose2EG) -> EG deformation -> raster (vertexColor)
+           -> masked L1 image loss
+      EG vertices -> camera projection -> mesh boundary -> silhouette DT loss
+      adjoints back to node rotations / translations and vertex colours.
+
+    ``loss`` holds (L1, silhouette model->data, silhouette data->model);
+    ``buf`` holds every intermediate and gradient (``gT`` / ``gA`` are the
+    node translation / rotation gradients, ``gcol`` the vertex colours',
+    ``gdofs`` the joint angles' when ``joint_gradients`` is set: the EG then
+    returns its skinned-transform gradients and the node skinning's adjoint
+    carries them to the dofs; the reference chain has no such gradient, its
+    Pose2EmbeddedGraphCpu op being non-differentiable)."""
+
+    def __init__(self, sc, dev, frames: int, views: int, width: int, height: int, w_sil: float = 1e-3,
+                 w_sil1: float = 1e-3, tile: int = 8, bin_capacity: int = 256, gradient_parity: bool = False,
+                 joint_gradients: bool = True):
+        B, C, H, W, N = frames, views, height, width, int(sc["verts"].shape[0])
+        M = int(sc["graph"].n_nodes)
+        Mk = int(len(sc["markers"]))
+        self.B, self.C, self.H, self.W, self.N, self.M, self.Mk = B, C, H, W, N, M, Mk
+        self.w_sil, self.w_sil1 = float(w_sil), float(w_sil1)
+        self.skin = SkinningEngine(character(sc))
+        self.skin.reserve(B)
+        self.joint_gradients = bool(joint_gradients)
+        self.eg = EmbeddedGraphEngine(eg_data(sc), full_skinned_gradient=self.joint_gradients)
+        self.eg.reserve(B)
+        self.rend = RendererEngine(sc["faces"], sc["texcoords"], N, C, W, H, "vertexColor", "shadeless", 2, 2)
+        self.rend.set_tuning(tile, bin_capacity)
+        if gradient_parity:
+            _lib.call("hc_renderer_set_gradient_parity", self.rend.handle, 1)
+        self.rend.reserve(B)
+        self.mb = MeshBoundaryEngine(sc["faces"], N)
+        self.mb.reserve(B, C, W, H)
+        self.sil = SilhouetteEngine()
+        self.sil.reserve(B, C, N, W, H)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+        self.inp = {k: t(sc[k]) for k in ("dofs", "dT", "dA", "disp", "colors", "texture", "sh", "extr", "intr",
+                                          "target", "dt", "crops")}
+        self.tex_hw = (int(sc["texture"].shape[1]), int(sc["texture"].shape[2]))
+        self.node_vertex = t(sc["graph"].node_vertex.astype(np.int32))
+        self.skin_w = t(np.asarray(sc["skin_weights"], np.float32))
+        e = lambda *shape, dt=torch.float32: torch.empty(shape, device=dev, dtype=dt)  # noqa: E731
+        self.buf = dict(
+            sT=e(B, M, 3), sA=e(B, M, 3), dq=e(B, self.skin.S, 8),
+            v=e(B, N, 3), n=e(B, N, 3), mk=e(B, Mk, 3), graph=e(B, M, 3), da=e(B, M, 3), sa=e(B, M, 3),
+            bary=e(B, C, H, W, 2), face=e(B, C, H, W, dt=torch.int32), render=e(B, C, H, W, 3),
+            vnormal=e(B, C, N, 3), grad_img=e(B, C, H, W, 3),
+            p2d=e(B, C, N, 2), n2d=e(B, C, N, 2), isb=e(B, C, N, dt=torch.uint8),
+            res=e(B, C, N), res1=e(B, C, H, W, 2), dtg=e(B, C, N, 2), cid=e(B, C, H, W),
+            g_res=e(B, C, N), g_res1=e(B, C, H, W, 2), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
+            gv=e(B, N, 3), gcol=e(B, N, 3), gsh=e(B, C, 27), gm=torch.zeros((B, Mk, 3), device=dev),
+            gT=e(B, M, 3), gA=e(B, M, 3), gsT=e(B, M, 3), gsA=e(B, M, 3), gdisp=e(B, N, 3),
+            gdofs=torch.zeros((B, self.skin.D), device=dev))
+        self.loss = torch.zeros((3,), device=dev)
+        self.ws = torch.zeros((8,), device=dev, dtype=torch.float64)
+
+    def forward(self):
+        """Node skinning, EG deformation, raster and the L1 image loss + its gradient."""
+        L, P, s = _lib.call, _lib.ptr, _stream()
+        i, o = self.inp, self.buf
+        B, C, H, W, M = self.B, self.C, self.H, self.W, self.M
+        L("hc_pose2eg_forward", self.skin.handle, s, B, P(i["dofs"]), M, P(self.node_vertex), P(self.skin_w),
+          P(o["sT"]), P(o["sA"]), P(o["dq"]))
+        L("hc_eg_forward", self.eg.handle, s, B, P(i["dT"]), P(i["dA"]), P(o["sT"]), P(o["sA"]), P(i["disp"]),
+          P(o["v"]), P(o["n"]), P(o["mk"]), P(o["graph"]), P(o["da"]), P(o["sa"]))
+        L("hc_renderer_forward", self.rend.handle, s, B, P(o["v"]), P(i["colors"]), P(i["texture"]), *self.tex_hw,
+          P(i["sh"]), P(i["extr"]), P(i["intr"]), P(o["bary"]), P(o["face"]), P(o["render"]), P(o["vnormal"]), None)
+        L("hc_image_l1_loss", s, B * C * H * W, P(o["render"]), P(i["target"]), P(o["face"]), None, P(self.ws),
+          P(self.loss), P(o["grad_img"]))
+
+    def silhouette_forward(self):
+        """Camera projection, mesh boundary, silhouette DT loss + residual gradients."""
+        L, P, s = _lib.call, _lib.ptr, _stream()
+        i, o = self.inp, self.buf
+        B, C, H, W, N = self.B, self.C, self.H, self.W, self.N
+        L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), None, P(i["extr"]), P(i["intr"]), 1, P(o["p2d"]))
+        L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), P(o["n"]), P(i["extr"]), P(i["intr"]), 0,
+          P(o["n2d"]))
+        L("hc_mesh_boundary_forward", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]), P(i["intr"]),
+          P(o["p2d"]), P(o["isb"]))
+        L("hc_silhouette_forward", self.sil.handle, s, B, C, N, W, H, P(o["p2d"]), P(o["n2d"]), P(o["isb"]),
+          P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
+        L("hc_sum_squares_loss", s, B * C * N, P(o["res"]), self.w_sil, self.ws.data_ptr() + 16,
+          self.loss.data_ptr() + 4, P(o["g_res"]))
+        L("hc_sum_squares_loss", s, B * C * H * W * 2, P(o["res1"]), self.w_sil1, self.ws.data_ptr() + 24,
+          self.loss.data_ptr() + 8, P(o["g_res1"]))
+
+    def silhouette_backward(self):
+        """Silhouette adjoint and the camera-projection adjoint to vertex positions."""
+        L, P, s = _lib.call, _lib.ptr, _stream()
+        i, o = self.inp, self.buf
+        B, C, H, W, N = self.B, self.C, self.H, self.W, self.N
+        L("hc_silhouette_backward", s, B, C, N, W, H, P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]),
+          P(i["crops"]), P(o["gp2d"]))
+        L("hc_camera_projection_backward", s, B, C, N, P(o["gp2d"]), P(o["v"]), P(i["extr"]), P(i["intr"]), 1,
+          P(o["gv_sil"]))
+
+    def backward(self):
+        """Raster adjoint, the sum of the two vertex-position gradients, EG adjoint
+        (and the node-skinning adjoint to the joint angles)."""
+        L, P, s = _lib.call, _lib.ptr, _stream()
+        i, o = self.inp, self.buf
+        B, N = self.B, self.N
+        L("hc_renderer_backward", self.rend.handle, s, B, P(o["grad_img"]), P(o["v"]), P(i["colors"]),
+          P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]), P(o["bary"]), P(o["face"]),
+          P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
+        L("hc_add_inplace", s, B * N * 3, P(o["gv"]), P(o["gv_sil"]))
+        full = self.joint_gradients
+        L("hc_eg_backward", self.eg.handle, s, B, P(o["gv"]), P(o["gm"]), P(o["da"]), P(o["sa"]), P(o["gT"]),
+          P(o["gA"]), P(o["gsT"]), P(o["gsA"]), P(o["gdisp"]), P(i["dT"]) if full else None,
+          P(i["disp"]) if full else None)
+        if full:  # joint angles through the node skinning
+            L("hc_pose2eg_backward", self.skin.handle, s, B, P(i["dofs"]), self.M, P(self.node_vertex),
+              P(self.skin_w), P(o["gsT"]), P(o["gsA"]), P(o["gdofs"]))
+
+    def step(self):
+        self.forward()
+        self.silhouette_forward()
+        self.silhouette_backward()
+        self.backward()
+
+    def stages(self):
+        return (("deform_render_forward", self.forward), ("silhouette_forward", self.silhouette_forward),
+                ("silhouette_backward", self.silhouette_backward), ("render_eg_backward", self.backward))

@@ -4,6 +4,8 @@
 // loss = sum |difference| / count_nonzero(difference)), and its gradient
 // d loss / d R = 255 sign(difference) * mask * model_mask / count
 // (the count is a constant for the gradient, as in TF).
+#include <math.h>
+
 #include "hc_common.cuh"
 
 namespace hc {
@@ -76,10 +78,148 @@ __global__ void k_l1_grad(long long n_px, const float* __restrict__ render, cons
     }
 }
 
+// sum of squares: acc += sum x^2 (block partials in double)
+__global__ void k_sumsq_reduce(long long n, const float* __restrict__ x, double* __restrict__ acc) {
+    float s = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        s += x[i] * x[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ float ss[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) ss[w] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += ss[i];
+        atomicAdd(acc, t);
+    }
+}
+
+__global__ void k_sumsq_grad(long long n, const float* __restrict__ x, float weight, const double* __restrict__ acc,
+                             float* __restrict__ grad, float* __restrict__ loss) {
+    if (blockIdx.x == 0 && threadIdx.x == 0 && loss) *loss = (float)(weight * *acc);
+    const float k = 2.f * weight;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        grad[i] = k * x[i];
+}
+
+__global__ void k_add_inplace(long long n, float* __restrict__ dst, const float* __restrict__ src) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+
+// Gaussian smoothing of images (Projects/CustomTFOperators/GaussianSmoothingGpu.py:12-37):
+// a depthwise (2s+1)^2 convolution with the normalised outer product of a
+// sampled normal density, zero padding ("SAME").  The kernel is separable, so
+// each CTA stages a 32x32 output tile with its halo in shared memory and runs
+// a horizontal then a vertical pass: one read and one write of the image.
+constexpr int kSmoothTile = 32;
+constexpr int kSmoothMax = 15;
+
+struct SmoothTaps {
+    float w[2 * kSmoothMax + 1];
+};
+
+__global__ void k_smooth(int H, int W, int Cn, int s, SmoothTaps taps, const float* __restrict__ in,
+                         float* __restrict__ out) {
+    extern __shared__ float sm[];
+    const int E = kSmoothTile + 2 * s;
+    float* s_in = sm;                       // [E][E][Cn]
+    float* s_h = sm + (size_t)E * E * Cn;   // [E][32][Cn]
+    const int img = blockIdx.z;
+    const int x0 = blockIdx.x * kSmoothTile - s, y0 = blockIdx.y * kSmoothTile - s;
+    const float* I = in + (long long)img * H * W * Cn;
+    for (int i = threadIdx.x; i < E * E * Cn; i += blockDim.x) {
+        const int c = i % Cn, p = i / Cn, xx = x0 + p % E, yy = y0 + p / E;
+        s_in[i] = (xx >= 0 && yy >= 0 && xx < W && yy < H) ? I[((long long)yy * W + xx) * Cn + c] : 0.f;
+    }
+    __syncthreads();
+    const int n = 2 * s + 1;
+    for (int i = threadIdx.x; i < E * kSmoothTile * Cn; i += blockDim.x) {
+        const int c = i % Cn, p = i / Cn, x = p % kSmoothTile, y = p / kSmoothTile;
+        const float* row = s_in + ((size_t)y * E + x) * Cn + c;
+        float acc = 0.f;
+        for (int k = 0; k < n; ++k) acc += taps.w[k] * row[k * Cn];
+        s_h[i] = acc;
+    }
+    __syncthreads();
+    float* O = out + (long long)img * H * W * Cn;
+    for (int i = threadIdx.x; i < kSmoothTile * kSmoothTile * Cn; i += blockDim.x) {
+        const int c = i % Cn, p = i / Cn, x = p % kSmoothTile, y = p / kSmoothTile;
+        const int gx = blockIdx.x * kSmoothTile + x, gy = blockIdx.y * kSmoothTile + y;
+        if (gx >= W || gy >= H) continue;
+        const float* col = s_h + ((size_t)y * kSmoothTile + x) * Cn + c;
+        float acc = 0.f;
+        for (int k = 0; k < n; ++k) acc += taps.w[k] * col[(size_t)k * kSmoothTile * Cn];
+        O[((long long)gy * W + gx) * Cn + c] = acc;
+    }
+}
+
 }  // namespace
 }  // namespace hc
 
 using namespace hc;
+
+extern "C" hc_status hc_gaussian_smooth(void* stream, int32_t n_images, int32_t height, int32_t width,
+                                        int32_t channels, int32_t size, float mean, float std, const float* image,
+                                        float* out) {
+    clear_error();
+    HC_REQUIRE(n_images >= 0 && height > 0 && width > 0 && channels > 0 && channels <= 4, "bad sizes");
+    HC_REQUIRE(size >= 0 && size <= kSmoothMax, "kernel size %d outside [0, %d]", size, kSmoothMax);
+    HC_REQUIRE(image && out, "NULL pointer");
+    HC_REQUIRE(image != out || size == 0 || std == 0.f, "in-place smoothing is not supported");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t bytes = sizeof(float) * (size_t)n_images * height * width * channels;
+    if (size == 0 || std == 0.f) {  // the reference returns the image unchanged
+        if (image != out && bytes) HC_CUDA(cudaMemcpyAsync(out, image, bytes, cudaMemcpyDeviceToDevice, s));
+        return HC_OK;
+    }
+    if (n_images == 0) return HC_OK;
+    // normal density at -size..size, normalised so the 2-D kernel sums to one
+    SmoothTaps t;
+    double v[2 * kSmoothMax + 1], sum = 0.0;
+    for (int k = 0; k <= 2 * size; ++k) {
+        const double z = ((double)(k - size) - mean) / std;
+        v[k] = exp(-0.5 * z * z);
+        sum += v[k];
+    }
+    for (int k = 0; k <= 2 * size; ++k) t.w[k] = (float)(v[k] / sum);
+    const int E = kSmoothTile + 2 * size;
+    const size_t smem = sizeof(float) * ((size_t)E * E + (size_t)E * kSmoothTile) * channels;
+    HC_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid(div_up(width, kSmoothTile), div_up(height, kSmoothTile), n_images);
+    k_smooth<<<grid, 256, smem, s>>>(height, width, channels, size, t, image, out);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_sum_squares_loss(void* stream, int64_t n, const float* x, float weight, void* workspace,
+                                         float* loss, float* grad) {
+    clear_error();
+    HC_REQUIRE(n >= 0, "n < 0");
+    HC_REQUIRE(x && workspace && grad, "NULL input/output pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    double* acc = (double*)workspace;
+    HC_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), s));
+    const int blocks = 148 * 8;
+    k_sumsq_reduce<<<blocks, 256, 0, s>>>(n, x, acc);
+    HC_CHECK_LAUNCH();
+    k_sumsq_grad<<<blocks, 256, 0, s>>>(n, x, weight, acc, grad, loss);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_add_inplace(void* stream, int64_t n, float* dst, const float* src) {
+    clear_error();
+    HC_REQUIRE(n >= 0, "n < 0");
+    HC_REQUIRE(dst && src, "NULL pointer");
+    if (n == 0) return HC_OK;
+    const long long blocks = n / 1024 + 1 < 148 * 8 ? n / 1024 + 1 : 148 * 8;
+    k_add_inplace<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, dst, src);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
 
 extern "C" hc_status hc_image_l1_loss(void* stream, int64_t n_pixels, const float* render_buffer,
                                       const float* target_image, const int32_t* face_buffer,

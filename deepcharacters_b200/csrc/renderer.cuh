@@ -154,6 +154,72 @@ __device__ __forceinline__ float3 project_point(const float* ext, const float* i
     return make_float3(x, y, z);
 }
 
+// Conservative 2-D footprint of a triangle in a view: the three edge lines of
+// its projection, each widened by a margin, as signed pixel distances that
+// are non-negative inside.  A pixel centre outside the widened triangle
+// cannot pass the exact test that follows:
+//  * the ray test: for vertices in front of the camera the projected
+//    triangle is the exact image of the 3-D one, and the float error of
+//    either computation is below 1e-3 px for the coordinate ranges admitted
+//    here (|u|, |v| < 1e5 px, z > 1), against a margin of kEdgeMargin px;
+//  * the image-space barycentric test with its -0.001 tolerance: edge k is
+//    additionally widened by 0.0011 x the triangle's height over that edge,
+//    and by num_err / |edge k| px, num_err bounding the rounding error of
+//    that test's edge-function numerator (2e-6 M^2 for coordinates up to M).
+// Outside that coordinate range, or for a projected area under 1e-2 px^2, the
+// footprint is disabled (every pixel passes).  It only skips work; it never
+// decides a hit.
+constexpr float kEdgeMargin = 0.125f;
+
+struct Footprint {
+    float a[3], b[3], c[3];  // edge k: a*x + b*y + c >= 0 inside (margin included)
+};
+
+__device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, float rel_margin = 0.f,
+                                               float num_err = 0.f) {
+    Footprint fp;
+    const float3 q[3] = {p0, p1, p2};
+    bool ok = p0.z > 1.f && p1.z > 1.f && p2.z > 1.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ok = ok && fabsf(q[k].x) < 1e5f && fabsf(q[k].y) < 1e5f;
+    const float area = (p1.x - p0.x) * (p2.y - p0.y) - (p1.y - p0.y) * (p2.x - p0.x);
+    ok = ok && fabsf(area) >= 1e-2f;
+    const float sg = area > 0.f ? 1.f : -1.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float3 u = q[k], w = q[(k + 1) % 3];
+        const float ex = w.x - u.x, ey = w.y - u.y;
+        const float len = sqrtf(ex * ex + ey * ey);
+        if (!(len > 1e-6f)) ok = false;
+        const float inv = ok ? sg / len : 0.f;
+        const float margin = kEdgeMargin + (ok ? rel_margin * fabsf(area) / len + num_err / len : 0.f);
+        // signed distance of (x, y) from the edge u -> w, positive on the inside
+        fp.a[k] = -ey * inv;
+        fp.b[k] = ex * inv;
+        fp.c[k] = (ey * u.x - ex * u.y) * inv + margin;
+    }
+    if (!ok) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            fp.a[k] = 0.f;
+            fp.b[k] = 0.f;
+            fp.c[k] = 1.f;
+        }
+    }
+    return fp;
+}
+
+// false when no pixel centre of [x0, x1] x [y0, y1] can be inside the footprint
+__device__ __forceinline__ bool footprint_overlaps(const Footprint& fp, int x0, int x1, int y0, int y1) {
+    const float xa = x0 + 0.5f, xb = x1 + 0.5f, ya = y0 + 0.5f, yb = y1 + 0.5f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float m = fp.a[k] * (fp.a[k] > 0.f ? xb : xa) + fp.b[k] * (fp.b[k] > 0.f ? yb : ya) + fp.c[k];
+        if (m < 0.f) return false;
+    }
+    return true;
+}
+
 // Second-order SH shading of an albedo (reference getShading,
 // CudaRenderer/cpp/src/Utils/RendererUtil.h:135-173), one band set per channel.
 __device__ __forceinline__ float sh_channel(const float* s, float3 d, float3 d2) {
@@ -181,6 +247,12 @@ struct Topology {
     DevBuf vf_id;        // int2[N]  (start, count)
     DevBuf texcoords;    // float[6F]
     bool has_texcoords = false;
+};
+
+// texel -> (face, barycentrics) table of the UV-space maps, per texture size
+struct UvTable {
+    int th = 0, tw = 0;
+    DevBuf faces, table;
 };
 
 struct RasterWorkspace {

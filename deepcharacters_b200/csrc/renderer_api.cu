@@ -13,6 +13,9 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
                          int tex_h, int tex_w, const float* sh, const float* extr, const float* intr, float* bary,
                          int* face, float* render, float* vnormal, int* depth_q, int* tie_count);
 hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H);
+hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, int W, int H, int mode,
+                         const float* verts, int tex_h, int tex_w, float* bary, int* face, float* render,
+                         float* vnormal, float* uv_map);
 hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
                           int W, int H, int albedo, int shading, int ifs, int tfs, const float* grad,
                           const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
@@ -102,6 +105,7 @@ struct hc_renderer_s {
     hc::Topology topo;
     hc::RasterWorkspace ws;
     hc::DevBuf nrm_grad;  // backward: gradient w.r.t. unnormalised vertex normals
+    hc::UvTable uv;       // texel table of the UV-space maps
     int C = 0, W = 0, H = 0;
     int albedo = 0, shading = 0, normal_map = hc::kNmNone;
     int image_filter = 2, texture_filter = 2;
@@ -159,7 +163,8 @@ extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, 
 static void release_all(hc_renderer_s* r) {
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
-                      &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad};
+                      &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
+                      &r->uv.faces, &r->uv.table};
     for (DevBuf* b : bufs) b->release();
 }
 
@@ -216,11 +221,10 @@ extern "C" hc_status hc_renderer_forward_ex(hc_renderer h, void* stream, int32_t
     const bool needs_sh = (h->shading == kShaded && h->albedo != kNormal) || h->albedo == kLighting;
     if (needs_sh) HC_REQUIRE(sh_coeff, "shading needs sh_coeff");
     cudaStream_t s = (cudaStream_t)stream;
-    if (h->normal_map != kNmNone) {
-        HC_FAIL(HC_ERR_INVALID, "compute_normal_map='%s' is not supported by this build",
-                h->normal_map == kNmOriginal ? "normal" : h->normal_map == kNmHitPosition ? "position" : "face");
-    }
-    (void)normal_map;
+    if (h->normal_map != kNmNone)
+        return raster_uv_maps(h->topo, h->uv, s, batch, h->C, h->W, h->H, h->normal_map, vertex_pos, texture_height,
+                              texture_width, barycentric_buffer, face_buffer, render_buffer, vertex_normal,
+                              normal_map);
     return raster_forward(h->topo, h->ws, s, batch, h->C, h->W, h->H, h->albedo, h->shading, vertex_pos,
                           vertex_color, texture, texture_height, texture_width, sh_coeff, extrinsics, intrinsics,
                           barycentric_buffer, face_buffer, render_buffer, vertex_normal, depth_q, tie_count);

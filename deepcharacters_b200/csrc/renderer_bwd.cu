@@ -153,16 +153,25 @@ __device__ __forceinline__ bool bary_rows(float3 d, float3 v0, float3 v1, float3
 constexpr int MAXFS = 4;                 // image filter sizes staged in shared memory
 constexpr int TILE_S = BT + 2 * MAXFS;   // staged target tile edge
 
-__global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams,
-                                                     int parity) {
-    __shared__ float s_red[BNT / 32][32][9];
-    __shared__ float s_sh[BNT / 32][27];
-    __shared__ float s_tgt[TILE_S * TILE_S * 3];
+constexpr int MAXTAPS = (2 * MAXFS + 1) * (2 * MAXFS + 1);
+
+// Albedo classes of the adjoint: vertex colours, texture, and the modes
+// whose albedo has no parameters (normal, lighting, mask, position, depth, uv).
+enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2 };
+
+template <bool SHADED, int ALB, bool PARITY>
+__global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams) {
+    constexpr int NV = SHADED ? 9 : 6;  // per-vertex values merged in the warp
+    __shared__ float s_red[BNT / 32][32][NV];
+    __shared__ float s_sh[SHADED ? BNT / 32 : 1][27];
+    __shared__ float4 s_tgt[TILE_S * TILE_S];
+    __shared__ float2 s_tap[MAXTAPS];  // image-gradient tap weights (i, j) / (i^2 + j^2)
+    __shared__ float s_norm;
     const int tile = blockIdx.x, view = blockIdx.y;
     const int b = view / A.C;
-    const bool shaded = A.shading == kShaded;
-    const bool vcol = A.albedo == kVertexColor;
-    const bool textured = A.albedo == kTextured;
+    constexpr bool shaded = SHADED;
+    constexpr bool vcol = ALB == kAlbVcol;
+    constexpr bool textured = ALB == kAlbTex;
     const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
     const int px = tx0 + threadIdx.x % BT;
     const int py = ty0 + threadIdx.x / BT;
@@ -176,13 +185,30 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             const int yy = ty0 - A.ifs + i / e, xx = tx0 - A.ifs + i % e;
             float3 v = make_float3(0.f, 0.f, 0.f);
             if (xx >= 0 && yy >= 0 && xx < A.W && yy < A.H) v = ld3(tgt + 3 * ((long long)yy * A.W + xx));
-            st3(s_tgt + 3 * i, v);
+            s_tgt[i] = make_float4(v.x, v.y, v.z, 0.f);
+        }
+        // tap weights and their normaliser, once per CTA: the same divisions
+        // and the same summation order as evaluating them per pixel
+        const int fs = A.ifs, ew = 2 * fs + 1;
+        if (threadIdx.x < ew * ew) {
+            const int i = (int)threadIdx.x % ew - fs, j = (int)threadIdx.x / ew - fs;
+            const float den = (float)(i * i + j * j);
+            s_tap[threadIdx.x] = den == 0.f ? make_float2(0.f, 0.f) : make_float2((float)i / den, (float)j / den);
+        }
+        if (threadIdx.x == 0) {
+            float norm = 0.f;
+            for (int j = -fs; j <= fs; ++j)
+                for (int i = -fs; i <= fs; ++i) {
+                    const float den = (float)(i * i + j * j);
+                    if (den != 0.f) norm += fabsf((float)i / den);
+                }
+            s_norm = norm;
         }
     }
     __syncthreads();
-    float shg[27];
+    float shg[SHADED ? 27 : 1];
 #pragma unroll
-    for (int k = 0; k < 27; ++k) shg[k] = 0.f;
+    for (int k = 0; k < (SHADED ? 27 : 1); ++k) shg[k] = 0.f;
     const long long pix = ((long long)view * A.H + py) * A.W + px;
     const int f = (px < A.W && py < A.H) ? A.face[pix] : -1;
     int vid[3] = {-1, -1, -1};
@@ -220,16 +246,16 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         const float* sh = A.sh + (long long)view * 27;
         float3 alb = make_float3(0.f, 0.f, 0.f);
         float3 coal = make_float3(1.f, 1.f, 1.f);
-        if (shaded) coal = sh_illum(sh, pn);
+        if constexpr (SHADED) coal = sh_illum(sh, pn);
         gA = G * coal;  // d loss / d albedo
         float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
         const float* tcp = A.texcoords + (long long)f * 6;
-        if (vcol) {
+        if constexpr (vcol) {
             const float* Cc = A.colors + (long long)b * A.N * 3;
             const float3 c0 = ld3(Cc + 3 * id.x), c1 = ld3(Cc + 3 * id.y), c2 = ld3(Cc + 3 * id.z);
             alb = ba * c0 + bb * c1 + bc * c2;
             gbc = make_float3(dot(gA, c0), dot(gA, c1), dot(gA, c2));
-        } else if (textured) {
+        } else if constexpr (textured) {
             const float2 t0 = make_float2(tcp[0], 1.f - tcp[1]);
             const float2 t1 = make_float2(tcp[2], 1.f - tcp[3]);
             const float2 t2 = make_float2(tcp[4], 1.f - tcp[5]);
@@ -261,7 +287,7 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             gbc = make_float3(gu * (t0.x * A.tex_w) + gv * (t0.y * A.tex_h), gu * (t1.x * A.tex_w) + gv * (t1.y * A.tex_h),
                               gu * (t2.x * A.tex_w) + gv * (t2.y * A.tex_h));
         }
-        if (shaded) {
+        if constexpr (SHADED) {
             // SH coefficients: G_r * albedo_r * basis(pn)
             const float basis[9] = {1.f, pn.y, pn.z, pn.x, pn.x * pn.y, pn.z * pn.y, 3.f * pn.z * pn.z - 1.f,
                                     pn.x * pn.z, pn.x * pn.x - pn.y * pn.y};
@@ -293,26 +319,34 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             if (px >= fs + 1 && py >= fs + 1 && px < A.W - (fs + 1) && py < A.H - (fs + 1)) {
                 // taps weighted (x, y)/(x^2 + y^2), normalised by sum |x|/(x^2 + y^2)
                 // (imageGradient, RendererUtil.h:566-620), contracted with G
-                float norm = 0.f;
-                const int e = BT + 2 * fs;
-                for (int j = -fs; j <= fs; ++j)
-                    for (int i = -fs; i <= fs; ++i) {
-                        const float den = (float)(i * i + j * j);
-                        if (den == 0.f) continue;
-                        float3 I;
-                        if (staged) {
-                            const int si = (py - ty0 + fs + j) * e + (px - tx0 + fs + i);
-                            I = make_float3(s_tgt[3 * si], s_tgt[3 * si + 1], s_tgt[3 * si + 2]);
-                        } else {
-                            I = ld3(tgt + 3 * ((long long)(py + j) * A.W + (px + i)));
+                if (staged) {
+                    const int e = BT + 2 * fs, ew = 2 * fs + 1;
+                    const int s0 = (py - ty0) * e + (px - tx0);
+                    for (int j = 0; j < ew; ++j)
+                        for (int i = 0; i < ew; ++i) {
+                            const float2 w = s_tap[j * ew + i];
+                            const float4 I = s_tgt[s0 + j * e + i];
+                            const float gi = G.x * I.x + G.y * I.y + G.z * I.z;
+                            gu += gi * w.x;
+                            gv += gi * w.y;
                         }
-                        const float gi = dot(G, I);
-                        gu += gi * ((float)i / den);
-                        gv += gi * ((float)j / den);
-                        norm += fabsf((float)i / den);
-                    }
-                gu /= norm;
-                gv /= norm;
+                    gu /= s_norm;
+                    gv /= s_norm;
+                } else {
+                    float norm = 0.f;
+                    for (int j = -fs; j <= fs; ++j)
+                        for (int i = -fs; i <= fs; ++i) {
+                            const float den = (float)(i * i + j * j);
+                            if (den == 0.f) continue;
+                            const float3 I = ld3(tgt + 3 * ((long long)(py + j) * A.W + (px + i)));
+                            const float gi = dot(G, I);
+                            gu += gi * ((float)i / den);
+                            gv += gi * ((float)j / den);
+                            norm += fabsf((float)i / den);
+                        }
+                    gu /= norm;
+                    gv /= norm;
+                }
             }
             if (gu != 0.f || gv != 0.f) {
                 const float* e = cam.ext;
@@ -339,7 +373,7 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             }
         }
         // data -> model through the barycentric Jacobian
-        if (parity) {
+        if constexpr (PARITY) {
             const float3 o = make_float3(cam.ro[0], cam.ro[1], cam.ro[2]);
             float ja[9], jb[9];
             bary_jacobian(o, d, v0, v1, v2, ja, jb);
@@ -375,40 +409,42 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         row[3] = gA.x * bw[i];
         row[4] = gA.y * bw[i];
         row[5] = gA.z * bw[i];
-        row[6] = gnu.x * bw[i];
-        row[7] = gnu.y * bw[i];
-        row[8] = gnu.z * bw[i];
+        if constexpr (SHADED) {
+            row[6] = gnu.x * bw[i];
+            row[7] = gnu.y * bw[i];
+            row[8] = gnu.z * bw[i];
+        }
         __syncwarp();
         const int key = vid[i];
         const unsigned grp = __match_any_sync(0xffffffffu, key);
         if (key >= 0 && lane == __ffs(grp) - 1) {
-            float acc[9];
+            float acc[NV];
 #pragma unroll
-            for (int k = 0; k < 9; ++k) acc[k] = 0.f;
+            for (int k = 0; k < NV; ++k) acc[k] = 0.f;
             for (unsigned mm = grp; mm; mm &= mm - 1) {
                 const float* r = s_red[warp][__ffs(mm) - 1];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) acc[k] += r[k];
+                for (int k = 0; k < NV; ++k) acc[k] += r[k];
             }
             const long long o3 = ((long long)b * A.N + key) * 3;
             atomicAdd(A.vpos_grad + o3 + 0, acc[0]);
             atomicAdd(A.vpos_grad + o3 + 1, acc[1]);
             atomicAdd(A.vpos_grad + o3 + 2, acc[2]);
-            if (vcol) {
+            if constexpr (vcol) {
                 atomicAdd(A.vcol_grad + o3 + 0, acc[3]);
                 atomicAdd(A.vcol_grad + o3 + 1, acc[4]);
                 atomicAdd(A.vcol_grad + o3 + 2, acc[5]);
             }
-            if (shaded) {
-                atomicAdd(A.nrm_grad + o3 + 0, acc[6]);
-                atomicAdd(A.nrm_grad + o3 + 1, acc[7]);
-                atomicAdd(A.nrm_grad + o3 + 2, acc[8]);
+            if constexpr (SHADED) {
+                atomicAdd(A.nrm_grad + o3 + 0, acc[NV - 3]);
+                atomicAdd(A.nrm_grad + o3 + 1, acc[NV - 2]);
+                atomicAdd(A.nrm_grad + o3 + 2, acc[NV - 1]);
             }
         }
         __syncwarp();
     }
     // SH: reduce over the CTA, one atomic per coefficient
-    if (shaded) {
+    if constexpr (SHADED) {
 #pragma unroll
         for (int k = 0; k < 27; ++k) {
             float v = shg[k];
@@ -504,7 +540,26 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.sh_grad = sh_grad;
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
     const int tiles_x = div_up(W, BT), tiles_y = div_up(H, BT);
-    k_render_grad<<<dim3(tiles_x * tiles_y, V), BNT, 0, s>>>(A, tiles_x, cams, parity);
+    const dim3 grid(tiles_x * tiles_y, V);
+    const int alb = albedo == kVertexColor ? kAlbVcol : albedo == kTextured ? kAlbTex : kAlbNone;
+    const int sel = (shaded ? 6 : 0) + alb * 2 + (parity ? 1 : 0);
+    switch (sel) {
+#define HC_GRAD_CASE(SH, AL, PA) \
+    case (SH ? 6 : 0) + AL * 2 + PA: k_render_grad<SH, AL, PA><<<grid, BNT, 0, s>>>(A, tiles_x, cams); break;
+        HC_GRAD_CASE(false, kAlbVcol, false)
+        HC_GRAD_CASE(false, kAlbVcol, true)
+        HC_GRAD_CASE(false, kAlbTex, false)
+        HC_GRAD_CASE(false, kAlbTex, true)
+        HC_GRAD_CASE(false, kAlbNone, false)
+        HC_GRAD_CASE(false, kAlbNone, true)
+        HC_GRAD_CASE(true, kAlbVcol, false)
+        HC_GRAD_CASE(true, kAlbVcol, true)
+        HC_GRAD_CASE(true, kAlbTex, false)
+        HC_GRAD_CASE(true, kAlbTex, true)
+        HC_GRAD_CASE(true, kAlbNone, false)
+        HC_GRAD_CASE(true, kAlbNone, true)
+#undef HC_GRAD_CASE
+    }
     HC_CHECK_LAUNCH();
     if (shaded) {
         k_normal_chain<<<div_up((long long)B * N, 256), 256, 0, s>>>(B, N, topo.faces.as<int3>(), topo.vf.as<int>(),

@@ -134,6 +134,46 @@ __global__ void k_tri_frame(int B, int F, int N, const int3* __restrict__ faces,
 // counter (match + ballot + popc); entries beyond the tile's capacity go to
 // the spill list.
 // ---------------------------------------------------------------------------
+constexpr int kBinSmall = 4;  // tiles a thread bins on its own
+
+// Where a (tile, triangle) pair goes once it has a slot in the tile's bin:
+// the bin itself, or beyond the bin's capacity the spill list (the first
+// overflowing pair of a tile claims and clears the tile's spill key block).
+struct BinSink {
+    int TS, cap;
+    int2* tile_state;
+    int* bins;
+    int4* spill;
+    long long spill_cap;
+    unsigned long long* spill_keys;
+    int spill_tile_cap;
+    RasterStats* stats;
+
+    __device__ __forceinline__ int place(int slot, long long key, int view, int T, int f) const {
+        if (slot < cap) {
+            bins[key * cap + slot] = f;
+            return 1;
+        }
+        if (slot == cap) {
+            const int ks = atomicAdd(&stats->spill_tiles, 1);
+            if (ks < spill_tile_cap) {
+                unsigned long long* kp = spill_keys + (long long)ks * TS * TS;
+                for (int p = 0; p < TS * TS; ++p) kp[p] = ~0ull;
+                tile_state[key].y = ks + 1;
+            } else {
+                atomicOr(&stats->overflow, 2);
+            }
+        }
+        const unsigned long long si = atomicAdd(&stats->spilled, 1ull);
+        if ((long long)si < spill_cap) {
+            spill[si] = make_int4(view, (int)(key - (long long)view * T), f, 0);
+        } else {
+            atomicOr(&stats->overflow, 1);
+        }
+        return 0;
+    }
+};
+
 __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tiles_x, int tiles_y, int cap,
                       const int3* __restrict__ faces, const float* __restrict__ verts,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
@@ -144,6 +184,7 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
     const bool live = i < (long long)V * F;
     int view = 0, f = 0;
     int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
+    Footprint fp;
     if (live) {
         view = (int)(i / F);
         f = (int)(i % F);
@@ -174,6 +215,7 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         // front-facing: the plane normal points towards the camera (num < 0)
         tv.dqmin = depth_lower_bound(tv.num, T.n, T, ro_s) | (tv.num < 0.f ? 0 : (int)0x80000000);
         tri_view[i] = tv;
+        fp = footprint(p0, p1, p2);
     }
     const bool nonempty = live && x1 >= x0 && y1 >= y0;
     int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
@@ -186,19 +228,26 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
     const int T = tiles_x * tiles_y;
     const int ntx = tx1 - tx0 + 1;
     const int nt = nonempty ? ntx * (ty1 - ty0 + 1) : 0;
-    // lanes walk their tile lists in lock step; same-tile lanes aggregate
-    int maxnt = nt;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
+    const bool big = nt > kBinSmall;
+    BinSink sink{TS, cap, tile_state, bins, spill, spill_cap, spill_keys, spill_tile_cap, stats};
     unsigned long long nbinned = 0;
     const unsigned lane = threadIdx.x & 31;
+    // boxes of up to kBinSmall tiles: lanes walk their tile lists in lock
+    // step and lanes that hit the same tile share one counter atomic
+    const int my_nt = big ? 0 : nt;
+    int maxnt = my_nt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
     for (int k = 0; k < maxnt; ++k) {
-        const bool act = k < nt;
+        bool act = k < my_nt;
         long long key = -1;
         if (act) {
             const int tx = tx0 + k % ntx;
             const int ty = ty0 + k / ntx;
-            key = (long long)view * T + ty * tiles_x + tx;
+            // tiles of the box that the triangle's footprint misses get no entry
+            act = nt == 1 || footprint_overlaps(fp, max(tx * TS, x0), min(tx * TS + TS - 1, x1), max(ty * TS, y0),
+                                                min(ty * TS + TS - 1, y1));
+            if (act) key = (long long)view * T + ty * tiles_x + tx;
         }
         const unsigned same = __match_any_sync(0xffffffffu, key);
         if (!act) continue;
@@ -207,29 +256,33 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         int base = 0;
         if ((int)lane == leader) base = atomicAdd(&tile_state[key].x, __popc(same));
         base = __shfl_sync(same, base, leader);
-        const int slot = base + rank;
-        if (slot < cap) {
-            bins[key * cap + slot] = f;
-            ++nbinned;
-        } else {
-            if (slot == cap) {
-                // first overflow of this tile: claim a spill key block and clear it
-                const int ks = atomicAdd(&stats->spill_tiles, 1);
-                if (ks < spill_tile_cap) {
-                    unsigned long long* kp = spill_keys + (long long)ks * TS * TS;
-                    for (int p = 0; p < TS * TS; ++p) kp[p] = ~0ull;
-                    tile_state[key].y = ks + 1;
-                } else {
-                    atomicOr(&stats->overflow, 2);
-                }
-            }
-            const unsigned long long si = atomicAdd(&stats->spilled, 1ull);
-            if ((long long)si < spill_cap) {
-                const int tile = (int)(key - (long long)view * T);
-                spill[si] = make_int4(view, tile, f, 0);
-            } else {
-                atomicOr(&stats->overflow, 1);
-            }
+        nbinned += sink.place(base + rank, key, view, T, f);
+    }
+    // larger boxes: the warp takes them one at a time, a tile per lane
+    unsigned pending = __ballot_sync(0xffffffffu, big);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
+        const int qx0 = __shfl_sync(0xffffffffu, x0, src), qx1 = __shfl_sync(0xffffffffu, x1, src);
+        const int qy0 = __shfl_sync(0xffffffffu, y0, src), qy1 = __shfl_sync(0xffffffffu, y1, src);
+        Footprint qfp;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            qfp.a[e] = __shfl_sync(0xffffffffu, fp.a[e], src);
+            qfp.b[e] = __shfl_sync(0xffffffffu, fp.b[e], src);
+            qfp.c[e] = __shfl_sync(0xffffffffu, fp.c[e], src);
+        }
+        const int qtx0 = qx0 / TS, qty0 = qy0 / TS, qntx = qx1 / TS - qtx0 + 1;
+        const int qnt = qntx * (qy1 / TS - qty0 + 1);
+        for (int k = lane; k < qnt; k += 32) {
+            const int tx = qtx0 + k % qntx;
+            const int ty = qty0 + k / qntx;
+            if (!footprint_overlaps(qfp, max(tx * TS, qx0), min(tx * TS + TS - 1, qx1), max(ty * TS, qy0),
+                                    min(ty * TS + TS - 1, qy1)))
+                continue;
+            const long long key = (long long)qv * T + ty * tiles_x + tx;
+            nbinned += sink.place(atomicAdd(&tile_state[key].x, 1), key, qv, T, qf);
         }
     }
     // one counter update per warp
@@ -393,13 +446,45 @@ __device__ __forceinline__ float3 shade_pixel(const ShadeArgs& A, const ViewCam&
 }
 
 struct TileTri {
-    int4 hdr;        // x01, y01, dqmin (depth lower bound | back-facing bit 31), face id
+    int4 hdr;        // column mask, row mask (tile-relative bbox), depth lower bound, face id
+    float4 ea;       // footprint edges 0, 1: (a0, b0, a1, b1)
+    float4 nm;       // ray-plane numerator, footprint offsets c0, c1, c2
+    float4 eb;       // footprint edge 2: (a2, b2, -, -)
     float4 a, b, c;  // TriFrame
-    float4 nm;       // ray-plane numerator
 };
 
+// Hit test with an early depth rejection: the quantised depth int(t * 1e4) is
+// known as soon as t is, so a triangle that cannot reach the pixel's current
+// best depth skips the edge tests.  Accepted hits and their depth / barycentrics
+// are those of raster_hit.
+__device__ __forceinline__ bool raster_hit_below(float3 ro_s, float3 dir, const TriS& T, float num,
+                                                 unsigned best_d, int& depth_q, float& a, float& b) {
+    const float ndr = dot(dir, T.n);
+    if (fabsf(ndr) < 0.0000001f) return false;
+    const float t = num / ndr;
+    if (t < 0.f) return false;
+    depth_q = (int)(t * 10000.f);
+    if ((unsigned)depth_q > best_d) return false;
+    const float3 P = ro_s + t * dir;
+    float3 C = cross(T.s1 - T.s0, P - T.s0);
+    if (dot(T.n, C) < 0.f) return false;
+    C = cross(T.s2 - T.s1, P - T.s1);
+    if ((a = dot(T.n, C)) < 0.f) return false;
+    C = cross(T.s0 - T.s2, P - T.s2);
+    if ((b = dot(T.n, C)) < 0.f) return false;
+    const float denom = dot(T.n, T.n);
+    a /= denom;
+    b /= denom;
+    return (a >= -0.001f) && (b >= -0.001f) && (a <= 1.001f) && (b <= 1.001f);
+}
+
+// bits lo..hi of a 32-bit mask (empty when hi < lo)
+__device__ __forceinline__ unsigned bit_range(int lo, int hi) {
+    return hi < lo ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
+}
+
 template <int TS>
-__global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : 1) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
                                                    const TriView* __restrict__ tri_view,
@@ -410,12 +495,15 @@ __global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, in
     constexpr int NT = TS * TS;
     constexpr int CHUNK = NT > 256 ? 256 : NT;  // triangles staged per round
     __shared__ TileTri s_tri[CHUNK];
+    __shared__ int s_count[2];
     const int tile = blockIdx.x;
     const int view = blockIdx.y;
     const int b = view / A.C;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int lx = threadIdx.x % TS, ly = threadIdx.x / TS;
     const int px = tx * TS + lx, py = ty * TS + ly;
+    const unsigned col_bit = 1u << lx, row_bit = 1u << ly;
+    const float cx = px + 0.5f, cy = py + 0.5f;
     const bool valid = px < A.W && py < A.H;
     const ViewCam& cam = cams[view];
     const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
@@ -426,51 +514,76 @@ __global__ void __launch_bounds__(TS* TS) k_resolve(ShadeArgs A, int tiles_x, in
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
-    // Two passes over the tile's triangles: front-facing first, then
-    // back-facing.  A triangle whose depth lower bound exceeds the pixel's
-    // current best depth can neither win nor tie, so once the front surface
-    // is resolved most back faces are rejected without a ray test.  The
-    // result is the same minimum (depth, id) as one unordered pass.
+    // Each staged chunk is split into its front-facing triangles (from the
+    // start) and back-facing ones (from the end).  All front faces are tested
+    // first, then the back faces: a triangle whose depth lower bound exceeds
+    // the pixel's current best depth can neither win nor tie, so once the
+    // front surface is resolved most back faces are rejected by one compare.
+    // The result is the same minimum (depth, id) as one unordered pass.
+    // Per pixel a triangle is only tested when the pixel lies in the
+    // triangle's bounding box, kept as a column and a row bit mask relative
+    // to the tile.
+    int n_front = 0;
     for (int pass = 0; pass < 2; ++pass) {
         for (int base = 0; base < n; base += CHUNK) {
+            const int m = min(CHUNK, n - base);
             if (pass == 0 || n > CHUNK) {
-                const int k = base + threadIdx.x;
                 __syncthreads();
-                if (threadIdx.x < CHUNK && k < n) {
+                if (threadIdx.x < 2) s_count[threadIdx.x] = 0;
+                __syncthreads();
+                const int k = base + threadIdx.x;
+                if (threadIdx.x < CHUNK && k < m + base) {
                     const int f = tb[k];
-                    const TriFrame tf = tri_frame[(long long)b * A.F + f];
                     const TriView tv = tri_view[(long long)view * A.F + f];
+                    const bool back = tv.dqmin < 0;
+                    const int slot = back ? m - 1 - atomicAdd(&s_count[1], 1) : atomicAdd(&s_count[0], 1);
+                    const TriFrame tf = tri_frame[(long long)b * A.F + f];
+                    const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
+                    const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
+                    const float3 q0 = project_point(cam.ext, cam.intr, make_float3(tf.a.x, tf.a.y, tf.a.z) * 1000.f);
+                    const float3 q1 = project_point(cam.ext, cam.intr, make_float3(tf.b.x, tf.b.y, tf.b.z) * 1000.f);
+                    const float3 q2 = project_point(cam.ext, cam.intr, make_float3(tf.c.x, tf.c.y, tf.c.z) * 1000.f);
+                    const Footprint fp = footprint(q0, q1, q2);
                     TileTri t;
-                    t.hdr = make_int4(tv.x01, tv.y01, tv.dqmin, f);
+                    t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
+                                      (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
+                                      tv.dqmin & 0x7fffffff, f);
+                    t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
+                    t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
+                    t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
                     t.a = tf.a;
                     t.b = tf.b;
                     t.c = tf.c;
-                    t.nm = make_float4(tv.num, 0.f, 0.f, 0.f);
-                    s_tri[threadIdx.x] = t;
+                    s_tri[slot] = t;
                 }
                 __syncthreads();
+                n_front = s_count[0];
             }
-            const int m = min(CHUNK, n - base);
+            const int j0 = pass == 0 ? 0 : n_front;
+            const int j1 = pass == 0 ? n_front : m;
             if (valid) {
-                for (int j = 0; j < m; ++j) {
+                for (int j = j0; j < j1; ++j) {
                     // one 16-byte header load decides whether the ray test runs
                     const int4 h = s_tri[j].hdr;
-                    if ((h.z < 0) != (pass == 1)) continue;             // wrong facing for this pass
-                    if ((unsigned)(h.z & 0x7fffffff) > best_d) continue;  // cannot reach the best depth
-                    if (px < (h.x & 0xffff) || px > (h.x >> 16) || py < (h.y & 0xffff) || py > (h.y >> 16)) continue;
+                    if (!((unsigned)h.x & col_bit) || !((unsigned)h.y & row_bit)) continue;
+                    if ((unsigned)h.z > best_d) continue;  // cannot reach the best depth
+                    const float4 ea = s_tri[j].ea, nm = s_tri[j].nm, eb = s_tri[j].eb;
+                    if (ea.x * cx + ea.y * cy + nm.y < 0.f || ea.z * cx + ea.w * cy + nm.z < 0.f ||
+                        eb.x * cx + eb.y * cy + nm.w < 0.f)
+                        continue;  // pixel centre clearly outside the projected triangle
                     TriFrame tf;
                     tf.a = s_tri[j].a;
                     tf.b = s_tri[j].b;
                     tf.c = s_tri[j].c;
                     int dq;
                     float a, bb;
-                    if (!raster_hit(ro_s, dir, tri_from(tf), s_tri[j].nm.x, dq, a, bb)) continue;
+                    if (!raster_hit_below(ro_s, dir, tri_from(tf), nm.x, best_d, dq, a, bb)) continue;
                     const int f = h.w;
                     if ((unsigned)dq < best_d) {
                         best_d = (unsigned)dq;
                         best_f = f;
                         ties = 1;
-                    } else if ((unsigned)dq == best_d) {
+                    } else {  // equal depth (deeper hits were rejected)
                         best_f = min(best_f, f);
                         ++ties;
                     }

@@ -19,6 +19,7 @@
 
 #include "hc_common.cuh"
 #include "hc_math.cuh"
+#include "renderer.cuh"
 
 namespace hc {
 namespace {
@@ -126,6 +127,159 @@ __global__ void k_boundary(int B, int C, int N, int W, int H, const float* __res
         for (int c = u - 1; c <= u + 1; ++c)
             for (int rr = v - 1; rr <= v + 1; ++rr)
                 if (F[(long long)rr * W + c] < 0) r = 1;
+    }
+    out[i] = r;
+}
+
+// 2-D coverage of the projected mesh, the ProjectedMeshBoundaryGpu op's own
+// raster (Skeletool/Mesh/CUDABasedRasterization.cu:80-145): every pixel of a
+// triangle's clamped bounding box whose centre has image-space barycentrics
+// within [-0.001, 1.001] is marked covered.  The barycentric expressions keep
+// the reference's operation order, so coverage is bit-identical; only
+// "covered" is ever written, so the unordered stores need no atomics.
+//
+// Deformed meshes mix long thin triangles whose boxes span 10^4 pixels with
+// triangles of a few pixels, and the reference's one-thread-per-triangle loop
+// leaves most lanes idle.  Here each thread takes a (view, triangle); boxes of
+// up to kCoverSmall pixels are swept by their own thread, larger ones are
+// queued in the warp (ballot) and swept by the whole warp, one row per lane.
+// A row only visits the pixels between the edges of the triangle's
+// conservative footprint (widened by the -0.001 tolerance and the test's
+// rounding error, see Footprint), so a thin triangle costs its area, not its
+// box.  Skipped pixels cannot pass the exact test.
+constexpr int kCoverSmall = 64;
+
+struct CoverTri {
+    float2 a, b, c;
+    float d1, d2;
+    int x0, x1, y0, y1;
+};
+
+__device__ __forceinline__ bool cover_test(const CoverTri& t, float pu, float pv) {
+    const float2 a = t.a, b = t.b, c = t.c;
+    const float e2 = ((a.y - b.y) * pu + (b.x - a.x) * pv + a.x * b.y - b.x * a.y) / t.d2;
+    const float e1 = ((a.y - c.y) * pu + (c.x - a.x) * pv + a.x * c.y - c.x * a.y) / t.d1;
+    const float e0 = 1.f - e2 - e1;
+    return e0 >= -0.001f && e1 >= -0.001f && e2 >= -0.001f && e0 <= 1.001f && e1 <= 1.001f && e2 <= 1.001f;
+}
+
+__device__ __forceinline__ bool fp_inside(const Footprint& fp, float pu, float pv) {
+    return fp.a[0] * pu + fp.b[0] * pv + fp.c[0] >= 0.f && fp.a[1] * pu + fp.b[1] * pv + fp.c[1] >= 0.f &&
+           fp.a[2] * pu + fp.b[2] * pv + fp.c[2] >= 0.f;
+}
+
+// pixel columns of row v whose centres can be inside the footprint
+__device__ __forceinline__ void fp_span(const Footprint& fp, float pv, int x0, int x1, int& u0, int& u1) {
+    float lo = x0 + 0.5f, hi = x1 + 0.5f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float r = fp.b[k] * pv + fp.c[k];  // need a x + r >= 0
+        if (fabsf(fp.a[k]) < 1e-12f) {
+            if (r < 0.f) hi = -1e30f;
+        } else if (fp.a[k] > 0.f) {
+            lo = fmaxf(lo, -r / fp.a[k]);
+        } else {
+            hi = fminf(hi, -r / fp.a[k]);
+        }
+    }
+    if (!(lo <= hi)) {
+        u0 = 1;
+        u1 = 0;
+        return;
+    }
+    // one extra column on each side absorbs the rounding of the bounds
+    u0 = max(x0, (int)floorf(lo - 0.5f) - 1);
+    u1 = min(x1, (int)ceilf(hi - 0.5f) + 1);
+}
+
+__device__ __forceinline__ Footprint cover_footprint(const CoverTri& t, int W, int H) {
+    const float M = fmaxf(fmaxf(fmaxf(fabsf(t.a.x), fabsf(t.a.y)), fmaxf(fabsf(t.b.x), fabsf(t.b.y))),
+                          fmaxf(fmaxf(fabsf(t.c.x), fabsf(t.c.y)), (float)max(W, H)));
+    return footprint(make_float3(t.a.x, t.a.y, 2.f), make_float3(t.b.x, t.b.y, 2.f), make_float3(t.c.x, t.c.y, 2.f),
+                     0.0011f, 2e-6f * M * M);
+}
+
+__global__ void k_cover(int B, int C, int N, int F, int W, int H, const int* __restrict__ faces,
+                        const float2* __restrict__ p2d, unsigned char* __restrict__ cover) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool live = i < (long long)B * C * F;
+    long long view = 0;
+    CoverTri t;
+    t.x0 = 0;
+    t.x1 = -1;
+    t.y0 = 0;
+    t.y1 = -1;
+    if (live) {
+        view = i / F;
+        const int f = (int)(i % F);
+        const float2* P = p2d + view * N;
+        t.a = P[faces[3 * f]];
+        t.b = P[faces[3 * f + 1]];
+        t.c = P[faces[3 * f + 2]];
+        const float2 a = t.a, b = t.b, c = t.c;
+        t.x0 = (int)fmaxf(fminf(a.x, fminf(b.x, c.x)) - 0.5f, 0);
+        t.y0 = (int)fmaxf(fminf(a.y, fminf(b.y, c.y)) - 0.5f, 0);
+        t.x1 = (int)fminf(fmaxf(a.x, fmaxf(b.x, c.x)) + 0.5f, W - 1);
+        t.y1 = (int)fminf(fmaxf(a.y, fmaxf(b.y, c.y)) + 0.5f, H - 1);
+        t.d2 = (a.y - b.y) * c.x + (b.x - a.x) * c.y + a.x * b.y - b.x * a.y;
+        t.d1 = (a.y - c.y) * b.x + (c.x - a.x) * b.y + a.x * c.y - c.x * a.y;
+    }
+    const bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
+    const long long box = nonempty ? (long long)(t.x1 - t.x0 + 1) * (t.y1 - t.y0 + 1) : 0;
+    const bool big = box > kCoverSmall;
+    if (nonempty && !big) {
+        const Footprint fp = cover_footprint(t, W, H);
+        unsigned char* img = cover + view * H * W;
+        for (int v = t.y0; v <= t.y1; ++v) {
+            const float pv = v + 0.5f;
+            for (int u = t.x0; u <= t.x1; ++u) {
+                const float pu = u + 0.5f;
+                if (fp_inside(fp, pu, pv) && cover_test(t, pu, pv)) img[(long long)v * W + u] = 1;
+            }
+        }
+    }
+    // large boxes: the warp sweeps them one at a time, a row per lane
+    unsigned pending = __ballot_sync(0xffffffffu, big);
+    while (pending) {
+        const int src = __ffs(pending) - 1;
+        pending &= pending - 1;
+        CoverTri q;
+        q.a = make_float2(__shfl_sync(0xffffffffu, t.a.x, src), __shfl_sync(0xffffffffu, t.a.y, src));
+        q.b = make_float2(__shfl_sync(0xffffffffu, t.b.x, src), __shfl_sync(0xffffffffu, t.b.y, src));
+        q.c = make_float2(__shfl_sync(0xffffffffu, t.c.x, src), __shfl_sync(0xffffffffu, t.c.y, src));
+        q.d1 = __shfl_sync(0xffffffffu, t.d1, src);
+        q.d2 = __shfl_sync(0xffffffffu, t.d2, src);
+        q.x0 = __shfl_sync(0xffffffffu, t.x0, src);
+        q.x1 = __shfl_sync(0xffffffffu, t.x1, src);
+        q.y0 = __shfl_sync(0xffffffffu, t.y0, src);
+        q.y1 = __shfl_sync(0xffffffffu, t.y1, src);
+        const long long qv = __shfl_sync(0xffffffffu, view, src);
+        const Footprint fp = cover_footprint(q, W, H);
+        unsigned char* img = cover + qv * H * W;
+        for (int v = q.y0 + lane; v <= q.y1; v += 32) {
+            const float pv = v + 0.5f;
+            int u0, u1;
+            fp_span(fp, pv, q.x0, q.x1, u0, u1);
+            for (int u = u0; u <= u1; ++u)
+                if (cover_test(q, u + 0.5f, pv)) img[(long long)v * W + u] = 1;
+        }
+    }
+}
+
+// boundary test of k_boundary against the coverage image instead of a face buffer
+__global__ void k_boundary_cover(int B, int C, int N, int W, int H, const float* __restrict__ p2d,
+                                 const unsigned char* __restrict__ cover, unsigned char* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * C * N) return;
+    const long long view = i / N;
+    const int u = (int)p2d[2 * i], v = (int)p2d[2 * i + 1];
+    unsigned char r = 0;
+    if (u - 1 >= 0 && u + 1 < W && v - 1 >= 0 && v + 1 < H) {
+        const unsigned char* img = cover + view * H * W;
+        for (int c = u - 1; c <= u + 1; ++c)
+            for (int rr = v - 1; rr <= v + 1; ++rr)
+                if (!img[(long long)rr * W + c]) r = 1;
     }
     out[i] = r;
 }
@@ -382,6 +536,79 @@ extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int
     if (n == 0) return HC_OK;
     k_boundary<<<div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(batch, n_cameras, n_points, width, height,
                                                                  points_image_space, face_buffer, is_boundary);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+struct hc_mesh_boundary_s {
+    int F = 0, N = 0;
+    DevBuf faces, p2d, cover;
+};
+
+extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
+                                             int32_t n_vertices) {
+    clear_error();
+    HC_REQUIRE(out && faces && n_faces > 0 && n_vertices > 0, "bad arguments");
+    for (long long k = 0; k < 3LL * n_faces; ++k)
+        HC_REQUIRE(faces[k] >= 0 && faces[k] < n_vertices, "face index %d out of range at %lld", faces[k], k);
+    auto* h = new hc_mesh_boundary_s();
+    h->F = n_faces;
+    h->N = n_vertices;
+    hc_status st = upload(h->faces, faces, 3 * (size_t)n_faces);
+    if (st != HC_OK) {
+        delete h;
+        return st;
+    }
+    *out = h;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
+    clear_error();
+    if (!h) return HC_OK;
+    h->faces.release();
+    h->p2d.release();
+    h->cover.release();
+    delete h;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch, int32_t n_cameras, int32_t width,
+                                              int32_t height) {
+    clear_error();
+    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 0 && height > 0, "bad sizes");
+    const size_t views = (size_t)batch * n_cameras;
+    HC_TRY(h->p2d.ensure(sizeof(float) * 2 * views * h->N));
+    HC_TRY(h->cover.ensure(views * (size_t)width * height));
+    return HC_OK;
+}
+
+extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                              int32_t width, int32_t height, const float* points_global_space,
+                                              const float* extrinsics, const float* intrinsics,
+                                              const float* points_image_space, uint8_t* is_boundary) {
+    clear_error();
+    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 2 && height > 2, "bad sizes");
+    HC_REQUIRE(is_boundary && (points_image_space || (points_global_space && extrinsics && intrinsics)),
+               "NULL pointer");
+    HC_TRY(hc_mesh_boundary_reserve(h, batch, n_cameras, width, height));
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long nv = (long long)batch * n_cameras * h->N;
+    const float* p2d = points_image_space;
+    if (!p2d) {
+        k_project<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, points_global_space, nullptr, extrinsics,
+                                                  intrinsics, 1, h->p2d.as<float>());
+        HC_CHECK_LAUNCH();
+        p2d = h->p2d.as<float>();
+    }
+    const long long views = (long long)batch * n_cameras;
+    HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
+    const long long nt = views * h->F;
+    k_cover<<<div_up(nt, 256), 256, 0, s>>>(batch, n_cameras, h->N, h->F, width, height, h->faces.as<int>(),
+                                            reinterpret_cast<const float2*>(p2d), h->cover.as<unsigned char>());
+    HC_CHECK_LAUNCH();
+    k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
+                                                     h->cover.as<unsigned char>(), is_boundary);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }

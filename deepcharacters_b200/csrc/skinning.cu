@@ -104,20 +104,27 @@ struct Skel {
     const float* base_n;   // [N,3]
 };
 
-// Forward kinematics, one thread per frame.  Writes joint transforms [B,J],
-// global joint positions / axes [B,J,3] and skinning transforms [B,S].
+// Forward kinematics, one CTA per frame: the joint parameters and every
+// joint's local transform are formed in parallel in shared memory, one thread
+// composes the chain (parents precede children), and the outputs -- joint
+// transforms [B,J], global joint positions / axes [B,J,3], skinning
+// transforms [B,S] -- are written in parallel.
 __global__ void k_fk(Skel sk, int B, const float* __restrict__ dofs, Xf* __restrict__ joints, float* __restrict__ gpos,
                      float* __restrict__ gaxis, Xf* __restrict__ skin_xf, float* __restrict__ params) {
-    const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= B) return;
-    float* P = params + (long long)b * sk.J;
-    for (int j = 0; j < sk.J; ++j) P[j] = 0.f;
-    for (int d = 0; d < sk.D; ++d) {  // DOF -> joint parameters (dof.cpp:9-17)
-        const float v = dofs[(long long)b * sk.D + d];
-        for (int e = sk.dof_off[d]; e < sk.dof_off[d + 1]; ++e) P[sk.dof_joint[e]] += sk.dof_w[e] * v;
+    extern __shared__ float fk_sm[];
+    const int b = blockIdx.x;
+    float* P = fk_sm;                                        // [J]
+    Xf* Lx = reinterpret_cast<Xf*>(fk_sm + ((sk.J + 3) & ~3));  // [J] local transforms
+    Xf* T = Lx + sk.J;                                       // [J] global transforms
+    if (threadIdx.x == 0) {  // DOF -> joint parameters (dof.cpp:9-17), in dof order
+        for (int j = 0; j < sk.J; ++j) P[j] = 0.f;
+        for (int d = 0; d < sk.D; ++d) {
+            const float v = dofs[(long long)b * sk.D + d];
+            for (int e = sk.dof_off[d]; e < sk.dof_off[d + 1]; ++e) P[sk.dof_joint[e]] += sk.dof_w[e] * v;
+        }
     }
-    Xf* T = joints + (long long)b * sk.J;
-    for (int j = 0; j < sk.J; ++j) {
+    __syncthreads();
+    for (int j = threadIdx.x; j < sk.J; j += blockDim.x) {
         Xf local;
         const float s = sk.jscale[j];
         const float* ax = sk.axis + 3 * j;
@@ -128,19 +135,32 @@ __global__ void k_fk(Skel sk, int B, const float* __restrict__ dofs, Xf* __restr
             for (int c = 0; c < 9; ++c) local.r[c] = (c % 4 == 0) ? 1.f : 0.f;
             for (int c = 0; c < 3; ++c) local.t[c] = sk.offset[3 * j + c] * s + ax[c] * P[j];
         }
-        const int p = sk.parent[j];
-        if (p >= 0) xf_mul(T[p], local, T[j]);
-        else T[j] = local;
+        Lx[j] = local;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int j = 0; j < sk.J; ++j) {
+            const int p = sk.parent[j];
+            if (p >= 0) xf_mul(T[p], Lx[j], T[j]);
+            else T[j] = Lx[j];
+        }
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < sk.J; j += blockDim.x) {
+        const Xf X = T[j];
+        joints[(long long)b * sk.J + j] = X;
+        params[(long long)b * sk.J + j] = P[j];
+        const float* ax = sk.axis + 3 * j;
         float* gp = gpos + ((long long)b * sk.J + j) * 3;
         float* ga = gaxis + ((long long)b * sk.J + j) * 3;
         for (int c = 0; c < 3; ++c) {
-            gp[c] = T[j].t[c];
-            ga[c] = T[j].r[3 * c] * ax[0] + T[j].r[3 * c + 1] * ax[1] + T[j].r[3 * c + 2] * ax[2];
+            gp[c] = X.t[c];
+            ga[c] = X.r[3 * c] * ax[0] + X.r[3 * c + 1] * ax[1] + X.r[3 * c + 2] * ax[2];
         }
     }
     // skinning transforms J * scale * J0^-1 (DQSkinningGPUOp.cpp:274-306); the
     // rotation part has the uniform scale divided out (Eigen rotation())
-    for (int si = 0; si < sk.S; ++si) {
+    for (int si = threadIdx.x; si < sk.S; si += blockDim.x) {
         Xf A = T[sk.skin_joint[si]];
         const float sc = sk.skin_scale[si];
         Xf I0;
@@ -464,6 +484,229 @@ __global__ void k_lbs_disp_grad(Skel sk, int B, const float* __restrict__ xf12, 
                                  M[6] * g.x + M[7] * g.y + M[8] * g.z));
 }
 
+// Node-level skinning of the embedded graph (Pose2EmbeddedGraphCPUOp.cpp:129-300):
+// per (frame, node) the dual quaternions of the node's base vertex are blended
+// with the character's skin weights (same sign alignment and normalisation as
+// the vertices), turned into (R, t), and R into Z-Y-X Euler angles
+// (x = atan2(R21, R22), y = atan2(-R20, sy), z = atan2(R10, R00); singular
+// branch for sy < 1e-6).  The reference runs this on the host for every call.
+__global__ void k_pose2eg(Skel sk, int B, int M, const int* __restrict__ node_vertex, const float* __restrict__ dq,
+                          const float* __restrict__ w, float* __restrict__ out_t, float* __restrict__ out_a) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)B * M) return;
+    const int b = (int)(i / M), n = (int)(i % M);
+    const int v = node_vertex[n];
+    float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bt = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 first = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < sk.K; ++k) {
+        const int s = sk.skin_idx[(long long)v * sk.K + k];
+        const float wk = w[(long long)v * sk.K + k];
+        const float* q = dq + ((long long)b * sk.S + s) * 8;
+        const float4 r = f4(q), t = f4(q + 4);
+        float sign = 1.0f;
+        if (k == 0) first = r;
+        else if (dot4(first, r) < 0.0f) sign = -1.0f;
+        br = add4(br, mul4(mul4(r, wk), sign));
+        bt = add4(bt, mul4(mul4(t, wk), sign));
+    }
+    float scale = 1.f;
+    const float len = sqrtf(dot4(br, br));
+    if (len > 0.000001f) scale = 1.f / len;
+    br = mul4(br, scale);
+    bt = mul4(bt, scale);
+    float R[9];
+    dq_rotmat(br, R);
+    st3(out_t + 3 * i, dq_trans(br, bt));
+    const float sy = sqrtf(R[0] * R[0] + R[3] * R[3]);
+    float3 e;
+    if (!((double)sy < 1e-6)) {
+        e = make_float3(atan2f(R[7], R[8]), atan2f(-R[6], sy), atan2f(R[3], R[0]));
+    } else {
+        e = make_float3(atan2f(-R[5], R[4]), atan2f(-R[6], sy), 0.f);
+    }
+    st3(out_a + 3 * i, e);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the node skinning.  The reference registers no gradient for
+// Pose2EmbeddedGraphCpu (Pose2EmbeddedGraphCpu.py:55-60), so joint angles do
+// not train through the embedded graph there.  This is the exact adjoint of
+// the forward above, node by node:
+//   Euler angles <- rotation matrix <- blended, normalised rotation
+//   quaternion; translation <- (rotation, translation) quaternions;
+//   normalisation; weighted, sign-aligned blend of the joints' dual
+//   quaternions (the signs are locally constant).
+// The per-joint dual-quaternion gradients G_s (8 floats) are summed over the
+// nodes of a frame in shared memory.  A joint angle theta_j moves every
+// skinning transform below joint j by the world-frame rotation about the
+// joint's axis a through its position c, so
+//   d r_s / d theta_j = 1/2 (a, 0) x r_s,
+//   d t_s / d theta_j = a x (t_s - c),
+//   d tq_s / d theta_j = 1/2 (d t_s, 0) x r_s + 1/2 (t_s, 0) x d r_s
+// (tq = 1/2 (t, 0) x r, the translation part of the dual quaternion, "x" the
+// quaternion product); a prismatic joint translates them along a.
+// ---------------------------------------------------------------------------
+
+// quaternion product (x, y, z, w) convention: (p_v, p_w)(q_v, q_w)
+__device__ __forceinline__ float4 qmul(float4 p, float4 q) {
+    return make_float4(p.w * q.x + q.w * p.x + (p.y * q.z - p.z * q.y),
+                       p.w * q.y + q.w * p.y + (p.z * q.x - p.x * q.z),
+                       p.w * q.z + q.w * p.z + (p.x * q.y - p.y * q.x),
+                       p.w * q.w - (p.x * q.x + p.y * q.y + p.z * q.z));
+}
+
+// d loss / d (blended rotation, translation quaternions) of one node
+__device__ void pose2eg_node_grad(float4 br, float4 bt, float3 gT, float3 gE, float4& gbr, float4& gbt) {
+    float len = sqrtf(dot4(br, br));
+    const bool norm = len > 0.000001f;
+    const float scale = norm ? 1.f / len : 1.f;
+    const float4 q = mul4(br, scale), t = mul4(bt, scale);
+    float R[9];
+    dq_rotmat(q, R);
+    // Euler angles -> rotation matrix entries
+    float gR[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float sy2 = R[0] * R[0] + R[3] * R[3];
+    const float sy = sqrtf(sy2);
+    {   // y = atan2(-R20, sy)
+        const float u = -R[6], den = u * u + sy2;
+        if (den > 0.f) {
+            gR[6] += gE.y * (-sy / den);
+            if (sy > 0.f) {
+                const float gsy = gE.y * (-u / den);
+                gR[0] += gsy * R[0] / sy;
+                gR[3] += gsy * R[3] / sy;
+            }
+        }
+    }
+    if (!((double)sy < 1e-6)) {
+        const float dx = R[7] * R[7] + R[8] * R[8], dz = sy2;
+        if (dx > 0.f) {  // x = atan2(R21, R22)
+            gR[7] += gE.x * R[8] / dx;
+            gR[8] -= gE.x * R[7] / dx;
+        }
+        if (dz > 0.f) {  // z = atan2(R10, R00)
+            gR[3] += gE.z * R[0] / dz;
+            gR[0] -= gE.z * R[3] / dz;
+        }
+    } else {  // x = atan2(-R12, R11), z = 0
+        const float dx = R[5] * R[5] + R[4] * R[4];
+        if (dx > 0.f) {
+            gR[5] -= gE.x * R[4] / dx;
+            gR[4] += gE.x * R[5] / dx;
+        }
+    }
+    // rotation matrix of q = (x, y, z, w)
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    float4 gq;
+    gq.x = 2.f * (gR[1] * y + gR[2] * z + gR[3] * y - gR[4] * 2.f * x - gR[5] * w + gR[6] * z + gR[7] * w -
+                  gR[8] * 2.f * x);
+    gq.y = 2.f * (-gR[0] * 2.f * y + gR[1] * x + gR[2] * w + gR[3] * x + gR[5] * z - gR[6] * w + gR[7] * z -
+                  gR[8] * 2.f * y);
+    gq.z = 2.f * (-gR[0] * 2.f * z - gR[1] * w + gR[2] * x + gR[3] * w - gR[4] * 2.f * z + gR[5] * y + gR[6] * x +
+                  gR[7] * y);
+    gq.w = 2.f * (-gR[1] * z + gR[2] * y + gR[3] * z - gR[5] * x - gR[6] * y + gR[7] * x);
+    // translation T = dq_trans(q, t), bilinear in q and t
+    gq.x += 2.f * (-t.w * gT.x - t.z * gT.y + t.y * gT.z);
+    gq.y += 2.f * (t.z * gT.x - t.w * gT.y - t.x * gT.z);
+    gq.z += 2.f * (-t.y * gT.x + t.x * gT.y - t.w * gT.z);
+    gq.w += 2.f * (t.x * gT.x + t.y * gT.y + t.z * gT.z);
+    float4 gt;
+    gt.x = 2.f * (w * gT.x + z * gT.y - y * gT.z);
+    gt.y = 2.f * (-z * gT.x + w * gT.y + x * gT.z);
+    gt.z = 2.f * (y * gT.x - x * gT.y + w * gT.z);
+    gt.w = 2.f * (-x * gT.x - y * gT.y - z * gT.z);
+    if (norm) {  // q = br / |br|, t = bt / |br|
+        const float k = (dot4(br, gq) + dot4(bt, gt)) / (len * len * len);
+        gbr = add4(mul4(gq, scale), mul4(br, -k));
+        gbt = mul4(gt, scale);
+    } else {
+        gbr = gq;
+        gbt = gt;
+    }
+}
+
+// one CTA per frame: node gradients -> per-joint dual-quaternion gradients in shared memory
+__global__ void k_pose2eg_grad_nodes(Skel sk, int M, const int* __restrict__ node_vertex, const float* __restrict__ dq,
+                                     const float* __restrict__ w, const float* __restrict__ gT,
+                                     const float* __restrict__ gA, float* __restrict__ gdq) {
+    extern __shared__ float s_g[];  // [S][8]
+    const int b = blockIdx.x;
+    for (int i = threadIdx.x; i < sk.S * 8; i += blockDim.x) s_g[i] = 0.f;
+    __syncthreads();
+    for (int n = threadIdx.x; n < M; n += blockDim.x) {
+        const int v = node_vertex[n];
+        float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bt = br, first = br;
+        float sgn[16];
+        for (int k = 0; k < sk.K; ++k) {
+            const int s = sk.skin_idx[(long long)v * sk.K + k];
+            const float wk = w[(long long)v * sk.K + k];
+            const float* q = dq + ((long long)b * sk.S + s) * 8;
+            const float4 r = f4(q), t = f4(q + 4);
+            float sign = 1.0f;
+            if (k == 0) first = r;
+            else if (dot4(first, r) < 0.0f) sign = -1.0f;
+            if (k < 16) sgn[k] = sign;
+            br = add4(br, mul4(mul4(r, wk), sign));
+            bt = add4(bt, mul4(mul4(t, wk), sign));
+        }
+        const long long o = ((long long)b * M + n) * 3;
+        float4 gbr, gbt;
+        pose2eg_node_grad(br, bt, ld3(gT + o), ld3(gA + o), gbr, gbt);
+        for (int k = 0; k < sk.K && k < 16; ++k) {
+            const int s = sk.skin_idx[(long long)v * sk.K + k];
+            const float c = w[(long long)v * sk.K + k] * sgn[k];
+            float* g = s_g + s * 8;
+            atomicAdd(g + 0, c * gbr.x);
+            atomicAdd(g + 1, c * gbr.y);
+            atomicAdd(g + 2, c * gbr.z);
+            atomicAdd(g + 3, c * gbr.w);
+            atomicAdd(g + 4, c * gbt.x);
+            atomicAdd(g + 5, c * gbt.y);
+            atomicAdd(g + 6, c * gbt.z);
+            atomicAdd(g + 7, c * gbt.w);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < sk.S * 8; i += blockDim.x) gdq[(long long)b * sk.S * 8 + i] = s_g[i];
+}
+
+// per (frame, dof): sum over the dof's joints and the skinning joints below them
+__global__ void k_pose2eg_grad_dofs(Skel sk, int B, const float* __restrict__ dq, const float* __restrict__ gdq,
+                                    const float* __restrict__ gpos, const float* __restrict__ gaxis,
+                                    float* __restrict__ gdof) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B * sk.D) return;
+    const int b = i / sk.D, d = i % sk.D;
+    float acc = 0.f;
+    for (int e = sk.dof_off[d]; e < sk.dof_off[d + 1]; ++e) {
+        const int j = sk.dof_joint[e];
+        const float3 ax = ld3(gaxis + ((long long)b * sk.J + j) * 3);
+        const float3 c = ld3(gpos + ((long long)b * sk.J + j) * 3);
+        float gj = 0.f;
+        for (int s = 0; s < sk.S; ++s) {
+            if (!sk.in_chain[s * sk.J + j]) continue;
+            const float* q = dq + ((long long)b * sk.S + s) * 8;
+            const float4 r = f4(q), tq = f4(q + 4);
+            const float3 t = dq_trans(r, tq);
+            float4 dr, dt3;
+            float3 dtv;
+            if (sk.type[j] == kRevolute) {
+                dr = mul4(qmul(make_float4(ax.x, ax.y, ax.z, 0.f), r), 0.5f);
+                dtv = cross(ax, t - c);
+            } else {
+                dr = make_float4(0.f, 0.f, 0.f, 0.f);
+                dtv = ax;
+            }
+            dt3 = add4(mul4(qmul(make_float4(dtv.x, dtv.y, dtv.z, 0.f), r), 0.5f),
+                       mul4(qmul(make_float4(t.x, t.y, t.z, 0.f), dr), 0.5f));
+            const float* g = gdq + ((long long)b * sk.S + s) * 8;
+            gj += dot4(f4(g), dr) + dot4(f4(g + 4), dt3);
+        }
+        acc += sk.dof_w[e] * gj;
+    }
+    gdof[i] = acc;
+}
+
 }  // namespace
 }  // namespace hc
 
@@ -477,7 +720,7 @@ struct hc_skin_s {
     int parity = 1;
     DevBuf parent, type, offset, axis, jscale, dof_off, dof_joint, dof_w, skin_joint, skin_scale, t0inv, in_chain,
         skin_idx, base_v, base_n;
-    DevBuf joints, params, skin_xf, mom, lbs_xf;
+    DevBuf joints, params, skin_xf, mom, lbs_xf, gpos, gaxis, dq_ws, gdq;
     Skel skel() const {
         Skel s;
         s.J = J;
@@ -598,7 +841,8 @@ extern "C" hc_status hc_skin_destroy(hc_skin h) {
     if (!h) return HC_OK;
     DevBuf* bufs[] = {&h->parent, &h->type, &h->offset, &h->axis, &h->jscale, &h->dof_off, &h->dof_joint, &h->dof_w,
                       &h->skin_joint, &h->skin_scale, &h->t0inv, &h->in_chain, &h->skin_idx, &h->base_v,
-                      &h->base_n, &h->joints, &h->params, &h->skin_xf, &h->mom, &h->lbs_xf};
+                      &h->base_n, &h->joints, &h->params, &h->skin_xf, &h->mom, &h->lbs_xf, &h->gpos, &h->gaxis,
+                      &h->dq_ws, &h->gdq};
     for (DevBuf* b : bufs) b->release();
     delete h;
     return HC_OK;
@@ -615,8 +859,10 @@ static hc_status fk(hc_skin h, cudaStream_t s, int B, const float* dofs, float* 
     HC_TRY(h->joints.ensure(sizeof(Xf) * (size_t)B * h->J));
     HC_TRY(h->params.ensure(sizeof(float) * (size_t)B * h->J));
     HC_TRY(h->skin_xf.ensure(sizeof(Xf) * (size_t)B * h->S));
-    k_fk<<<div_up(B, 32), 32, 0, s>>>(h->skel(), B, dofs, h->joints.as<Xf>(), gpos, gaxis, h->skin_xf.as<Xf>(),
-                                      h->params.as<float>());
+    const size_t smem = sizeof(float) * ((h->J + 3) & ~3) + 2 * sizeof(Xf) * (size_t)h->J;
+    HC_REQUIRE(smem <= 48 * 1024, "skeleton too large for the kinematics kernel (%d joints)", h->J);
+    k_fk<<<B, 128, smem, s>>>(h->skel(), B, dofs, h->joints.as<Xf>(), gpos, gaxis, h->skin_xf.as<Xf>(),
+                              h->params.as<float>());
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
@@ -629,6 +875,8 @@ extern "C" hc_status hc_skin_reserve(hc_skin h, int32_t batch) {
     HC_TRY(h->skin_xf.ensure(sizeof(Xf) * (size_t)batch * h->S));
     HC_TRY(h->mom.ensure(sizeof(float) * 6 * (size_t)batch * h->S));
     HC_TRY(h->lbs_xf.ensure(sizeof(float) * 12 * (size_t)batch * h->S));
+    HC_TRY(h->gpos.ensure(sizeof(float) * 3 * (size_t)batch * h->J));
+    HC_TRY(h->gaxis.ensure(sizeof(float) * 3 * (size_t)batch * h->J));
     return HC_OK;
 }
 
@@ -734,6 +982,61 @@ extern "C" hc_status hc_lb_skinning_backward(hc_skin h, void* stream, int32_t ba
     k_lbs_disp_grad<<<div_up((long long)batch * h->N, 128), 128, 0, s>>>(
         h->skel(), batch, transformation, skinning_weights, skinned_vertex_positions_grad, h->parity,
         displacement_grad);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_pose2eg_forward(hc_skin h, void* stream, int32_t batch, const float* dofs, int32_t n_nodes,
+                                        const int32_t* node_vertex, const float* vertex_weights,
+                                        float* nodes_skinned_translation, float* nodes_skinned_rotation,
+                                        float* dual_quaternions) {
+    clear_error();
+    HC_REQUIRE(h && batch > 0 && n_nodes > 0, "invalid handle or sizes");
+    HC_REQUIRE(dofs && node_vertex && vertex_weights && nodes_skinned_translation && nodes_skinned_rotation &&
+                   dual_quaternions,
+               "NULL pointer");
+    cudaStream_t s = (cudaStream_t)stream;
+    HC_TRY(h->gpos.ensure(sizeof(float) * 3 * (size_t)batch * h->J));
+    HC_TRY(h->gaxis.ensure(sizeof(float) * 3 * (size_t)batch * h->J));
+    HC_TRY(fk(h, s, batch, dofs, h->gpos.as<float>(), h->gaxis.as<float>()));
+    const int BS = batch * h->S;
+    k_dq_from_xf<<<div_up(BS, 128), 128, 0, s>>>(BS, h->skin_xf.as<Xf>(), dual_quaternions);
+    HC_CHECK_LAUNCH();
+    k_pose2eg<<<div_up((long long)batch * n_nodes, 128), 128, 0, s>>>(h->skel(), batch, n_nodes, node_vertex,
+                                                                       dual_quaternions, vertex_weights,
+                                                                       nodes_skinned_translation,
+                                                                       nodes_skinned_rotation);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_pose2eg_backward(hc_skin h, void* stream, int32_t batch, const float* dofs, int32_t n_nodes,
+                                         const int32_t* node_vertex, const float* vertex_weights,
+                                         const float* nodes_skinned_translation_grad,
+                                         const float* nodes_skinned_rotation_grad, float* dofs_grad) {
+    clear_error();
+    HC_REQUIRE(h && batch > 0 && n_nodes > 0, "invalid handle or sizes");
+    HC_REQUIRE(dofs && node_vertex && vertex_weights && nodes_skinned_translation_grad &&
+                   nodes_skinned_rotation_grad && dofs_grad,
+               "NULL pointer");
+    HC_REQUIRE(h->K <= 16, "node skinning gradient supports up to 16 skinning joints per vertex");
+    cudaStream_t s = (cudaStream_t)stream;
+    HC_TRY(hc_skin_reserve(h, batch));
+    HC_TRY(h->dq_ws.ensure(sizeof(float) * 8 * (size_t)batch * h->S));
+    HC_TRY(h->gdq.ensure(sizeof(float) * 8 * (size_t)batch * h->S));
+    HC_TRY(fk(h, s, batch, dofs, h->gpos.as<float>(), h->gaxis.as<float>()));
+    const int BS = batch * h->S;
+    k_dq_from_xf<<<div_up(BS, 128), 128, 0, s>>>(BS, h->skin_xf.as<Xf>(), h->dq_ws.as<float>());
+    HC_CHECK_LAUNCH();
+    const size_t smem = sizeof(float) * 8 * (size_t)h->S;
+    HC_REQUIRE(smem <= 48 * 1024, "too many skinning joints (%d)", h->S);
+    k_pose2eg_grad_nodes<<<batch, 256, smem, s>>>(h->skel(), n_nodes, node_vertex, h->dq_ws.as<float>(),
+                                                  vertex_weights, nodes_skinned_translation_grad,
+                                                  nodes_skinned_rotation_grad, h->gdq.as<float>());
+    HC_CHECK_LAUNCH();
+    k_pose2eg_grad_dofs<<<div_up(batch * h->D, 128), 128, 0, s>>>(h->skel(), batch, h->dq_ws.as<float>(),
+                                                                  h->gdq.as<float>(), h->gpos.as<float>(),
+                                                                  h->gaxis.as<float>(), dofs_grad);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }

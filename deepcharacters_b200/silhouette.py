@@ -81,6 +81,61 @@ def projected_mesh_boundary(points_image_space, face_buffer, width: int, height:
     return out
 
 
+class MeshBoundaryEngine:
+    """Owns one ``hc_mesh_boundary`` handle: the mesh faces plus the
+    projection / coverage workspaces of ``ProjectedMeshBoundaryGpu``."""
+
+    def __init__(self, faces, n_vertices: int):
+        import numpy as np
+        f = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 3))
+        self.F, self.N = int(f.shape[0]), int(n_vertices)
+        h = C.c_void_p()
+        _lib.call("hc_mesh_boundary_create", C.byref(h), f.ctypes.data, self.F, self.N)
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and _lib._lib is not None:
+            _lib.lib().hc_mesh_boundary_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def reserve(self, B, Cn, width, height):
+        _lib.call("hc_mesh_boundary_reserve", self._h, B, Cn, int(width), int(height))
+
+    def forward(self, points_global_space, extrinsics, intrinsics, width: int, height: int,
+                points_image_space=None, out=None):
+        p = _f32(points_global_space, "points_global_space")
+        ex, it = _f32(extrinsics, "extrinsics"), _f32(intrinsics, "intrinsics")
+        B = p.shape[0]
+        Cn = ex.reshape(B, -1).shape[1] // 12
+        if p.shape[1] != self.N:
+            raise ValueError(f"points_global_space must be [B,{self.N},3]")
+        if out is None:
+            out = torch.empty((B, Cn, self.N), device=p.device, dtype=torch.uint8)
+        pis = _f32(points_image_space, "points_image_space") if points_image_space is not None else None
+        P = _lib.ptr
+        _lib.call("hc_mesh_boundary_forward", self._h, _stream(), B, Cn, int(width), int(height), P(p), P(ex), P(it),
+                  P(pis) if pis is not None else None, P(out))
+        return out
+
+
+class ProjectedMeshBoundaryGpu:
+    """Reference-shaped op (ProjectedMeshBoundaryGPUOp.cpp:5-17): faces stand in
+    for ``mesh_file_path_boundary_check``; output is_boundary [B,C,N] (uint8)."""
+
+    def __init__(self, faces, pointsGlobalSpace, extrinsics, intrinsics, numberBatches: int, numberCameras: int,
+                 renderU: int, renderV: int, useGapDetection: bool = False, engine: MeshBoundaryEngine | None = None):
+        eng = engine or MeshBoundaryEngine(faces, pointsGlobalSpace.shape[1])
+        self.isBoundary = eng.forward(pointsGlobalSpace, extrinsics, intrinsics, renderU, renderV)
+
+    def getNode(self):
+        return self.isBoundary
+
+
 class SilhouetteEngine:
     """Owns one ``hc_silhouette`` handle (its boundary-vertex grid workspace)."""
 
@@ -94,6 +149,10 @@ class SilhouetteEngine:
         if h is not None and _lib._lib is not None:
             _lib.lib().hc_silhouette_destroy(h)
             self._h = None
+
+    @property
+    def handle(self):
+        return self._h
 
     def reserve(self, B, Cn, N, U, V):
         _lib.call("hc_silhouette_reserve", self._h, B, Cn, N, U, V)

@@ -96,6 +96,10 @@ class SkinningEngine:
             _lib.lib().hc_skin_destroy(h)
             self._h = None
 
+    @property
+    def handle(self):
+        return self._h
+
     def set_parity(self, parity: bool):
         self.parity = bool(parity)
         _lib.call("hc_skin_set_parity", self._h, int(self.parity))
@@ -125,6 +129,42 @@ class SkinningEngine:
         P = _lib.ptr
         _lib.call("hc_dq_skinning_backward", self._h, _stream(), B, *(P(t) for t in args), P(gd), P(gw))
         return gd, gw
+
+    def pose2eg(self, dofs, node_vertex, weights):
+        """Pose2EmbeddedGraphCpu on the device (Pose2EmbeddedGraphCPUOp.cpp:129-300).
+
+        dofs [B,D]; node_vertex [M] int32 (base vertex of each graph node);
+        weights [N,K] (the character's skin weights).  Returns
+        (nodes_skinned_translation [B,M,3], nodes_skinned_rotation [B,M,3] Z-Y-X
+        Euler, dual_quaternions [B,S,8])."""
+        dofs, weights = _f32(dofs, "dofs"), _f32(weights, "skinning_weights")
+        nv = node_vertex.to(torch.int32).contiguous() if torch.is_tensor(node_vertex) else \
+            torch.as_tensor(node_vertex, dtype=torch.int32, device=dofs.device)
+        if weights.shape != (self.N, self.K):
+            raise ValueError(f"skin weights must be [{self.N},{self.K}], got {tuple(weights.shape)}")
+        if nv.numel() and (int(nv.min()) < 0 or int(nv.max()) >= self.N):
+            raise ValueError("node_vertex index out of range")
+        B, M = dofs.shape[0], nv.numel()
+        t = torch.empty((B, M, 3), device=dofs.device)
+        a = torch.empty((B, M, 3), device=dofs.device)
+        dq = torch.empty((B, self.S, 8), device=dofs.device)
+        P = _lib.ptr
+        _lib.call("hc_pose2eg_forward", self._h, _stream(), B, P(dofs), M, P(nv), P(weights), P(t), P(a), P(dq))
+        return t, a, dq
+
+    def pose2eg_backward(self, dofs, node_vertex, weights, grad_translation, grad_rotation):
+        """Adjoint of ``pose2eg``: d loss / d dofs [B,D] from the gradients of
+        the node translations / Euler rotations [B,M,3] (the reference op
+        has no gradient; this one is exact)."""
+        dofs, weights = _f32(dofs, "dofs"), _f32(weights, "skinning_weights")
+        gt, ga = _f32(grad_translation, "grad_translation"), _f32(grad_rotation, "grad_rotation")
+        nv = node_vertex.to(torch.int32).contiguous() if torch.is_tensor(node_vertex) else \
+            torch.as_tensor(node_vertex, dtype=torch.int32, device=dofs.device)
+        B, M = dofs.shape[0], nv.numel()
+        out = torch.empty((B, self.D), device=dofs.device)
+        P = _lib.ptr
+        _lib.call("hc_pose2eg_backward", self._h, _stream(), B, P(dofs), M, P(nv), P(weights), P(gt), P(ga), P(out))
+        return out
 
     def lbs_forward(self, dofs, weights, disp):
         dofs, weights, disp = _f32(dofs, "dofs"), _f32(weights, "skinning_weights"), _f32(disp, "displacement")

@@ -463,3 +463,44 @@ def identity_crops(batch: int, views: int, width: int, height: int) -> np.ndarra
     """Multi-view crops (border u, border v, scale, min u, min v, max u, max v) of uncropped images."""
     c = np.array([0, 0, 1, 0, 0, width, height], np.float32)
     return np.tile(c, (batch, views, 1))
+
+
+def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int, width: int, height: int, seed: int,
+                fx: float | None = None, ring_radius: float = 3.0 * MM, k: int = 4, pose_amplitude: float = 0.5,
+                delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, n_masks: int | None = None) -> dict:
+    """Inputs of the whole deform-and-render chain on one character: a
+    jittered icosphere with an embedded graph (``n_nodes`` farthest-point
+    nodes, K nearest nodes per vertex) and a random ``n_skel``-joint tree with
+    K-nearest-joint skinning weights; per frame an independent pose (joint
+    angles U(-a, a)) and node deltas (Euler N(0, 0.05) rad, translation
+    N(0, 10) mm); 8 markers on random nodes; cameras on a ring; vertex colours U[0,1]; target images
+    U[0,1]; silhouette distance-transform images of seeded random ellipses
+    (``n_masks`` distinct ones, default one per view, reused across frames)."""
+    rng = rng_for(seed)
+    verts, faces = sphere_mesh(subdiv, rng)
+    N = verts.shape[0]
+    graph = embedded_graph(verts, n_nodes, k, rng)
+    mk_nodes = rng.choice(n_nodes, size=8, replace=False).astype(np.int32)
+    markers = (verts[graph.node_vertex[mk_nodes]] + rng.normal(0, 5.0, (8, 3))).astype(np.float32)
+    sk = random_skeleton(n_skel, rng)
+    skin_idx, skin_w = skinning_weights(verts, sk, k, rng)
+    dofs = np.stack([random_pose(sk, rng_for(seed, b), pose_amplitude) for b in range(frames)])
+    f = lambda std, shape: rng.normal(0.0, std, size=shape).astype(np.float32)  # noqa: E731
+    if fx is None:
+        fx = 600.0 * min(width, height) / 512.0
+    ex, it = camera_ring(views, ring_radius, fx, width, height)
+    nm = views if n_masks is None else n_masks
+    masks = silhouette_masks(1, nm, width, height, seed=seed, scale=min(width, height) / 512.0)[0]
+    dt = np.stack([masks[np.arange(views) % nm]] * frames)
+    return dict(verts=verts, faces=faces, graph=graph, markers=markers, marker_node=mk_nodes, skeleton=sk,
+                skin_index=skin_idx, skin_weights=skin_w,
+                dofs=dofs, dT=f(delta_t_std, (frames, n_nodes, 3)), dA=f(delta_rot_std, (frames, n_nodes, 3)),
+                disp=np.zeros((frames, N, 3), np.float32),
+                colors=rng.uniform(0.0, 1.0, size=(frames, N, 3)).astype(np.float32),
+                texture=rng.uniform(0.0, 1.0, size=(frames, 16, 16, 3)).astype(np.float32),
+                sh=sh_coefficients(frames * views, rng).reshape(frames, views, 27),
+                extr=np.tile(ex[None], (frames, 1)), intr=np.tile(it[None], (frames, 1)),
+                texcoords=spherical_uvs(verts, faces),
+                target=rng.uniform(0.0, 1.0, size=(frames, views, height, width, 3)).astype(np.float32),
+                dt=dt, crops=identity_crops(frames, views, width, height),
+                N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=width, H=height)

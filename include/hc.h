@@ -284,6 +284,27 @@ hc_status hc_lb_skinning_backward(hc_skin h, void* stream, int32_t batch,
                                   const float* skinning_weights, const float* displacement, float* dofs_grad,
                                   float* skinning_weights_grad, float* displacement_grad);
 
+/* Pose2EmbeddedGraphCpu on the device (Pose2EmbeddedGraphCPUOp.cpp:6-13,129-300):
+ * dofs [B,D] -> per embedded-graph node the blended dual quaternion of its
+ * base vertex (node_vertex [M], device), with the character's skin weights
+ * vertex_weights [N,K] (device), as nodes_skinned_translation [B,M,3] and
+ * Z-Y-X Euler nodes_skinned_rotation [B,M,3] (the EG op's skinned inputs);
+ * dual_quaternions [B,S,8] receives the skinning joints' dual quaternions. */
+hc_status hc_pose2eg_forward(hc_skin h, void* stream, int32_t batch, const float* dofs, int32_t n_nodes,
+                             const int32_t* node_vertex, const float* vertex_weights,
+                             float* nodes_skinned_translation, float* nodes_skinned_rotation,
+                             float* dual_quaternions);
+/* Adjoint of hc_pose2eg_forward (no counterpart in the reference, which
+ * registers no gradient for Pose2EmbeddedGraphCpu, Pose2EmbeddedGraphCpu.py:
+ * 55-60): gradients of nodes_skinned_translation / nodes_skinned_rotation
+ * [B,M,3] -> dofs_grad [B,D], exact through the Euler angles, the blended
+ * dual quaternions and the kinematic chain.  Recomputes the forward
+ * kinematics from dofs. */
+hc_status hc_pose2eg_backward(hc_skin h, void* stream, int32_t batch, const float* dofs, int32_t n_nodes,
+                              const int32_t* node_vertex, const float* vertex_weights,
+                              const float* nodes_skinned_translation_grad,
+                              const float* nodes_skinned_rotation_grad, float* dofs_grad);
+
 /* ------------------------------------------------------------------------ */
 /* Camera projection, projected-mesh boundary, silhouette DT loss            */
 /* ------------------------------------------------------------------------ */
@@ -303,10 +324,32 @@ hc_status hc_camera_projection_backward(void* stream, int32_t batch, int32_t n_c
                                         const float* points_image_space_grad, const float* points_global_space,
                                         const float* extrinsics, const float* intrinsics, int32_t is_point,
                                         float* points_global_space_grad);
-/* ProjectedMeshBoundaryGpu (Skeletool/Mesh/CUDABasedRasterization.cu:168-200):
- * a vertex is a boundary vertex of a view when a pixel of the 3x3 window
- * around its truncated projection is uncovered; coverage is a renderer face
- * buffer [B,C,H,W] (-1 = empty).  is_boundary [B,C,N] uint8. */
+typedef struct hc_mesh_boundary_s* hc_mesh_boundary;
+
+/* ProjectedMeshBoundaryGpu (ProjectedMeshBoundaryGPUOp.cpp:5-17,139-160;
+ * Skeletool/Mesh/CUDABasedRasterization.cu:53-206).  The handle holds the
+ * mesh faces (the op's mesh_file_path_boundary_check).  Forward projects
+ * points_global_space [B,N,3] with extrinsics [B,12C] / intrinsics [B,9C]
+ * (or takes the projection from points_image_space [B,C,N,2] when that is
+ * non-NULL: CameraProjectionGpu gives the identical points), rasterises the
+ * image-space coverage of the mesh at width x height (render_u x render_v)
+ * and flags a vertex of a view when a pixel of the 3x3 window around its
+ * truncated projection is uncovered.  is_boundary [B,C,N] uint8 (TF bool).
+ * Bit-identical to the reference op. */
+hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
+                                  int32_t n_vertices);
+hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h);
+hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch, int32_t n_cameras, int32_t width,
+                                   int32_t height);
+hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                   int32_t width, int32_t height, const float* points_global_space,
+                                   const float* extrinsics, const float* intrinsics,
+                                   const float* points_image_space, uint8_t* is_boundary);
+/* The same boundary test with coverage taken from a renderer face buffer
+ * [B,C,H,W] (-1 = empty) instead of the op's own 2-D raster.  No separate
+ * reference counterpart: the renderer's ray test and the 2-D barycentric test
+ * disagree on some pixels along triangle edges, so flags can differ from
+ * ProjectedMeshBoundaryGpu there.  is_boundary [B,C,N] uint8. */
 hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
                                      int32_t width, int32_t height, const float* points_image_space,
                                      const int32_t* face_buffer, uint8_t* is_boundary);
@@ -379,6 +422,31 @@ hc_status hc_image_l1_loss(void* stream, int64_t n_pixels, const float* render_b
                            const float* target_image, const int32_t* face_buffer,
                            const uint8_t* foreground_mask, void* workspace, float* loss,
                            float* render_buffer_grad);
+
+/*
+ * Sum-of-squares loss of a residual and its gradient: loss = weight * sum x^2,
+ * grad = 2 * weight * x (n floats).  The silhouette residuals of
+ * MultiViewSilhouetteLossGpu (mv_dt_residual, mv_dt_residual_1) are trained
+ * with it; the reference leaves this reduction to the TF graph.  workspace is
+ * device scratch of at least 8 bytes.
+ */
+hc_status hc_sum_squares_loss(void* stream, int64_t n, const float* x, float weight, void* workspace, float* loss,
+                              float* grad);
+
+/*
+ * Gaussian smoothing of target images (GaussianSmoothingGpu.smoothImage,
+ * Projects/CustomTFOperators/GaussianSmoothingGpu.py:12-37): image [n, H, W,
+ * channels] (channels <= 4) convolved per channel with the (2 size + 1)^2
+ * normalised Gaussian of the given mean / std, zero padding; size <= 15.
+ * size == 0 or std == 0 copies the image, as the reference returns it.
+ */
+hc_status hc_gaussian_smooth(void* stream, int32_t n_images, int32_t height, int32_t width, int32_t channels,
+                             int32_t size, float mean, float std, const float* image, float* out);
+
+/* dst += src over n floats: the AddN that TF inserts where two gradient
+ * branches meet on one tensor (e.g. vertex positions, fed by the renderer
+ * and by the silhouette's camera projection). */
+hc_status hc_add_inplace(void* stream, int64_t n, float* dst, const float* src);
 
 #ifdef __cplusplus
 }

@@ -467,3 +467,100 @@ class RefSilhouette:
         if st != 0:
             raise RuntimeError(f"reference silhouette grad failed: {st}")
         return out
+
+
+# ---------------------------------------------------------------------------
+# projected-mesh boundary (reference GPU kernels, separate library)
+# ---------------------------------------------------------------------------
+REF_MB_LIB = os.path.join(HERE, "_ref", "libhcref_mb.so")
+_mblib = None
+
+
+def ref_mesh_boundary(faces, pts, extr, intr, width, height):
+    """ProjectedMeshBoundaryGpu through the reference's own kernels
+    (Skeletool/Mesh/CUDABasedRasterization.cu): bool [B,C,N] as uint8."""
+    import torch
+    global _mblib
+    if _mblib is None:
+        if not os.path.exists(REF_MB_LIB):
+            raise RuntimeError(f"{REF_MB_LIB} missing: run `make -C oracle ref` where the reference tree exists")
+        _mblib = C.CDLL(REF_MB_LIB)
+        _mblib.hcref_mesh_boundary.restype = C.c_int
+        _mblib.hcref_mesh_boundary.argtypes = [C.c_int] * 6 + [C.c_void_p] * 5
+    B, N = pts.shape[:2]
+    Cn = extr.reshape(B, -1).shape[1] // 12
+    f = torch.as_tensor(np.ascontiguousarray(faces, np.int32)).to(pts.device)
+    out = torch.zeros((B, Cn, N), device=pts.device, dtype=torch.uint8)
+    torch.cuda.synchronize()
+    st = _mblib.hcref_mesh_boundary(B, Cn, N, f.shape[0], int(width), int(height), _p(f), _p(pts), _p(extr),
+                                    _p(intr), _p(out))
+    if st != 0:
+        raise RuntimeError(f"reference mesh boundary failed: {st}")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# UV-space maps (reference host class + kernels)
+# ---------------------------------------------------------------------------
+class RefUV:
+    """The reference renderer object in a compute_normal_map mode
+    (CUDABasedRasterization.cpp, host texel table built on the first call)."""
+
+    def __init__(self, faces, texcoords, N, C_, W, H, normal_mode, albedo="vertexColor", shading="shadeless"):
+        L = ref_lib()
+        L.hcref_uv_create.restype = C.c_void_p
+        L.hcref_uv_create.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                      C.c_char_p, C.c_char_p, C.c_char_p]
+        L.hcref_uv_forward.restype = C.c_int
+        L.hcref_uv_forward.argtypes = [C.c_void_p] + [C.c_int] * 7 + [C.c_void_p] * 8
+        f = _c(faces, np.int32).reshape(-1)
+        tc = _c(texcoords, np.float32).reshape(-1)
+        self.N, self.C, self.W, self.H = N, C_, W, H
+        self.h = L.hcref_uv_create(N, _p(f), f.size // 3, _p(tc), C_, W, H, albedo.encode(), shading.encode(),
+                                   normal_mode.encode())
+
+    def forward(self, B, verts, extr, intr, TH, TW):
+        import torch
+        dev = verts.device
+        o = {"bary": torch.full((B, self.C, self.H, self.W, 2), 7.0, device=dev),
+             "face": torch.full((B, self.C, self.H, self.W), 7, device=dev, dtype=torch.int32),
+             "render": torch.full((B, self.C, self.H, self.W, 3), 7.0, device=dev),
+             "vnormal": torch.zeros((B, self.C, self.N, 3), device=dev),
+             "normal_map": torch.zeros((B, TH, TW, 3), device=dev)}
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_uv_forward(self.h, B, self.N, self.C, self.W, self.H, TW, TH, _p(verts), _p(extr),
+                                        _p(intr), _p(o["bary"]), _p(o["face"]), _p(o["render"]), _p(o["vnormal"]),
+                                        _p(o["normal_map"]))
+        if st != 0:
+            raise RuntimeError(f"reference uv forward failed: {st}")
+        return o
+
+
+def texel_table(texcoords, TH, TW):
+    """FP64 restatement of the reference's texel table (CUDABasedRasterization.cpp:266-330):
+    per texel (face, a, b, c) of the last (largest-id) face whose UV triangle
+    contains the texel centre; (0, 0, 0, 0) elsewhere."""
+    tc = np.asarray(texcoords, np.float64).reshape(-1, 3, 2)
+    F = tc.shape[0]
+    out = np.zeros((TH, TW, 4))
+    for f in range(F):
+        p = np.stack([TW * tc[f, :, 0], TH * (1.0 - tc[f, :, 1])], 1)
+        x0 = int(max(p[:, 0].min() - 2, 0))
+        x1 = int(min(p[:, 0].max() + 2, TW))
+        y0 = int(max(p[:, 1].min() - 2, 0))
+        y1 = int(min(p[:, 1].max() + 2, TH))
+        if x1 <= x0 or y1 <= y0:
+            continue
+        xx, yy = np.meshgrid(np.arange(x0, x1) + 0.5, np.arange(y0, y1) + 0.5)
+        e = lambda a, b, px, py: (b[0] - a[0]) * (py - a[1]) - (b[1] - a[1]) * (px - a[0])  # noqa: E731
+        nz = e(p[0], p[1], p[2][0], p[2][1])
+        if nz == 0:
+            continue
+        s0 = e(p[0], p[1], xx, yy) * nz
+        a = e(p[1], p[2], xx, yy) * nz
+        b = e(p[2], p[0], xx, yy) * nz
+        hit = (s0 >= 0) & (a >= 0) & (b >= 0)
+        aa, bb = a / (nz * nz), b / (nz * nz)
+        sl = out[y0:y1, x0:x1]
+        sl[hit] = np.stack([np.full(hit.sum(), f), aa[hit], bb[hit], 1 - aa[hit] - bb[hit]], 1)
+    return out

@@ -132,3 +132,47 @@ def silhouette_backward(g, g1, dtg, closest, crops):
             for y, x in zip(ys, xs):
                 out[b, c, int(closest[b, c, y, x])] += g1[b, c, y, x] / (30 * sc)
     return out
+
+
+def mesh_boundary(faces, p2d, width, height):
+    """ProjectedMeshBoundaryGpu in FP64 (Skeletool/Mesh/CUDABasedRasterization.cu:80-200):
+    2-D coverage of every projected triangle (pixel centres with image-space
+    barycentrics in [-0.001, 1.001] inside the clamped bounding box), then a
+    vertex is a boundary vertex when its 3x3 window (around the truncated
+    projection, fully inside the image) has an uncovered pixel.
+    p2d [B,C,N,2] -> uint8 [B,C,N]."""
+    p2d = np.asarray(p2d, np.float64)
+    f = np.asarray(faces, np.int64).reshape(-1, 3)
+    B, Cn, N = p2d.shape[:3]
+    out = np.zeros((B, Cn, N), np.uint8)
+    for b in range(B):
+        for c in range(Cn):
+            P = p2d[b, c]
+            cover = np.zeros((height, width), bool)
+            a, bb, cc = P[f[:, 0]], P[f[:, 1]], P[f[:, 2]]
+            tri = np.stack([a, bb, cc], 1)
+            x0 = np.maximum(tri[:, :, 0].min(1) - 0.5, 0).astype(np.int64)
+            y0 = np.maximum(tri[:, :, 1].min(1) - 0.5, 0).astype(np.int64)
+            x1 = np.minimum(tri[:, :, 0].max(1) + 0.5, width - 1).astype(np.int64)
+            y1 = np.minimum(tri[:, :, 1].max(1) + 0.5, height - 1).astype(np.int64)
+            d2 = (a[:, 1] - bb[:, 1]) * cc[:, 0] + (bb[:, 0] - a[:, 0]) * cc[:, 1] + a[:, 0] * bb[:, 1] - bb[:, 0] * a[:, 1]
+            d1 = (a[:, 1] - cc[:, 1]) * bb[:, 0] + (cc[:, 0] - a[:, 0]) * bb[:, 1] + a[:, 0] * cc[:, 1] - cc[:, 0] * a[:, 1]
+            for t in range(f.shape[0]):
+                if x0[t] > x1[t] or y0[t] > y1[t]:
+                    continue
+                uu, vv = np.meshgrid(np.arange(x0[t], x1[t] + 1) + 0.5, np.arange(y0[t], y1[t] + 1) + 0.5)
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    e2 = ((a[t, 1] - bb[t, 1]) * uu + (bb[t, 0] - a[t, 0]) * vv + a[t, 0] * bb[t, 1]
+                          - bb[t, 0] * a[t, 1]) / d2[t]
+                    e1 = ((a[t, 1] - cc[t, 1]) * uu + (cc[t, 0] - a[t, 0]) * vv + a[t, 0] * cc[t, 1]
+                          - cc[t, 0] * a[t, 1]) / d1[t]
+                e0 = 1.0 - e2 - e1
+                ins = ((e0 >= -0.001) & (e1 >= -0.001) & (e2 >= -0.001) & (e0 <= 1.001) & (e1 <= 1.001)
+                       & (e2 <= 1.001))
+                cover[y0[t]:y1[t] + 1, x0[t]:x1[t] + 1] |= ins
+            u = np.trunc(P[:, 0]).astype(np.int64)
+            v = np.trunc(P[:, 1]).astype(np.int64)
+            ok = (u - 1 >= 0) & (u + 1 < width) & (v - 1 >= 0) & (v + 1 < height)
+            for i in np.nonzero(ok)[0]:
+                out[b, c, i] = 0 if cover[v[i] - 1:v[i] + 2, u[i] - 1:u[i] + 2].all() else 1
+    return out

@@ -161,6 +161,46 @@ def dq_skin(ch, dq, weights):
     return out_v, out_n
 
 
+def pose2eg(ch, dofs, node_vertex, weights):
+    """Node-level skinning of the embedded graph in FP64
+    (Pose2EmbeddedGraphCPUOp.cpp:129-300): blend the dual quaternions of each
+    node's base vertex with the skin weights [N,K] (sign-aligned to the first,
+    normalised when the norm exceeds 1e-6), return the blended translation and
+    the Z-Y-X Euler angles of the blended rotation (singular branch for
+    sy < 1e-6), [B,M,3] each, plus the joints' dual quaternions [B,S,8]."""
+    dq = dual_quaternions(ch, dofs)
+    w = np.asarray(weights, np.float64)
+    nv = np.asarray(node_vertex, np.int64)
+    idx = ch.skin_index[nv]                      # [M,K]
+    q = dq[:, idx]                               # [B,M,K,8]
+    wk = w[nv][None, :, :, None]                 # [1,M,K,1]
+    first = q[:, :, :1, :4]
+    sign = np.where(np.sum(first * q[..., :4], -1, keepdims=True) < 0, -1.0, 1.0)
+    sign[:, :, 0] = 1.0
+    blend = np.sum(q * wk * sign, axis=2)        # [B,M,8]
+    ln = np.linalg.norm(blend[..., :4], axis=-1, keepdims=True)
+    blend = np.where(ln > 1e-6, blend / np.where(ln > 1e-6, ln, 1.0), blend)
+    r, t = blend[..., :4], blend[..., 4:]
+    x, y, z, ww = r[..., 0], r[..., 1], r[..., 2], r[..., 3]
+    tx, ty, tz, tw = t[..., 0], t[..., 1], t[..., 2], t[..., 3]
+    out_t = 2 * np.stack([-tw * x + tx * ww - ty * z + tz * y,
+                          -tw * y + tx * z + ty * ww - tz * x,
+                          -tw * z - tx * y + ty * x + tz * ww], -1)
+    R00 = 1 - 2 * y * y - 2 * z * z
+    R10 = 2 * y * x + 2 * z * ww
+    R20 = 2 * z * x - 2 * y * ww
+    R21 = 2 * z * y + 2 * x * ww
+    R22 = 1 - 2 * x * x - 2 * y * y
+    R11 = 1 - 2 * x * x - 2 * z * z
+    R12 = 2 * z * y - 2 * x * ww
+    sy = np.hypot(R00, R10)
+    sing = sy < 1e-6
+    ax = np.where(sing, np.arctan2(-R12, R11), np.arctan2(R21, R22))
+    ay = np.arctan2(-R20, sy)
+    az = np.where(sing, 0.0, np.arctan2(R10, R00))
+    return out_t, np.stack([ax, ay, az], -1), dq
+
+
 def lbs_skin(ch, Rs, ts, weights, disp):
     w = np.asarray(weights, np.float64)
     disp = np.asarray(disp, np.float64)

@@ -1,0 +1,50 @@
+"""Host logic of the chain: every C-ABI call that one step issues names an
+exported symbol with the declared number of arguments, in the order of the
+reference's TF graph (no GPU: the library calls are recorded, not run)."""
+import numpy as np
+import pytest
+
+from deepcharacters_b200 import _lib
+from deepcharacters_b200 import synthetic as S
+
+
+@pytest.fixture
+def recorder(monkeypatch):
+    calls = []
+
+    def fake_call(name, *args):
+        assert name in _lib._SIGS, name
+        assert len(args) == len(_lib._SIGS[name]), (name, len(args), len(_lib._SIGS[name]))
+        calls.append((name, args))
+
+    monkeypatch.setattr(_lib, "call", fake_call)
+    import deepcharacters_b200.chain as chain
+    monkeypatch.setattr(chain, "_stream", lambda: 0)
+    return calls
+
+
+def test_chain_step_calls(recorder):
+    from deepcharacters_b200.chain import DeformRenderChain
+    sc = S.chain_scene(1, 12, 2, 2, 2, 32, 32, seed=3)
+    ch = DeformRenderChain(sc, "cpu", 2, 2, 32, 32)
+    recorder.clear()
+    ch.step()
+    names = [n for n, _ in recorder]
+    assert names == ["hc_pose2eg_forward", "hc_eg_forward", "hc_renderer_forward", "hc_image_l1_loss",
+                     "hc_camera_projection_forward", "hc_camera_projection_forward", "hc_mesh_boundary_forward",
+                     "hc_silhouette_forward", "hc_sum_squares_loss", "hc_sum_squares_loss", "hc_silhouette_backward",
+                     "hc_camera_projection_backward", "hc_renderer_backward", "hc_add_inplace", "hc_eg_backward",
+                     "hc_pose2eg_backward"]
+    args = dict(recorder)
+    # the EG consumes the node transforms that the node skinning wrote
+    assert args["hc_eg_forward"][5] == args["hc_pose2eg_forward"][7]
+    assert args["hc_eg_forward"][6] == args["hc_pose2eg_forward"][8]
+    # the raster and the silhouette see the EG vertices; the summed gradient feeds the EG adjoint
+    v = args["hc_eg_forward"][8]
+    assert args["hc_renderer_forward"][3] == v and args["hc_camera_projection_forward"][4] == v
+    assert args["hc_eg_backward"][3] == args["hc_renderer_backward"][16] == args["hc_add_inplace"][2]
+    assert args["hc_add_inplace"][3] == args["hc_camera_projection_backward"][9]
+    # joint angles: the EG's skinned-transform gradients feed the node-skinning adjoint
+    assert args["hc_pose2eg_backward"][7] == args["hc_eg_backward"][9]
+    assert args["hc_pose2eg_backward"][8] == args["hc_eg_backward"][10]
+    assert np.isfinite(sc["dofs"]).all()

@@ -103,3 +103,36 @@ def test_silhouette_matches_fp64_oracle(scene):
     assert np.array_equal(ours[3].cpu().numpy(), ora[3])
     for a, b in zip(ours[:3], ora[:3]):
         assert nrel(a, b) < 1e-6
+
+
+@needs_ref
+def test_mesh_boundary_matches_reference_kernels(scene):
+    from deepcharacters_b200.silhouette import MeshBoundaryEngine
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    eng = MeshBoundaryEngine(sc["faces"], sc["N"])
+    ours = eng.forward(scene["verts"], ex, it, RES, RES)
+    ref = O.ref_mesh_boundary(sc["faces"], scene["verts"], ex, it, RES, RES)
+    torch.cuda.synchronize()
+    assert int(ref.sum()) > 0
+    assert torch.equal(ours, ref), int((ours != ref).sum())
+    # from a CameraProjectionGpu result: the same points, the same flags
+    p2d = camera_projection_forward(scene["verts"], None, ex, it, 1)
+    assert torch.equal(eng.forward(scene["verts"], ex, it, RES, RES, points_image_space=p2d), ref)
+    # a non-square raster
+    ours = eng.forward(scene["verts"], ex, it, RES, RES // 2)
+    ref = O.ref_mesh_boundary(sc["faces"], scene["verts"], ex, it, RES, RES // 2)
+    assert torch.equal(ours, ref), int((ours != ref).sum())
+
+
+def test_mesh_boundary_matches_fp64_oracle(scene):
+    from deepcharacters_b200.silhouette import MeshBoundaryEngine
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    ours = MeshBoundaryEngine(sc["faces"], sc["N"]).forward(scene["verts"], ex, it, RES, RES).cpu().numpy()
+    p2d = SO.project(sc["verts"], None, sc["extr"], sc["intr"], True)
+    ora = SO.mesh_boundary(sc["faces"], p2d, RES, RES)
+    # FP64 coverage differs from FP32 only where a pixel centre sits on the
+    # -0.001 / 1.001 barycentric tolerance
+    assert ora.sum() > 0
+    assert (ours != ora).mean() < 1e-3

@@ -121,3 +121,75 @@ def test_autograd_wrappers(scene):
     out = lb_skinning_gpu(eng, dofs, w, disp)
     out[0].square().sum().backward()
     assert disp.grad is not None and float(disp.grad.abs().sum()) > 0
+
+
+def _euler_to_rot(a):
+    """R = Rz(z) Ry(y) Rx(x) for Euler angles [...,3] (the convention the EG op reads)."""
+    x, y, z = a[..., 0], a[..., 1], a[..., 2]
+    cx, sx, cy, sy, cz, sz = np.cos(x), np.sin(x), np.cos(y), np.sin(y), np.cos(z), np.sin(z)
+    R = np.empty(a.shape[:-1] + (3, 3))
+    R[..., 0, 0] = cz * cy
+    R[..., 0, 1] = cz * sy * sx - sz * cx
+    R[..., 0, 2] = cz * sy * cx + sz * sx
+    R[..., 1, 0] = sz * cy
+    R[..., 1, 1] = sz * sy * sx + cz * cx
+    R[..., 1, 2] = sz * sy * cx - cz * sx
+    R[..., 2, 0] = -sy
+    R[..., 2, 1] = cy * sx
+    R[..., 2, 2] = cy * cx
+    return R
+
+
+def test_pose2eg_matches_fp64_oracle_and_dq_skinning(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    rng = np.random.default_rng(7)
+    nodes = rng.choice(ch.base_vertices.shape[0], size=97, replace=False).astype(np.int32)
+    w0 = sc["weights"][0]
+    t, a, dq = eng.pose2eg(_t(sc["dofs"]), torch.from_numpy(nodes).to(DEV), _t(w0))
+    to, ao, dqo = K.pose2eg(ch, sc["dofs"], nodes, w0)
+    assert nrel(t, to) < 1e-5
+    # angles compared on the circle; the rotation they encode compared directly
+    d = a.cpu().double().numpy() - ao
+    assert np.abs(np.arctan2(np.sin(d), np.cos(d))).max() < 1e-4
+    assert np.abs(_euler_to_rot(a.cpu().double().numpy()) - _euler_to_rot(ao)).max() < 1e-5
+    # same dual quaternions as the skinning op, and a node moves like its skinned base vertex
+    v, _, _, _, dq_s, _ = eng.dq_forward(_t(sc["dofs"]), _t(sc["weights"]))
+    assert torch.equal(dq, dq_s)
+    R = _euler_to_rot(a.cpu().double().numpy())
+    p = np.einsum("bmij,mj->bmi", R, ch.base_vertices[nodes].astype(np.float64)) + t.cpu().double().numpy()
+    assert nrel(p, v[:, torch.from_numpy(nodes).long()]) < 1e-5
+
+
+def test_pose2eg_rejects_bad_nodes(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    with pytest.raises(ValueError):
+        eng.pose2eg(_t(sc["dofs"]), torch.tensor([0, ch.base_vertices.shape[0]], device=DEV), _t(sc["weights"][0]))
+
+
+def test_pose2eg_backward_matches_fp64_finite_differences(scene):
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    rng = np.random.default_rng(11)
+    nodes = rng.choice(ch.base_vertices.shape[0], size=61, replace=False).astype(np.int32)
+    w0 = sc["weights"][0]
+    dofs = sc["dofs"].astype(np.float64)
+    B, D = dofs.shape
+    gt = rng.normal(size=(B, len(nodes), 3))
+    ga = rng.normal(size=(B, len(nodes), 3))
+    ours = eng.pose2eg_backward(_t(dofs), torch.from_numpy(nodes).to(DEV), _t(w0), _t(gt), _t(ga)).cpu().double()
+
+    def loss(d):  # per-frame loss of the FP64 restatement
+        t, a, _ = K.pose2eg(ch, d, nodes, w0)
+        return (gt * t).sum(axis=(1, 2)) + (ga * a).sum(axis=(1, 2))
+
+    h = 1e-6
+    fd = np.zeros((B, D))
+    for d in range(D):  # frames are independent: perturb one dof of every frame at once
+        p, m = dofs.copy(), dofs.copy()
+        p[:, d] += h
+        m[:, d] -= h
+        fd[:, d] = (loss(p) - loss(m)) / (2 * h)
+    assert np.abs(fd).max() > 1.0
+    assert nrel(ours, fd) < 1e-4, nrel(ours, fd)
