@@ -205,6 +205,17 @@ def stage_bytes(sc):
     }
 
 
+def kernel_bytes(sc):
+    """Algorithmic bytes per launch of the two raster kernels over FRAMES x VIEWS views:
+    k_resolve writes face 4 + barycentrics 8 + colour 12 B per pixel and reads each
+    frame's positions, colours and faces once; k_render_grad reads the image
+    gradient 12, barycentrics 8, face 4 and target 12 B per pixel and each frame's
+    positions, colours and faces, and writes the position and colour gradients."""
+    V, P, N, F = FRAMES * VIEWS, RES * RES, sc["N"], sc["F"]
+    return {"resolve": V * 24 * P + FRAMES * (24 * N + 12 * F),
+            "render_grad": V * 36 * P + FRAMES * (24 * N + 12 * F + 24 * N)}
+
+
 def run_ours(args, world, rank, local):
     from deepcharacters_b200 import _lib
     dev = torch.device("cuda", local)
@@ -212,6 +223,8 @@ def run_ours(args, world, rank, local):
     sc = make_workload(rank)
     ch = DeformRenderChain(sc, dev, FRAMES, VIEWS, RES, RES, W_SIL, W_SIL1)
     views_per_step = FRAMES * VIEWS
+    # autotuner: raster tile size and bin capacity (untimed)
+    tune = ch.autotune() if not args.no_autotune else {}
     # eager warm-up (allocates every workspace), then capture one step
     for _ in range(2):
         ch.step()
@@ -265,18 +278,32 @@ def run_ours(args, world, rank, local):
         stage_ms[name] = a.elapsed_time(b) / 3
     sbytes = stage_bytes(sc)
     N, F = sc["N"], sc["F"]
-    dom = max(stage_ms, key=stage_ms.get)
+    # per-kernel device time of the two raster kernels (events around each launch, eager)
+    ch.rend.set_kernel_timing(True)
+    kern_ms = {}
+    for _ in range(3):
+        ch.forward()
+        ch.backward()
+        kt = ch.rend.kernel_times()
+        for k in ("resolve", "render_grad"):
+            kern_ms.setdefault(k, []).append(kt[k])
+    ch.rend.set_kernel_timing(False)
+    kern_ms = {k: sum(v) / len(v) for k, v in kern_ms.items()}
+    kbytes = kernel_bytes(sc)
+    dom = max(kern_ms, key=kern_ms.get)
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    ach = sbytes[dom] / (stage_ms[dom] / 1e3) / 1e9
+    ach = kbytes[dom] / (kern_ms[dom] / 1e3) / 1e9
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = None
     if os.path.exists(traffic_path):
-        traffic = json.load(open(traffic_path)).get(dom)
+        tj = json.load(open(traffic_path)).get("k_" + dom)
+        if tj:  # ncu DRAM bytes per view of a smaller capture, scaled to this launch's views
+            traffic = tj["dram_bytes_per_view"] * FRAMES * VIEWS
 
     # e2e: public API, pinned host inputs copied every step, losses read back
     e2e = None if args.no_e2e else run_e2e(ch, sc, dev, args, world)
@@ -295,12 +322,14 @@ def run_ours(args, world, rank, local):
                    "nodes": N_NODES, "joints": 3 * N_SKEL,
                    "parallelism": f"frames sharded, {world} rank(s)",
                    "l2": "inputs larger than L2 (1.6 GB of target images per step)",
-                   "raster_tile": 8, "bin_capacity": 256},
+                   "raster_tile": ch.tuning[0], "bin_capacity": ch.tuning[1],
+                   "autotune_ms": {f"{t}x{c}": round(v, 3) for (t, c), v in tune.items()}},
         "e2e": e2e,
         "gpu_launches": int(launches_per_step * args.steps),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "traffic": traffic,
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
+                     "kernel_ms": kern_ms, "kernel_bytes": kbytes,
                      "stage_ms": stage_ms, "stage_bytes": sbytes,
                      "chain_bytes_per_view": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS),
                      "chain_frac": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS) * value / world / 1e9 / peak},
@@ -425,6 +454,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--frames", type=int, default=FRAMES, help="frames per rank (default 16; smaller for profiling)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default raster tiling (8 px, 256)")
     args = ap.parse_args()
     globals()["FRAMES"] = args.frames
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else max(args.warmup, 1)

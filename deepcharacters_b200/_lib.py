@@ -63,6 +63,8 @@ _SIGS: dict[str, list] = {
     "hc_sum_squares_loss": [vp, C.c_int64, vp, C.c_float, vp, vp, vp],
     "hc_add_inplace": [vp, C.c_int64, vp, vp],
     "hc_gaussian_smooth": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, vp, vp],
+    "hc_renderer_set_kernel_timing": [vp, C.c_int32],
+    "hc_renderer_kernel_times": [vp, vp, C.c_int32],
     "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
     "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
                              vp, vp, vp, vp],

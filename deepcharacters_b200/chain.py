@@ -64,6 +64,7 @@ class DeformRenderChain:
         self.eg.reserve(B)
         self.rend = RendererEngine(sc["faces"], sc["texcoords"], N, C, W, H, "vertexColor", "shadeless", 2, 2)
         self.rend.set_tuning(tile, bin_capacity)
+        self.tuning = (tile, bin_capacity)
         if gradient_parity:
             _lib.call("hc_renderer_set_gradient_parity", self.rend.handle, 1)
         self.rend.reserve(B)
@@ -150,6 +151,33 @@ class DeformRenderChain:
         if full:  # joint angles through the node skinning
             L("hc_pose2eg_backward", self.skin.handle, s, B, P(i["dofs"]), self.M, P(self.node_vertex),
               P(self.skin_w), P(o["gsT"]), P(o["gsA"]), P(o["gdofs"]))
+
+    def autotune(self, candidates=((8, 128), (8, 256), (16, 256), (16, 512), (32, 512), (32, 1024)), reps: int = 3):
+        """Pick the raster's bin-tile size and bin capacity by timing the
+        forward stage on the current inputs (CUDA events, after a warm-up
+        call per candidate); candidates whose spill capacity overflows are
+        skipped.  Sets the fastest and returns {(tile, cap): ms}."""
+        results = {}
+        for tile, cap in candidates:
+            self.rend.set_tuning(tile, cap)
+            self.rend.reserve(self.B)
+            try:
+                self.forward()
+                self.rend.stats()
+            except _lib.HcError:
+                continue
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                self.forward()
+            b.record()
+            torch.cuda.synchronize()
+            results[(tile, cap)] = a.elapsed_time(b) / reps
+        best = min(results, key=results.get)
+        self.rend.set_tuning(*best)
+        self.rend.reserve(self.B)
+        self.tuning = best
+        return results
 
     def step(self):
         self.forward()

@@ -240,8 +240,11 @@ __global__ void k_eg_grad_node(int B, int N, int M, int Mk, const float* __restr
                                const float* __restrict__ vnr, const NodeRT* __restrict__ tab, int full,
                                float* __restrict__ gT, float* __restrict__ gA, float* __restrict__ gsT,
                                float* __restrict__ gsA) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * M) return;
+    // one warp per (frame, node): lanes split the node's vertex list, then a
+    // warp reduction; lane 0 adds the marker term and writes
+    const long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= (long long)B * M) return;  // warp-uniform
     const int b = (int)(i / M), n = (int)(i % M);
     const float3 g = ld3(base + 3LL * node_vertex[n]);
     R33 da, db, dc;
@@ -251,7 +254,7 @@ __global__ void k_eg_grad_node(int B, int N, int M, int Mk, const float* __restr
     float3 t = make_float3(0.f, 0.f, 0.f), a = make_float3(0.f, 0.f, 0.f);
     float3 st = make_float3(0.f, 0.f, 0.f), sa = make_float3(0.f, 0.f, 0.f);
     const int off = n2v_off[n], cnt = n2v_size[n];
-    for (int k = 0; k < cnt; ++k) {
+    for (int k = lane; k < cnt; k += 32) {
         const int v = n2v_idx[off + k];
         const float w = n2v_w[off + k];
         const long long vi = (long long)b * N + v;
@@ -265,6 +268,24 @@ __global__ void k_eg_grad_node(int B, int N, int M, int Mk, const float* __restr
             sa += w * make_float3(dot(mv(sda, p), gvv), dot(mv(sdb, p), gvv), dot(mv(sdc, p), gvv));
         }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+        t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+        t.z += __shfl_xor_sync(0xffffffffu, t.z, o);
+        a.x += __shfl_xor_sync(0xffffffffu, a.x, o);
+        a.y += __shfl_xor_sync(0xffffffffu, a.y, o);
+        a.z += __shfl_xor_sync(0xffffffffu, a.z, o);
+        if (full) {
+            st.x += __shfl_xor_sync(0xffffffffu, st.x, o);
+            st.y += __shfl_xor_sync(0xffffffffu, st.y, o);
+            st.z += __shfl_xor_sync(0xffffffffu, st.z, o);
+            sa.x += __shfl_xor_sync(0xffffffffu, sa.x, o);
+            sa.y += __shfl_xor_sync(0xffffffffu, sa.y, o);
+            sa.z += __shfl_xor_sync(0xffffffffu, sa.z, o);
+        }
+    }
+    if (lane != 0) return;
     const int m = n2m ? n2m[n] : -1;
     if (m >= 0 && gm) {
         // marker residual (EmbeddedGraphGPUOpGrad.cu:90-123): weight 1, its own node
@@ -493,7 +514,7 @@ extern "C" hc_status hc_eg_backward(hc_eg h, void* stream, int32_t batch, const 
                                                      h->v2n_idx.as<int>(), h->v2n_w.as<float>(), tab,
                                                      deformed_vertices_grad, vertex_displacements_grad);
     HC_CHECK_LAUNCH();
-    k_eg_grad_node<<<div_up(BM, 128), 128, 0, s>>>(
+    k_eg_grad_node<<<div_up(BM * 32, 256), 256, 0, s>>>(
         batch, h->N, h->M, h->Mk, h->base.as<float>(), h->node_vertex.as<int>(), h->n2v_off.as<int>(),
         h->n2v_size.as<int>(), h->n2v_idx.as<int>(), h->n2v_w.as<float>(), h->n2m.as<int>(), h->markers.as<float>(),
         d_delta_a, d_skinned_a, deformed_vertices_grad, deformed_markers_grad, vertex_displacements_grad,

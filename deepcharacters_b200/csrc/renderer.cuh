@@ -174,6 +174,11 @@ constexpr float kEdgeMargin = 0.125f;
 struct Footprint {
     float a[3], b[3], c[3];  // edge k: a*x + b*y + c >= 0 inside (margin included)
 };
+// A pixel centre whose three footprint values are all >= kEdgeInterior lies
+// inside the (unwidened) projected triangle by more than kEdgeMargin px: the
+// exact ray test's edge and barycentric-window checks certainly pass there.
+// (A disabled footprint has values 0 and never qualifies.)
+constexpr float kEdgeInterior = 2.f * kEdgeMargin;
 
 __device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, float rel_margin = 0.f,
                                                float num_err = 0.f) {
@@ -198,12 +203,12 @@ __device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, 
         fp.b[k] = ex * inv;
         fp.c[k] = (ey * u.x - ex * u.y) * inv + margin;
     }
-    if (!ok) {
+    if (!ok) {  // disabled: every pixel is on the boundary band (passes, never "inside")
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             fp.a[k] = 0.f;
             fp.b[k] = 0.f;
-            fp.c[k] = 1.f;
+            fp.c[k] = 0.f;
         }
     }
     return fp;
@@ -255,6 +260,27 @@ struct UvTable {
     DevBuf faces, table;
 };
 
+// Optional per-kernel timing of the renderer (CUDA events around each
+// launch on the launching stream), for benchmarks; off by default.
+enum RendererKernel {
+    kKViewSetup = 0, kKVertexNormals, kKTriFrame, kKBin, kKSpill, kKResolve, kKRenderGrad, kKNormalChain,
+    kKCount
+};
+
+struct KernelClock {
+    bool on = false, made = false;
+    cudaEvent_t ev[2 * kKCount];
+    unsigned recorded = 0;  // kernels with both events recorded since the last read
+    void begin(int k, cudaStream_t s) {
+        if (on) cudaEventRecord(ev[2 * k], s);
+    }
+    void end(int k, cudaStream_t s) {
+        if (!on) return;
+        cudaEventRecord(ev[2 * k + 1], s);
+        recorded |= 1u << k;
+    }
+};
+
 struct RasterWorkspace {
     int cap_views = 0;   // views the buffers are sized for
     int tile = 16;
@@ -263,6 +289,7 @@ struct RasterWorkspace {
     long long spill_cap = 0;
     int spill_tile_cap = 0;
     DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;
+    KernelClock clock;
 };
 
 }  // namespace hc

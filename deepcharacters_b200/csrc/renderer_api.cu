@@ -161,6 +161,9 @@ extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, 
 }
 
 static void release_all(hc_renderer_s* r) {
+    if (r->ws.clock.made)
+        for (cudaEvent_t& e : r->ws.clock.ev) cudaEventDestroy(e);
+    r->ws.clock.made = false;
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
                       &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
@@ -285,5 +288,33 @@ extern "C" hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t pari
     clear_error();
     HC_REQUIRE(h, "invalid handle");
     h->grad_parity = parity ? 1 : 0;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_renderer_set_kernel_timing(hc_renderer h, int32_t enable) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    KernelClock& c = h->ws.clock;
+    if (enable && !c.made) {
+        for (cudaEvent_t& e : c.ev) HC_CUDA(cudaEventCreate(&e));
+        c.made = true;
+    }
+    c.on = enable != 0;
+    c.recorded = 0;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_renderer_kernel_times(hc_renderer h, float* ms, int32_t n) {
+    clear_error();
+    HC_REQUIRE(h && ms && n >= 0, "invalid arguments");
+    KernelClock& c = h->ws.clock;
+    for (int k = 0; k < n; ++k) {
+        ms[k] = -1.f;
+        if (k < kKCount && c.made && (c.recorded >> k & 1u)) {
+            HC_CUDA(cudaEventSynchronize(c.ev[2 * k + 1]));
+            HC_CUDA(cudaEventElapsedTime(&ms[k], c.ev[2 * k], c.ev[2 * k + 1]));
+        }
+    }
+    c.recorded = 0;
     return HC_OK;
 }

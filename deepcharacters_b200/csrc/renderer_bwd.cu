@@ -155,14 +155,35 @@ constexpr int TILE_S = BT + 2 * MAXFS;   // staged target tile edge
 
 constexpr int MAXTAPS = (2 * MAXFS + 1) * (2 * MAXFS + 1);
 
+// G . dTarget/d(u, v) over the staged (2 FS + 1)^2 window for a compile-time
+// filter size: the weights (i, j) / (i^2 + j^2) fold to the same correctly
+// rounded constants the per-CTA table holds, and the taps are summed in the
+// same (row, column) order, so both paths give identical results.
+template <int FS>
+__device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, float& gu, float& gv) {
+    constexpr int e = BT + 2 * FS;
+#pragma unroll
+    for (int j = -FS; j <= FS; ++j)
+#pragma unroll
+        for (int i = -FS; i <= FS; ++i) {
+            const float den = (float)(i * i + j * j);
+            const float wi = den == 0.f ? 0.f : (float)i / den, wj = den == 0.f ? 0.f : (float)j / den;
+            const float4 I = s_tgt[s0 + (j + FS) * e + (i + FS)];
+            const float gi = G.x * I.x + G.y * I.y + G.z * I.z;
+            gu += gi * wi;
+            gv += gi * wj;
+        }
+}
+
 // Albedo classes of the adjoint: vertex colours, texture, and the modes
 // whose albedo has no parameters (normal, lighting, mask, position, depth, uv).
 enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2 };
 
 template <bool SHADED, int ALB, bool PARITY>
-__global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams) {
-    constexpr int NV = SHADED ? 9 : 6;  // per-vertex values merged in the warp
-    __shared__ float s_red[BNT / 32][32][NV];
+__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams) {
+    constexpr int NVV = SHADED ? 9 : 6;               // values per vertex
+    constexpr int NROW = (3 * NVV + 3) / 4 * 4;       // per-lane row, padded for float4 loads
+    __shared__ __align__(16) float s_red[BNT / 32][32][NROW];
     __shared__ float s_sh[SHADED ? BNT / 32 : 1][27];
     __shared__ float4 s_tgt[TILE_S * TILE_S];
     __shared__ float2 s_tap[MAXTAPS];  // image-gradient tap weights (i, j) / (i^2 + j^2)
@@ -183,10 +204,19 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         const int e = BT + 2 * A.ifs;
         for (int i = threadIdx.x; i < e * e; i += BNT) {
             const int yy = ty0 - A.ifs + i / e, xx = tx0 - A.ifs + i % e;
-            float3 v = make_float3(0.f, 0.f, 0.f);
-            if (xx >= 0 && yy >= 0 && xx < A.W && yy < A.H) v = ld3(tgt + 3 * ((long long)yy * A.W + xx));
-            s_tgt[i] = make_float4(v.x, v.y, v.z, 0.f);
+            // asynchronous copies: the pixel work below that does not read the
+            // target overlaps them; they are waited for before the taps
+            if (xx >= 0 && yy >= 0 && xx < A.W && yy < A.H) {
+                const float* src = tgt + 3 * ((long long)yy * A.W + xx);
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(&s_tgt[i]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4), "l"(src + 1));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8), "l"(src + 2));
+            } else {
+                s_tgt[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
         }
+        asm volatile("cp.async.commit_group;\n" ::);
         // tap weights and their normaliser, once per CTA: the same divisions
         // and the same summation order as evaluating them per pixel
         const int fs = A.ifs, ew = 2 * fs + 1;
@@ -205,7 +235,6 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             s_norm = norm;
         }
     }
-    __syncthreads();
     float shg[SHADED ? 27 : 1];
 #pragma unroll
     for (int k = 0; k < (SHADED ? 27 : 1); ++k) shg[k] = 0.f;
@@ -217,9 +246,12 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
 #pragma unroll
     for (int k = 0; k < 9; ++k) gp[k] = 0.f;
     float3 gA = make_float3(0.f, 0.f, 0.f), gnu = make_float3(0.f, 0.f, 0.f);
+    // carried from the first half of the pixel work (no target reads) to the second
+    const ViewCam& cam = cams[view];
+    float3 d = make_float3(0.f, 0.f, 1.f), v0 = d, v1 = d, v2 = d, G = d, frag = d;
+    float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
     if (f >= 0) {
-        const ViewCam& cam = cams[view];
-        const float3 d = pixel_ray(cam, px, py);
+        d = pixel_ray(cam, px, py);
         const float ba = A.bary[2 * pix], bb = A.bary[2 * pix + 1];
         const float bc = 1.f - ba - bb;
         const int3 id = A.faces[f];
@@ -230,11 +262,13 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         bw[1] = bb;
         bw[2] = bc;
         const float* P = A.verts + (long long)b * A.N * 3;
-        const float3 v0 = ld3(P + 3 * id.x), v1 = ld3(P + 3 * id.y), v2 = ld3(P + 3 * id.z);
+        v0 = ld3(P + 3 * id.x);
+        v1 = ld3(P + 3 * id.y);
+        v2 = ld3(P + 3 * id.z);
         const float* VN = A.vnormal + (long long)view * A.N * 3;
         const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
-        const float3 G = ld3(A.grad + 3 * pix);
-        const float3 frag = ba * v0 + bb * v1 + bc * v2;
+        G = ld3(A.grad + 3 * pix);
+        frag = ba * v0 + bb * v1 + bc * v2;
         const float3 pnu = ba * n0 + bb * n1 + bc * n2;
         const float pnv = sqrtf(pnu.x * pnu.x + pnu.y * pnu.y + pnu.z * pnu.z);
         float3 pn = pnu / pnv;
@@ -248,7 +282,6 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         float3 coal = make_float3(1.f, 1.f, 1.f);
         if constexpr (SHADED) coal = sh_illum(sh, pn);
         gA = G * coal;  // d loss / d albedo
-        float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
         const float* tcp = A.texcoords + (long long)f * 6;
         if constexpr (vcol) {
             const float* Cc = A.colors + (long long)b * A.N * 3;
@@ -311,6 +344,10 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
             gnu = (gno * v2n - pnu * gu) / v3n;
             gbc += make_float3(dot(gnu, n0), dot(gnu, n1), dot(gnu, n2));
         }
+    }
+    if (staged) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    if (f >= 0) {
         // model -> data: -G^T dTarget/d(u,v) d(u,v)/d(frag) d(frag)/d(v)
         float3 m = make_float3(0.f, 0.f, 0.f);
         {
@@ -322,14 +359,20 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
                 if (staged) {
                     const int e = BT + 2 * fs, ew = 2 * fs + 1;
                     const int s0 = (py - ty0) * e + (px - tx0);
-                    for (int j = 0; j < ew; ++j)
-                        for (int i = 0; i < ew; ++i) {
-                            const float2 w = s_tap[j * ew + i];
-                            const float4 I = s_tgt[s0 + j * e + i];
-                            const float gi = G.x * I.x + G.y * I.y + G.z * I.z;
-                            gu += gi * w.x;
-                            gv += gi * w.y;
-                        }
+                    switch (fs) {
+                        case 1: taps_fs<1>(s_tgt, s0, G, gu, gv); break;
+                        case 2: taps_fs<2>(s_tgt, s0, G, gu, gv); break;
+                        case 3: taps_fs<3>(s_tgt, s0, G, gu, gv); break;
+                        default:
+                            for (int j = 0; j < ew; ++j)
+                                for (int i = 0; i < ew; ++i) {
+                                    const float2 w = s_tap[j * ew + i];
+                                    const float4 I = s_tgt[s0 + j * e + i];
+                                    const float gi = G.x * I.x + G.y * I.y + G.z * I.z;
+                                    gu += gi * w.x;
+                                    gv += gi * w.y;
+                                }
+                    }
                     gu /= s_norm;
                     gv /= s_norm;
                 } else {
@@ -398,50 +441,61 @@ __global__ void __launch_bounds__(BNT) k_render_grad(BwdArgs A, int tiles_x, con
         }
     }
     // per-vertex contributions, merged inside the warp: lanes are matched by
-    // vertex id and the lowest lane of each group sums the group's values
-    // from shared memory and issues one reduction per value
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
+    // face id (a face fixes all three vertices) and the lowest lane of each
+    // group sums the group's rows from shared memory and issues one reduction
+    // per value and vertex
+    {
         float* row = s_red[warp][lane];
-        row[0] = gp[3 * i];
-        row[1] = gp[3 * i + 1];
-        row[2] = gp[3 * i + 2];
-        row[3] = gA.x * bw[i];
-        row[4] = gA.y * bw[i];
-        row[5] = gA.z * bw[i];
-        if constexpr (SHADED) {
-            row[6] = gnu.x * bw[i];
-            row[7] = gnu.y * bw[i];
-            row[8] = gnu.z * bw[i];
-        }
-        __syncwarp();
-        const int key = vid[i];
-        const unsigned grp = __match_any_sync(0xffffffffu, key);
-        if (key >= 0 && lane == __ffs(grp) - 1) {
-            float acc[NV];
 #pragma unroll
-            for (int k = 0; k < NV; ++k) acc[k] = 0.f;
-            for (unsigned mm = grp; mm; mm &= mm - 1) {
-                const float* r = s_red[warp][__ffs(mm) - 1];
-#pragma unroll
-                for (int k = 0; k < NV; ++k) acc[k] += r[k];
-            }
-            const long long o3 = ((long long)b * A.N + key) * 3;
-            atomicAdd(A.vpos_grad + o3 + 0, acc[0]);
-            atomicAdd(A.vpos_grad + o3 + 1, acc[1]);
-            atomicAdd(A.vpos_grad + o3 + 2, acc[2]);
-            if constexpr (vcol) {
-                atomicAdd(A.vcol_grad + o3 + 0, acc[3]);
-                atomicAdd(A.vcol_grad + o3 + 1, acc[4]);
-                atomicAdd(A.vcol_grad + o3 + 2, acc[5]);
-            }
+        for (int i = 0; i < 3; ++i) {
+            row[NVV * i + 0] = gp[3 * i];
+            row[NVV * i + 1] = gp[3 * i + 1];
+            row[NVV * i + 2] = gp[3 * i + 2];
+            row[NVV * i + 3] = gA.x * bw[i];
+            row[NVV * i + 4] = gA.y * bw[i];
+            row[NVV * i + 5] = gA.z * bw[i];
             if constexpr (SHADED) {
-                atomicAdd(A.nrm_grad + o3 + 0, acc[NV - 3]);
-                atomicAdd(A.nrm_grad + o3 + 1, acc[NV - 2]);
-                atomicAdd(A.nrm_grad + o3 + 2, acc[NV - 1]);
+                row[NVV * i + 6] = gnu.x * bw[i];
+                row[NVV * i + 7] = gnu.y * bw[i];
+                row[NVV * i + 8] = gnu.z * bw[i];
             }
         }
         __syncwarp();
+        const unsigned grp = __match_any_sync(0xffffffffu, f);
+        if (f >= 0 && lane == __ffs(grp) - 1) {
+            float4 acc[NROW / 4];
+#pragma unroll
+            for (int k = 0; k < NROW / 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+            for (unsigned mm = grp; mm; mm &= mm - 1) {
+                const float4* r = reinterpret_cast<const float4*>(s_red[warp][__ffs(mm) - 1]);
+#pragma unroll
+                for (int k = 0; k < NROW / 4; ++k) {
+                    const float4 x = r[k];
+                    acc[k].x += x.x;
+                    acc[k].y += x.y;
+                    acc[k].z += x.z;
+                    acc[k].w += x.w;
+                }
+            }
+            const float* a = reinterpret_cast<const float*>(acc);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const long long o3 = ((long long)b * A.N + vid[i]) * 3;
+                atomicAdd(A.vpos_grad + o3 + 0, a[NVV * i + 0]);
+                atomicAdd(A.vpos_grad + o3 + 1, a[NVV * i + 1]);
+                atomicAdd(A.vpos_grad + o3 + 2, a[NVV * i + 2]);
+                if constexpr (vcol) {
+                    atomicAdd(A.vcol_grad + o3 + 0, a[NVV * i + 3]);
+                    atomicAdd(A.vcol_grad + o3 + 1, a[NVV * i + 4]);
+                    atomicAdd(A.vcol_grad + o3 + 2, a[NVV * i + 5]);
+                }
+                if constexpr (SHADED) {
+                    atomicAdd(A.nrm_grad + o3 + 0, a[NVV * i + 6]);
+                    atomicAdd(A.nrm_grad + o3 + 1, a[NVV * i + 7]);
+                    atomicAdd(A.nrm_grad + o3 + 2, a[NVV * i + 8]);
+                }
+            }
+        }
     }
     // SH: reduce over the CTA, one atomic per coefficient
     if constexpr (SHADED) {
@@ -541,6 +595,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
     const int tiles_x = div_up(W, BT), tiles_y = div_up(H, BT);
     const dim3 grid(tiles_x * tiles_y, V);
+    ws.clock.begin(kKRenderGrad, s);
     const int alb = albedo == kVertexColor ? kAlbVcol : albedo == kTextured ? kAlbTex : kAlbNone;
     const int sel = (shaded ? 6 : 0) + alb * 2 + (parity ? 1 : 0);
     switch (sel) {
@@ -561,11 +616,14 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
 #undef HC_GRAD_CASE
     }
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKRenderGrad, s);
     if (shaded) {
+        ws.clock.begin(kKNormalChain, s);
         k_normal_chain<<<div_up((long long)B * N, 256), 256, 0, s>>>(B, N, topo.faces.as<int3>(), topo.vf.as<int>(),
                                                                      topo.vf_id.as<int2>(), verts, nrm_ws.as<float>(),
                                                                      vpos_grad);
         HC_CHECK_LAUNCH();
+        ws.clock.end(kKNormalChain, s);
     }
     return HC_OK;
 }

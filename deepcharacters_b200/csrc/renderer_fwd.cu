@@ -484,7 +484,7 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : 1) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
                                                    const TriView* __restrict__ tri_view,
@@ -495,7 +495,8 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : 1) k_resolve(ShadeArgs 
     constexpr int NT = TS * TS;
     constexpr int CHUNK = NT > 256 ? 256 : NT;  // triangles staged per round
     __shared__ TileTri s_tri[CHUNK];
-    __shared__ int s_count[2];
+    __shared__ unsigned long long s_key[CHUNK];  // facing | depth lower bound | slot
+    __shared__ unsigned short s_order[CHUNK];    // slots in key order
     const int tile = blockIdx.x;
     const int view = blockIdx.y;
     const int b = view / A.C;
@@ -514,70 +515,96 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : 1) k_resolve(ShadeArgs 
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
-    // Each staged chunk is split into its front-facing triangles (from the
-    // start) and back-facing ones (from the end).  All front faces are tested
-    // first, then the back faces: a triangle whose depth lower bound exceeds
-    // the pixel's current best depth can neither win nor tie, so once the
-    // front surface is resolved most back faces are rejected by one compare.
-    // The result is the same minimum (depth, id) as one unordered pass.
-    // Per pixel a triangle is only tested when the pixel lies in the
-    // triangle's bounding box, kept as a column and a row bit mask relative
-    // to the tile.
+    // Each staged chunk is sorted by (back-facing, depth lower bound).  All
+    // front faces are tested first, nearest bound first, then the back faces.
+    // A triangle whose depth lower bound exceeds the pixel's current best
+    // depth can neither win nor tie, and neither can any triangle after it in
+    // the same run, so a pixel stops scanning a run there.  The result is the
+    // same minimum (depth, id) as one unordered pass.  Per pixel a triangle
+    // is only tested when the pixel lies in its bounding box (a column and a
+    // row bit mask relative to the tile) and in its conservative footprint.
     int n_front = 0;
     for (int pass = 0; pass < 2; ++pass) {
         for (int base = 0; base < n; base += CHUNK) {
             const int m = min(CHUNK, n - base);
             if (pass == 0 || n > CHUNK) {
                 __syncthreads();
-                if (threadIdx.x < 2) s_count[threadIdx.x] = 0;
-                __syncthreads();
                 const int k = base + threadIdx.x;
-                if (threadIdx.x < CHUNK && k < m + base) {
-                    const int f = tb[k];
-                    const TriView tv = tri_view[(long long)view * A.F + f];
-                    const bool back = tv.dqmin < 0;
-                    const int slot = back ? m - 1 - atomicAdd(&s_count[1], 1) : atomicAdd(&s_count[0], 1);
-                    const TriFrame tf = tri_frame[(long long)b * A.F + f];
-                    const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
-                    const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
-                    const float3 q0 = project_point(cam.ext, cam.intr, make_float3(tf.a.x, tf.a.y, tf.a.z) * 1000.f);
-                    const float3 q1 = project_point(cam.ext, cam.intr, make_float3(tf.b.x, tf.b.y, tf.b.z) * 1000.f);
-                    const float3 q2 = project_point(cam.ext, cam.intr, make_float3(tf.c.x, tf.c.y, tf.c.z) * 1000.f);
-                    const Footprint fp = footprint(q0, q1, q2);
-                    TileTri t;
-                    t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
-                                      (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
-                                      tv.dqmin & 0x7fffffff, f);
-                    t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
-                    t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
-                    t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
-                    t.a = tf.a;
-                    t.b = tf.b;
-                    t.c = tf.c;
-                    s_tri[slot] = t;
+                bool front = false;
+                if (threadIdx.x < CHUNK) {
+                    unsigned long long key = ~0ull;
+                    if (k < m + base) {
+                        const int f = tb[k];
+                        const TriView tv = tri_view[(long long)view * A.F + f];
+                        front = tv.dqmin >= 0;
+                        const TriFrame tf = tri_frame[(long long)b * A.F + f];
+                        const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
+                        const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
+                        const float3 q0 =
+                            project_point(cam.ext, cam.intr, make_float3(tf.a.x, tf.a.y, tf.a.z) * 1000.f);
+                        const float3 q1 =
+                            project_point(cam.ext, cam.intr, make_float3(tf.b.x, tf.b.y, tf.b.z) * 1000.f);
+                        const float3 q2 =
+                            project_point(cam.ext, cam.intr, make_float3(tf.c.x, tf.c.y, tf.c.z) * 1000.f);
+                        const Footprint fp = footprint(q0, q1, q2);
+                        TileTri t;
+                        t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
+                                          (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
+                                          tv.dqmin & 0x7fffffff, f);
+                        t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
+                        t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
+                        t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
+                        t.a = tf.a;
+                        t.b = tf.b;
+                        t.c = tf.c;
+                        s_tri[threadIdx.x] = t;
+                        key = ((unsigned long long)(front ? 0u : 1u) << 62) |
+                              ((unsigned long long)(unsigned)(tv.dqmin & 0x7fffffff) << 16) | threadIdx.x;
+                    }
+                    s_key[threadIdx.x] = key;  // unused keys (beyond m) are never ranked or read
+                }
+                n_front = __syncthreads_count(front);
+                // sort by rank: keys are distinct (the slot is part of the key)
+                if ((int)threadIdx.x < m) {
+                    const unsigned long long mine = s_key[threadIdx.x];
+                    int rank = 0;
+                    for (int q = 0; q < m; ++q) rank += s_key[q] < mine;
+                    s_order[rank] = (unsigned short)threadIdx.x;
                 }
                 __syncthreads();
-                n_front = s_count[0];
             }
             const int j0 = pass == 0 ? 0 : n_front;
             const int j1 = pass == 0 ? n_front : m;
             if (valid) {
                 for (int j = j0; j < j1; ++j) {
+                    const int slot = s_order[j];
                     // one 16-byte header load decides whether the ray test runs
-                    const int4 h = s_tri[j].hdr;
+                    const int4 h = s_tri[slot].hdr;
+                    if ((unsigned)h.z > best_d) break;  // neither this nor a later one can reach the best depth
                     if (!((unsigned)h.x & col_bit) || !((unsigned)h.y & row_bit)) continue;
-                    if ((unsigned)h.z > best_d) continue;  // cannot reach the best depth
-                    const float4 ea = s_tri[j].ea, nm = s_tri[j].nm, eb = s_tri[j].eb;
-                    if (ea.x * cx + ea.y * cy + nm.y < 0.f || ea.z * cx + ea.w * cy + nm.z < 0.f ||
-                        eb.x * cx + eb.y * cy + nm.w < 0.f)
-                        continue;  // pixel centre clearly outside the projected triangle
-                    TriFrame tf;
-                    tf.a = s_tri[j].a;
-                    tf.b = s_tri[j].b;
-                    tf.c = s_tri[j].c;
+                    const float4 ea = s_tri[slot].ea, nm = s_tri[slot].nm, eb = s_tri[slot].eb;
+                    const float e0 = ea.x * cx + ea.y * cy + nm.y, e1 = ea.z * cx + ea.w * cy + nm.z,
+                                e2 = eb.x * cx + eb.y * cy + nm.w;
+                    if (e0 < 0.f || e1 < 0.f || e2 < 0.f) continue;  // clearly outside the projected triangle
                     int dq;
-                    float a, bb;
-                    if (!raster_hit_below(ro_s, dir, tri_from(tf), nm.x, best_d, dq, a, bb)) continue;
+                    if (e0 >= kEdgeInterior && e1 >= kEdgeInterior && e2 >= kEdgeInterior) {
+                        // clearly inside: the edge tests would pass, only the depth is needed
+                        // (the same operations as ray_tri up to t)
+                        const float3 n = make_float3(s_tri[slot].a.w, s_tri[slot].b.w, s_tri[slot].c.w);
+                        const float ndr = dot(dir, n);
+                        if (fabsf(ndr) < 0.0000001f) continue;
+                        const float t = nm.x / ndr;
+                        if (t < 0.f) continue;
+                        dq = (int)(t * 10000.f);
+                        if ((unsigned)dq > best_d) continue;
+                    } else {
+                        TriFrame tf;
+                        tf.a = s_tri[slot].a;
+                        tf.b = s_tri[slot].b;
+                        tf.c = s_tri[slot].c;
+                        float a, bb;
+                        if (!raster_hit_below(ro_s, dir, tri_from(tf), nm.x, best_d, dq, a, bb)) continue;
+                    }
                     const int f = h.w;
                     if ((unsigned)dq < best_d) {
                         best_d = (unsigned)dq;
@@ -681,22 +708,32 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
 
     HC_CUDA(cudaMemsetAsync(tstate, 0, sizeof(int2) * (size_t)V * T, s));
     HC_CUDA(cudaMemsetAsync(stats, 0, sizeof(RasterStats), s));
+    ws.clock.begin(kKViewSetup, s);
     k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, extr, intr, cams);
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKViewSetup, s);
+    ws.clock.begin(kKVertexNormals, s);
     k_vertex_normals<<<div_up((long long)B * N, 256), 256, 0, s>>>(
         B, C, N, topo.faces.as<int3>(), topo.vf.as<int>(), topo.vf_id.as<int2>(), verts, vnormal);
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKVertexNormals, s);
+    ws.clock.begin(kKTriFrame, s);
     k_tri_frame<<<div_up((long long)B * F, 256), 256, 0, s>>>(B, F, N, topo.faces.as<int3>(), verts, tf);
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKTriFrame, s);
+    ws.clock.begin(kKBin, s);
     k_bin<<<div_up((long long)V * F, 256), 256, 0, s>>>(
         V, C, F, N, W, H, TS, ws.tiles_x, ws.tiles_y, ws.bin_cap, topo.faces.as<int3>(), verts, cams, tf, tv, tstate,
         ws.bins.as<int>(), ws.spill.as<int4>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(),
         ws.spill_tile_cap, stats);
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKBin, s);
+    ws.clock.begin(kKSpill, s);
     k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
                                     ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(), stats,
                                     nullptr, nullptr, T);
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKSpill, s);
     ShadeArgs A;
     A.B = B;
     A.C = C;
@@ -721,6 +758,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.depth_q = depth_q;
     A.tie_count = tie_count;
     const dim3 grid(T, V);
+    ws.clock.begin(kKResolve, s);
     switch (TS) {
         case 8:
             k_resolve<8><<<grid, 64, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate, ws.bins.as<int>(),
@@ -739,6 +777,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
             HC_FAIL(HC_ERR_INVALID, "unsupported tile size %d", TS);
     }
     HC_CHECK_LAUNCH();
+    ws.clock.end(kKResolve, s);
     if (tie_count && depth_q) {
         k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
                                         ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(),

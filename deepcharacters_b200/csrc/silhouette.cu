@@ -136,18 +136,10 @@ __global__ void k_boundary(int B, int C, int N, int W, int H, const float* __res
 // triangle's clamped bounding box whose centre has image-space barycentrics
 // within [-0.001, 1.001] is marked covered.  The barycentric expressions keep
 // the reference's operation order, so coverage is bit-identical; only
-// "covered" is ever written, so the unordered stores need no atomics.
-//
-// Deformed meshes mix long thin triangles whose boxes span 10^4 pixels with
-// triangles of a few pixels, and the reference's one-thread-per-triangle loop
-// leaves most lanes idle.  Here each thread takes a (view, triangle); boxes of
-// up to kCoverSmall pixels are swept by their own thread, larger ones are
-// queued in the warp (ballot) and swept by the whole warp, one row per lane.
-// A row only visits the pixels between the edges of the triangle's
-// conservative footprint (widened by the -0.001 tolerance and the test's
-// rounding error, see Footprint), so a thin triangle costs its area, not its
-// box.  Skipped pixels cannot pass the exact test.
-constexpr int kCoverSmall = 64;
+// "covered" is ever written, so unordered stores need no atomics.  Pixels
+// outside a triangle's conservative footprint (widened by the -0.001
+// tolerance and the test's rounding error, see Footprint) are never tested
+// against it: they cannot pass the exact test.
 
 struct CoverTri {
     float2 a, b, c;
@@ -168,30 +160,6 @@ __device__ __forceinline__ bool fp_inside(const Footprint& fp, float pu, float p
            fp.a[2] * pu + fp.b[2] * pv + fp.c[2] >= 0.f;
 }
 
-// pixel columns of row v whose centres can be inside the footprint
-__device__ __forceinline__ void fp_span(const Footprint& fp, float pv, int x0, int x1, int& u0, int& u1) {
-    float lo = x0 + 0.5f, hi = x1 + 0.5f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float r = fp.b[k] * pv + fp.c[k];  // need a x + r >= 0
-        if (fabsf(fp.a[k]) < 1e-12f) {
-            if (r < 0.f) hi = -1e30f;
-        } else if (fp.a[k] > 0.f) {
-            lo = fmaxf(lo, -r / fp.a[k]);
-        } else {
-            hi = fminf(hi, -r / fp.a[k]);
-        }
-    }
-    if (!(lo <= hi)) {
-        u0 = 1;
-        u1 = 0;
-        return;
-    }
-    // one extra column on each side absorbs the rounding of the bounds
-    u0 = max(x0, (int)floorf(lo - 0.5f) - 1);
-    u1 = min(x1, (int)ceilf(hi - 0.5f) + 1);
-}
-
 __device__ __forceinline__ Footprint cover_footprint(const CoverTri& t, int W, int H) {
     const float M = fmaxf(fmaxf(fmaxf(fabsf(t.a.x), fabsf(t.a.y)), fmaxf(fabsf(t.b.x), fabsf(t.b.y))),
                           fmaxf(fmaxf(fabsf(t.c.x), fabsf(t.c.y)), (float)max(W, H)));
@@ -199,47 +167,89 @@ __device__ __forceinline__ Footprint cover_footprint(const CoverTri& t, int W, i
                      0.0011f, 2e-6f * M * M);
 }
 
-__global__ void k_cover(int B, int C, int N, int F, int W, int H, const int* __restrict__ faces,
-                        const float2* __restrict__ p2d, unsigned char* __restrict__ cover) {
+// Binned coverage.  The reference's one-thread-per-triangle sweep costs the
+// summed box area of all triangles (10^4-pixel boxes of long thin triangles
+// on deformed meshes, with most lanes idle); the coverage of a pixel only
+// needs the first triangle that covers it.  So, as for the renderer, triangles are binned into 8x8-pixel
+// tiles (the tiles their footprint reaches), and one CTA per tile tests each
+// pixel against the tile's triangles until one covers it.  Pairs beyond a
+// tile's bin capacity are swept at once by the binning thread (coverage is an
+// OR of triangles, so any order of writes gives the same image).
+constexpr int kCovTile = 8;
+constexpr int kCovCap = 256;
+
+__device__ __forceinline__ void cover_tri(int view, int f, int N, int W, int H, const int* __restrict__ faces,
+                                          const float2* __restrict__ p2d, CoverTri& t) {
+    const float2* P = p2d + (long long)view * N;
+    t.a = P[faces[3 * f]];
+    t.b = P[faces[3 * f + 1]];
+    t.c = P[faces[3 * f + 2]];
+    const float2 a = t.a, b = t.b, c = t.c;
+    t.x0 = (int)fmaxf(fminf(a.x, fminf(b.x, c.x)) - 0.5f, 0);
+    t.y0 = (int)fmaxf(fminf(a.y, fminf(b.y, c.y)) - 0.5f, 0);
+    t.x1 = (int)fminf(fmaxf(a.x, fmaxf(b.x, c.x)) + 0.5f, W - 1);
+    t.y1 = (int)fminf(fmaxf(a.y, fmaxf(b.y, c.y)) + 0.5f, H - 1);
+    t.d2 = (a.y - b.y) * c.x + (b.x - a.x) * c.y + a.x * b.y - b.x * a.y;
+    t.d1 = (a.y - c.y) * b.x + (c.x - a.x) * b.y + a.x * c.y - c.x * a.y;
+}
+
+struct CovBins {
+    int tiles_x, T;
+    int* count;  // [V*T]
+    int* bins;   // [V*T*kCovCap]
+    unsigned char* cover;
+    int W, H;
+};
+
+// append (tile, triangle) or, beyond the bin capacity, sweep the pair now
+__device__ __forceinline__ void cov_place(const CovBins& cb, int view, int tile, int f, const CoverTri& t,
+                                          const Footprint& fp) {
+    const long long key = (long long)view * cb.T + tile;
+    const int slot = atomicAdd(cb.count + key, 1);
+    if (slot < kCovCap) {
+        cb.bins[key * kCovCap + slot] = f;
+        return;
+    }
+    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+    unsigned char* img = cb.cover + (long long)view * cb.H * cb.W;
+    for (int v = max(t.y0, ty * kCovTile); v <= min(t.y1, ty * kCovTile + kCovTile - 1); ++v)
+        for (int u = max(t.x0, tx * kCovTile); u <= min(t.x1, tx * kCovTile + kCovTile - 1); ++u) {
+            const float pu = u + 0.5f, pv = v + 0.5f;
+            if (fp_inside(fp, pu, pv) && cover_test(t, pu, pv)) img[(long long)v * cb.W + u] = 1;
+        }
+}
+
+__global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
+                          CovBins cb) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const bool live = i < (long long)B * C * F;
-    long long view = 0;
+    const bool live = i < (long long)V * F;
+    int view = 0, f = 0;
     CoverTri t;
     t.x0 = 0;
     t.x1 = -1;
     t.y0 = 0;
     t.y1 = -1;
+    Footprint fp;
     if (live) {
-        view = i / F;
-        const int f = (int)(i % F);
-        const float2* P = p2d + view * N;
-        t.a = P[faces[3 * f]];
-        t.b = P[faces[3 * f + 1]];
-        t.c = P[faces[3 * f + 2]];
-        const float2 a = t.a, b = t.b, c = t.c;
-        t.x0 = (int)fmaxf(fminf(a.x, fminf(b.x, c.x)) - 0.5f, 0);
-        t.y0 = (int)fmaxf(fminf(a.y, fminf(b.y, c.y)) - 0.5f, 0);
-        t.x1 = (int)fminf(fmaxf(a.x, fmaxf(b.x, c.x)) + 0.5f, W - 1);
-        t.y1 = (int)fminf(fmaxf(a.y, fmaxf(b.y, c.y)) + 0.5f, H - 1);
-        t.d2 = (a.y - b.y) * c.x + (b.x - a.x) * c.y + a.x * b.y - b.x * a.y;
-        t.d1 = (a.y - c.y) * b.x + (c.x - a.x) * b.y + a.x * c.y - c.x * a.y;
+        view = (int)(i / F);
+        f = (int)(i % F);
+        cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
+        fp = cover_footprint(t, cb.W, cb.H);
     }
     const bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
-    const long long box = nonempty ? (long long)(t.x1 - t.x0 + 1) * (t.y1 - t.y0 + 1) : 0;
-    const bool big = box > kCoverSmall;
+    const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
+    const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
+    const int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
+    const bool big = nt > 4;
     if (nonempty && !big) {
-        const Footprint fp = cover_footprint(t, W, H);
-        unsigned char* img = cover + view * H * W;
-        for (int v = t.y0; v <= t.y1; ++v) {
-            const float pv = v + 0.5f;
-            for (int u = t.x0; u <= t.x1; ++u) {
-                const float pu = u + 0.5f;
-                if (fp_inside(fp, pu, pv) && cover_test(t, pu, pv)) img[(long long)v * W + u] = 1;
-            }
+        for (int k = 0; k < nt; ++k) {
+            const int tx = tx0 + k % ntx, ty = ty0 + k / ntx;
+            if (nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
+                                              max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1)))
+                cov_place(cb, view, ty * cb.tiles_x + tx, f, t, fp);
         }
     }
-    // large boxes: the warp sweeps them one at a time, a row per lane
     unsigned pending = __ballot_sync(0xffffffffu, big);
     while (pending) {
         const int src = __ffs(pending) - 1;
@@ -254,17 +264,80 @@ __global__ void k_cover(int B, int C, int N, int F, int W, int H, const int* __r
         q.x1 = __shfl_sync(0xffffffffu, t.x1, src);
         q.y0 = __shfl_sync(0xffffffffu, t.y0, src);
         q.y1 = __shfl_sync(0xffffffffu, t.y1, src);
-        const long long qv = __shfl_sync(0xffffffffu, view, src);
-        const Footprint fp = cover_footprint(q, W, H);
-        unsigned char* img = cover + qv * H * W;
-        for (int v = q.y0 + lane; v <= q.y1; v += 32) {
-            const float pv = v + 0.5f;
-            int u0, u1;
-            fp_span(fp, pv, q.x0, q.x1, u0, u1);
-            for (int u = u0; u <= u1; ++u)
-                if (cover_test(q, u + 0.5f, pv)) img[(long long)v * W + u] = 1;
+        const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
+        Footprint qfp;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            qfp.a[e] = __shfl_sync(0xffffffffu, fp.a[e], src);
+            qfp.b[e] = __shfl_sync(0xffffffffu, fp.b[e], src);
+            qfp.c[e] = __shfl_sync(0xffffffffu, fp.c[e], src);
+        }
+        const int qtx0 = q.x0 / kCovTile, qty0 = q.y0 / kCovTile, qntx = q.x1 / kCovTile - qtx0 + 1;
+        const int qnt = qntx * (q.y1 / kCovTile - qty0 + 1);
+        for (int k = lane; k < qnt; k += 32) {
+            const int tx = qtx0 + k % qntx, ty = qty0 + k / qntx;
+            if (footprint_overlaps(qfp, max(tx * kCovTile, q.x0), min(tx * kCovTile + kCovTile - 1, q.x1),
+                                   max(ty * kCovTile, q.y0), min(ty * kCovTile + kCovTile - 1, q.y1)))
+                cov_place(cb, qv, ty * cb.tiles_x + tx, qf, q, qfp);
         }
     }
+}
+
+struct CovTileTri {
+    float4 e0;  // footprint a0, b0, c0, a1
+    float4 e1;  // b1, c1, a2, b2
+    float4 e2;  // c2, d1, d2, -
+    float4 ab;  // a.x, a.y, b.x, b.y
+    float2 c;
+};
+
+// one CTA per (tile, view): a pixel stops at the first binned triangle that covers it
+__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int N, const int* __restrict__ faces,
+                                                                 const float2* __restrict__ p2d, CovBins cb) {
+    __shared__ CovTileTri s_t[kCovTile * kCovTile];
+    const int tile = blockIdx.x, view = blockIdx.y;
+    const long long key = (long long)view * cb.T + tile;
+    const int n = min(cb.count[key], kCovCap);
+    if (n == 0) return;  // CTA-uniform
+    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+    const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
+    const bool valid = px < cb.W && py < cb.H;
+    unsigned char* pix = cb.cover + ((long long)view * cb.H + py) * cb.W + px;
+    bool covered = !valid || *pix;
+    const float pu = px + 0.5f, pv = py + 0.5f;
+    for (int base = 0; base < n; base += kCovTile * kCovTile) {
+        const int m = min(kCovTile * kCovTile, n - base);
+        __syncthreads();
+        if ((int)threadIdx.x < m) {
+            const int f = cb.bins[key * kCovCap + base + threadIdx.x];
+            CoverTri t;
+            cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
+            const Footprint fp = cover_footprint(t, cb.W, cb.H);
+            CovTileTri e;
+            e.e0 = make_float4(fp.a[0], fp.b[0], fp.c[0], fp.a[1]);
+            e.e1 = make_float4(fp.b[1], fp.c[1], fp.a[2], fp.b[2]);
+            e.e2 = make_float4(fp.c[2], t.d1, t.d2, 0.f);
+            e.ab = make_float4(t.a.x, t.a.y, t.b.x, t.b.y);
+            e.c = t.c;
+            s_t[threadIdx.x] = e;
+        }
+        __syncthreads();
+        for (int j = 0; j < m && !covered; ++j) {
+            const float4 e0 = s_t[j].e0, e1 = s_t[j].e1, e2 = s_t[j].e2;
+            if (e0.x * pu + e0.y * pv + e0.z < 0.f || e0.w * pu + e1.x * pv + e1.y < 0.f ||
+                e1.z * pu + e1.w * pv + e2.x < 0.f)
+                continue;
+            CoverTri t;
+            const float4 ab = s_t[j].ab;
+            t.a = make_float2(ab.x, ab.y);
+            t.b = make_float2(ab.z, ab.w);
+            t.c = s_t[j].c;
+            t.d1 = e2.y;
+            t.d2 = e2.z;
+            covered = cover_test(t, pu, pv);
+        }
+    }
+    if (valid && covered && !*pix) *pix = 1;
 }
 
 // boundary test of k_boundary against the coverage image instead of a face buffer
@@ -542,7 +615,7 @@ extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover;
+    DevBuf faces, p2d, cover, count, bins;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -569,6 +642,8 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     h->faces.release();
     h->p2d.release();
     h->cover.release();
+    h->count.release();
+    h->bins.release();
     delete h;
     return HC_OK;
 }
@@ -580,6 +655,9 @@ extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch,
     const size_t views = (size_t)batch * n_cameras;
     HC_TRY(h->p2d.ensure(sizeof(float) * 2 * views * h->N));
     HC_TRY(h->cover.ensure(views * (size_t)width * height));
+    const size_t tiles = (size_t)div_up(width, kCovTile) * div_up(height, kCovTile);
+    HC_TRY(h->count.ensure(sizeof(int) * views * tiles));
+    HC_TRY(h->bins.ensure(sizeof(int) * views * tiles * kCovCap));
     return HC_OK;
 }
 
@@ -604,8 +682,20 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
     const long long views = (long long)batch * n_cameras;
     HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
     const long long nt = views * h->F;
-    k_cover<<<div_up(nt, 256), 256, 0, s>>>(batch, n_cameras, h->N, h->F, width, height, h->faces.as<int>(),
-                                            reinterpret_cast<const float2*>(p2d), h->cover.as<unsigned char>());
+    CovBins cb;
+    cb.tiles_x = div_up(width, kCovTile);
+    cb.T = cb.tiles_x * div_up(height, kCovTile);
+    cb.count = h->count.as<int>();
+    cb.bins = h->bins.as<int>();
+    cb.cover = h->cover.as<unsigned char>();
+    cb.W = width;
+    cb.H = height;
+    HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)views * cb.T, s));
+    k_cov_bin<<<div_up(nt, 256), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
+                                              reinterpret_cast<const float2*>(p2d), cb);
+    HC_CHECK_LAUNCH();
+    k_cov_tile<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(
+        h->N, h->faces.as<int>(), reinterpret_cast<const float2*>(p2d), cb);
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
                                                      h->cover.as<unsigned char>(), is_boundary);

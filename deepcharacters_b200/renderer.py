@@ -70,6 +70,20 @@ class RendererEngine:
             _lib.lib().hc_renderer_destroy(h)
             self._h = None
 
+    KERNELS = ("view_setup", "vertex_normals", "tri_frame", "bin", "spill", "resolve", "render_grad",
+               "normal_chain")
+
+    def set_kernel_timing(self, enable: bool):
+        """Bracket every renderer launch with CUDA events (benchmarks only)."""
+        _lib.call("hc_renderer_set_kernel_timing", self._h, int(bool(enable)))
+
+    def kernel_times(self) -> dict:
+        """Last recorded duration (ms) of each renderer kernel since the previous read."""
+        import ctypes as _C
+        out = (_C.c_float * len(self.KERNELS))()
+        _lib.call("hc_renderer_kernel_times", self._h, _C.cast(out, _C.c_void_p), len(self.KERNELS))
+        return {k: float(v) for k, v in zip(self.KERNELS, out) if v >= 0}
+
     @property
     def handle(self):
         return self._h

@@ -157,6 +157,16 @@ hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t parity);
  */
 hc_status hc_renderer_stats(hc_renderer h, void* stream, int64_t* binned, int64_t* spilled);
 
+/* Per-kernel timing for benchmarks (no reference counterpart).  When enabled,
+ * every renderer launch is bracketed by CUDA events on its stream;
+ * hc_renderer_kernel_times writes the last recorded duration (ms) of each
+ * kernel, in the order view set-up, vertex normals, triangle frames, binning,
+ * spill, tile resolve, render adjoint, normal chain (-1 if not run since the
+ * previous read), waiting for the last events.  Off by default; not for
+ * stream capture. */
+hc_status hc_renderer_set_kernel_timing(hc_renderer h, int32_t enable);
+hc_status hc_renderer_kernel_times(hc_renderer h, float* ms, int32_t n);
+
 /* ------------------------------------------------------------------------ */
 /* Embedded-graph deformation                                                */
 /* ------------------------------------------------------------------------ */
