@@ -41,6 +41,8 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
+from deepcharacters_b200 import dist as D  # noqa: E402
+
 METRIC = "fwd+bwd views/s at 81,920 tris 1024²: batched/graph vs plain per-view (same B200)"
 FRAMES, VIEWS, RES, SUBDIV = 16, 8, 1024, 6
 
@@ -111,30 +113,17 @@ class ClockSampler:
 # distributed plumbing
 # --------------------------------------------------------------------------
 def dist_setup(gpus: int):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        torch.cuda.set_device(local)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                             device_id=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
-    return world, rank, local
+    world, rank, local = D.env_rank()
+    torch.cuda.set_device(local if world > 1 else 0)
+    return D.init("nccl", timeout_s=120, device=torch.device("cuda", local))
 
 
 def barrier(world):
-    if world > 1:
-        torch.distributed.barrier()
+    D.barrier(world)
 
 
 def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    return float(t.item())
+    return D.max_over_ranks(x, world, "cuda")
 
 
 # --------------------------------------------------------------------------
@@ -240,9 +229,8 @@ def run_ours(args, world, rank, local):
     torch.cuda.current_stream().wait_stream(s)
     torch.cuda.synchronize()
 
-    def allreduce():
-        if world > 1:
-            torch.distributed.all_reduce(ch.buf["gcol"])
+    def allreduce():  # the shared vertex-colour gradient; frames are sharded
+        D.allreduce_shared([ch.buf["gcol"]], world)
 
     for _ in range(args.warmup):
         g.replay()
@@ -377,8 +365,7 @@ def run_e2e(ch, sc, dev, args, world):
             for k in E2E_KEYS:
                 ch.inp[k] = bufs[slot][k]
             ch.step()
-            if world > 1:
-                torch.distributed.all_reduce(ch.buf["gcol"])
+            D.allreduce_shared([ch.buf["gcol"]], world)
             done[slot].record()
             loss_host.copy_(ch.loss, non_blocking=True)
         torch.cuda.synchronize()
@@ -465,8 +452,7 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
-            torch.distributed.destroy_process_group()
+        D.finalize(world)
 
 
 if __name__ == "__main__":
