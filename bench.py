@@ -214,6 +214,7 @@ def run_ours(args, world, rank, local):
     views_per_step = FRAMES * VIEWS
     # autotuner: raster tile size and bin capacity (untimed)
     tune = ch.autotune() if not args.no_autotune else {}
+    binned, spilled = ch.check()  # raises if the raster's spill capacity overflowed
     # eager warm-up (allocates every workspace), then capture one step
     for _ in range(2):
         ch.step()
@@ -311,7 +312,8 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"frames sharded, {world} rank(s)",
                    "l2": "inputs larger than L2 (1.6 GB of target images per step)",
                    "raster_tile": ch.tuning[0], "bin_capacity": ch.tuning[1],
-                   "autotune_ms": {f"{t}x{c}": round(v, 3) for (t, c), v in tune.items()}},
+                   "autotune_ms": {f"{t}x{c}": round(v, 3) for (t, c), v in tune.items()},
+                   "bin_pairs": binned, "spilled_pairs": spilled},
         "e2e": e2e,
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": ach, "peak": peak, "unit": "GB/s",

@@ -64,6 +64,9 @@ _SIGS: dict[str, list] = {
     "hc_add_inplace": [vp, C.c_int64, vp, vp],
     "hc_gaussian_smooth": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, vp, vp],
     "hc_renderer_set_kernel_timing": [vp, C.c_int32],
+    "hc_renderer_create_multires": [vp, vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_char_p,
+                                    C.c_char_p, C.c_int32, C.c_int32, C.c_char_p],
+    "hc_renderer_frame_pixels": [vp, vp],
     "hc_renderer_kernel_times": [vp, vp, C.c_int32],
     "hc_image_l1_loss": [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp],
     "hc_renderer_backward": [vp, vp, C.c_int32, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,

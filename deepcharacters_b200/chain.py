@@ -179,6 +179,13 @@ class DeformRenderChain:
         self.tuning = best
         return results
 
+    def check(self):
+        """Run the forward stage once and raise if the raster's spill
+        capacity overflowed (the result would be incomplete); returns
+        (binned, spilled) pair counts."""
+        self.forward()
+        return self.rend.stats()
+
     def step(self):
         self.forward()
         self.silhouette_forward()

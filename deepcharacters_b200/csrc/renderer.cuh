@@ -10,12 +10,19 @@
 //   u64       spill_keys[K*TS*TS] packed (depth_q << 32 | triangle) per spilled tile pixel
 #pragma once
 
+#include <vector>
+
 #include "hc_common.cuh"
 #include "hc_math.cuh"
 
 namespace hc {
 
-enum AlbedoMode { kVertexColor = 0, kTextured, kNormal, kLighting, kForegroundMask, kPosition, kDepth, kUV };
+enum AlbedoMode {
+    kVertexColor = 0, kTextured, kNormal, kLighting, kForegroundMask, kPosition, kDepth, kUV,
+    // bilinear texture sampling (no reference counterpart: the reference's
+    // textured mode samples the nearest texel, CUDABasedRasterization.cu:347-373)
+    kTexturedBilinear
+};
 enum ShadingMode { kShaded = 0, kShadeless };
 enum NormalMapMode { kNmOriginal = 0, kNmHitPosition, kNmNone, kNmFace };
 
@@ -26,6 +33,20 @@ struct ViewCam {
     float intr[9];   // row-major 3x3
     float ro[3];     // ray origin (camera centre)
     float ro_s[3];   // ray origin / 1000
+    // the view's image: resolution, tile grids and where its pixels / tiles
+    // start in the call's buffers (cameras of a frame may differ in size)
+    int W, H, tiles_x, tiles_x_b;
+    long long pix_base, tile_base, tile_base_b;
+};
+
+constexpr int kAdjointTile = 16;  // tile edge of the renderer adjoint
+
+// One camera's image inside a frame: the frame's cameras are concatenated,
+// so views of different resolutions share one launch.
+struct CamLayout {
+    int W, H;
+    int tiles_x, tiles_x_b;        // raster tiles (ws.tile px) / adjoint tiles (16 px) per row
+    long long pix, tile, tile_b;   // first pixel / raster tile / adjoint tile in the frame
 };
 
 struct TriFrame {    // 48 bytes: s0.xyz n.x | s1.xyz n.y | s2.xyz n.z
@@ -225,6 +246,37 @@ __device__ __forceinline__ bool footprint_overlaps(const Footprint& fp, int x0, 
     return true;
 }
 
+// Bilinear texture lookup at texel coordinates (x, y), texel centres at
+// integer + 0.5, clamp-to-edge addressing: the four texel offsets (floats,
+// x3 channels) and weights.
+struct BilinearTaps {
+    long long o00, o10, o01, o11;
+    float fx, fy;
+};
+
+__device__ __forceinline__ BilinearTaps bilinear_taps(float x, float y, int tw, int th) {
+    const float sx = x - 0.5f, sy = y - 0.5f;
+    const float x0f = floorf(sx), y0f = floorf(sy);
+    BilinearTaps t;
+    t.fx = sx - x0f;
+    t.fy = sy - y0f;
+    const int x0 = (int)x0f, y0 = (int)y0f;
+    const int xa = min(max(x0, 0), tw - 1), xb = min(max(x0 + 1, 0), tw - 1);
+    const int ya = min(max(y0, 0), th - 1), yb = min(max(y0 + 1, 0), th - 1);
+    t.o00 = 3LL * ((long long)ya * tw + xa);
+    t.o10 = 3LL * ((long long)ya * tw + xb);
+    t.o01 = 3LL * ((long long)yb * tw + xa);
+    t.o11 = 3LL * ((long long)yb * tw + xb);
+    return t;
+}
+
+__device__ __forceinline__ float3 bilinear_sample(const float* T, const BilinearTaps& t) {
+    const float3 c00 = ld3(T + t.o00), c10 = ld3(T + t.o10), c01 = ld3(T + t.o01), c11 = ld3(T + t.o11);
+    const float w00 = (1.f - t.fx) * (1.f - t.fy), w10 = t.fx * (1.f - t.fy), w01 = (1.f - t.fx) * t.fy,
+                w11 = t.fx * t.fy;
+    return c00 * w00 + c10 * w10 + c01 * w01 + c11 * w11;
+}
+
 // Second-order SH shading of an albedo (reference getShading,
 // CudaRenderer/cpp/src/Utils/RendererUtil.h:135-173), one band set per channel.
 __device__ __forceinline__ float sh_channel(const float* s, float3 d, float3 d2) {
@@ -285,7 +337,11 @@ struct RasterWorkspace {
     int cap_views = 0;   // views the buffers are sized for
     int tile = 16;
     int bin_cap = 512;
-    int tiles_x = 0, tiles_y = 0;
+    // per-camera resolution and the device layout derived from it
+    std::vector<int> cam_w, cam_h;
+    int layout_tile = 0;                              // tile size the layout was built for
+    long long P_frame = 0, T_frame = 0, Tb_frame = 0; // pixels / raster tiles / adjoint tiles per frame
+    DevBuf layout, tile_cam, tile_cam_b;              // CamLayout[C]; camera of each tile of a frame
     long long spill_cap = 0;
     int spill_tile_cap = 0;
     DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;

@@ -8,26 +8,26 @@
 
 namespace hc {
 
-hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int W, int H,
-                         int albedo, int shading, const float* verts, const float* colors, const float* texture,
-                         int tex_h, int tex_w, const float* sh, const float* extr, const float* intr, float* bary,
-                         int* face, float* render, float* vnormal, int* depth_q, int* tie_count);
-hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H);
-hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, int W, int H, int mode,
+hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int albedo,
+                         int shading, const float* verts, const float* colors, const float* texture, int tex_h,
+                         int tex_w, const float* sh, const float* extr, const float* intr, float* bary, int* face,
+                         float* render, float* vnormal, int* depth_q, int* tie_count);
+hc_status raster_reserve(RasterWorkspace& ws, int views, int F);
+hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, long long P_frame, int mode,
                          const float* verts, int tex_h, int tex_w, float* bary, int* face, float* render,
                          float* vnormal, float* uv_map);
 hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
-                          int W, int H, int albedo, int shading, int ifs, int tfs, const float* grad,
-                          const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
-                          const float* sh, const float* target, const float* vnormal, const float* bary,
-                          const int* face, const float* extr, const float* intr, float* vpos_grad,
-                          float* vcol_grad, float* tex_grad, float* sh_grad, int parity);
+                          int albedo, int shading, int ifs, int tfs, const float* grad, const float* verts,
+                          const float* colors, const float* texture, int tex_h, int tex_w, const float* sh,
+                          const float* target, const float* vnormal, const float* bary, const int* face,
+                          const float* extr, const float* intr, float* vpos_grad, float* vcol_grad, float* tex_grad,
+                          float* sh_grad, int parity);
 
 static int parse_albedo(const char* m) {
     if (!m) return -1;
-    static const char* names[] = {"vertexColor", "textured", "normal", "lighting",
-                                  "foregroundMask", "position", "depth", "uv"};
-    for (int i = 0; i < 8; ++i)
+    static const char* names[] = {"vertexColor", "textured", "normal", "lighting", "foregroundMask",
+                                  "position", "depth", "uv", "texturedBilinear"};
+    for (int i = 0; i < 9; ++i)
         if (!strcmp(m, names[i])) return i;
     return -1;
 }
@@ -114,6 +114,12 @@ struct hc_renderer_s {
 
 using namespace hc;
 
+static long long frame_pixels(const hc_renderer_s* h) {
+    long long p = 0;
+    for (size_t c = 0; c < h->ws.cam_w.size(); ++c) p += (long long)h->ws.cam_w[c] * h->ws.cam_h[c];
+    return p;
+}
+
 extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, int32_t n_faces,
                                         const float* texture_coordinates, int32_t n_texcoords,
                                         int32_t number_of_vertices, int32_t number_of_cameras,
@@ -141,7 +147,7 @@ extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, 
                "texture_coordinates has %d values, expected 6 per face (%d)", n_texcoords, 6 * n_faces);
     // the reference op forces shadeless for every mode but vertexColor / textured
     // (CudaRenderer/cpp/src/TensorflowOperators/CudaRenderer/CudaRenderer.cpp:70-74)
-    if (albedo != kVertexColor && albedo != kTextured) shading = kShadeless;
+    if (albedo != kVertexColor && albedo != kTextured && albedo != kTexturedBilinear) shading = kShadeless;
     hc_renderer_s* r = new hc_renderer_s();
     hc_status st = topology_upload(r->topo, number_of_vertices, faces, n_faces, texture_coordinates, n_texcoords);
     if (st != HC_OK) {
@@ -151,6 +157,8 @@ extern "C" hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, 
     r->C = number_of_cameras;
     r->W = render_resolution_u;
     r->H = render_resolution_v;
+    r->ws.cam_w.assign(number_of_cameras, render_resolution_u);
+    r->ws.cam_h.assign(number_of_cameras, render_resolution_v);
     r->albedo = albedo;
     r->shading = shading;
     r->normal_map = nm;
@@ -167,7 +175,7 @@ static void release_all(hc_renderer_s* r) {
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
                       &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
-                      &r->uv.faces, &r->uv.table};
+                      &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b};
     for (DevBuf* b : bufs) b->release();
 }
 
@@ -182,7 +190,7 @@ extern "C" hc_status hc_renderer_destroy(hc_renderer h) {
 extern "C" hc_status hc_renderer_reserve(hc_renderer h, int32_t batch) {
     clear_error();
     HC_REQUIRE(h && batch > 0, "invalid handle or batch");
-    HC_TRY(raster_reserve(h->ws, batch * h->C, h->topo.F, h->W, h->H));
+    HC_TRY(raster_reserve(h->ws, batch * h->C, h->topo.F));
     HC_TRY(h->ws.tri_frame.ensure(sizeof(TriFrame) * (size_t)batch * h->topo.F));
     return HC_OK;
 }
@@ -217,7 +225,7 @@ extern "C" hc_status hc_renderer_forward_ex(hc_renderer h, void* stream, int32_t
                    vertex_normal,
                "NULL input/output pointer");
     if (h->albedo == kVertexColor) HC_REQUIRE(vertex_color, "vertexColor mode needs vertex_color");
-    if (h->albedo == kTextured) {
+    if (h->albedo == kTextured || h->albedo == kTexturedBilinear) {
         HC_REQUIRE(texture && texture_width > 0 && texture_height > 0, "textured mode needs a texture");
         HC_REQUIRE(h->topo.has_texcoords, "textured mode needs texture_coordinates");
     }
@@ -225,10 +233,10 @@ extern "C" hc_status hc_renderer_forward_ex(hc_renderer h, void* stream, int32_t
     if (needs_sh) HC_REQUIRE(sh_coeff, "shading needs sh_coeff");
     cudaStream_t s = (cudaStream_t)stream;
     if (h->normal_map != kNmNone)
-        return raster_uv_maps(h->topo, h->uv, s, batch, h->C, h->W, h->H, h->normal_map, vertex_pos, texture_height,
+        return raster_uv_maps(h->topo, h->uv, s, batch, h->C, frame_pixels(h), h->normal_map, vertex_pos, texture_height,
                               texture_width, barycentric_buffer, face_buffer, render_buffer, vertex_normal,
                               normal_map);
-    return raster_forward(h->topo, h->ws, s, batch, h->C, h->W, h->H, h->albedo, h->shading, vertex_pos,
+    return raster_forward(h->topo, h->ws, s, batch, h->C, h->albedo, h->shading, vertex_pos,
                           vertex_color, texture, texture_height, texture_width, sh_coeff, extrinsics, intrinsics,
                           barycentric_buffer, face_buffer, render_buffer, vertex_normal, depth_q, tie_count);
 }
@@ -268,16 +276,16 @@ extern "C" hc_status hc_renderer_backward(hc_renderer h, void* stream, int32_t b
     clear_error();
     HC_REQUIRE(h, "invalid handle");
     HC_REQUIRE(batch > 0, "batch must be positive (%d)", batch);
-    HC_REQUIRE(h->albedo == kVertexColor || h->albedo == kTextured,
+    HC_REQUIRE(h->albedo == kVertexColor || h->albedo == kTextured || h->albedo == kTexturedBilinear,
                "renderer gradients exist only for vertexColor and textured albedo");
     HC_REQUIRE(render_buffer_grad && vertex_pos && target_image && vertex_normal && barycentric_buffer &&
                    face_buffer && extrinsics && intrinsics && vertex_pos_grad,
                "NULL input/output pointer");
     if (h->albedo == kVertexColor) HC_REQUIRE(vertex_color && vertex_color_grad, "vertexColor mode needs colours");
-    if (h->albedo == kTextured)
+    if (h->albedo == kTextured || h->albedo == kTexturedBilinear)
         HC_REQUIRE(texture && texture_grad && texture_width > 0 && texture_height > 0, "textured mode needs a texture");
     if (h->shading == kShaded) HC_REQUIRE(sh_coeff && sh_coeff_grad, "shaded mode needs sh_coeff");
-    return raster_backward(h->topo, h->ws, h->nrm_grad, (cudaStream_t)stream, batch, h->C, h->W, h->H, h->albedo,
+    return raster_backward(h->topo, h->ws, h->nrm_grad, (cudaStream_t)stream, batch, h->C, h->albedo,
                            h->shading, h->image_filter, h->texture_filter, render_buffer_grad, vertex_pos,
                            vertex_color, texture, texture_height, texture_width, sh_coeff, target_image,
                            vertex_normal, barycentric_buffer, face_buffer, extrinsics, intrinsics, vertex_pos_grad,
@@ -316,5 +324,36 @@ extern "C" hc_status hc_renderer_kernel_times(hc_renderer h, float* ms, int32_t 
         }
     }
     c.recorded = 0;
+    return HC_OK;
+}
+
+extern "C" hc_status hc_renderer_create_multires(hc_renderer* out, const int32_t* faces, int32_t n_faces,
+                                                 const float* texture_coordinates, int32_t n_texcoords,
+                                                 int32_t number_of_vertices, int32_t number_of_cameras,
+                                                 const int32_t* camera_widths, const int32_t* camera_heights,
+                                                 const char* albedo_mode, const char* shading_mode,
+                                                 int32_t image_filter_size, int32_t texture_filter_size,
+                                                 const char* compute_normal_map) {
+    clear_error();
+    HC_REQUIRE(out, "out is NULL");
+    *out = nullptr;
+    HC_REQUIRE(camera_widths && camera_heights && number_of_cameras > 0, "camera sizes must be given");
+    for (int c = 0; c < number_of_cameras; ++c)
+        HC_REQUIRE(camera_widths[c] > 0 && camera_widths[c] < 32768 && camera_heights[c] > 0 &&
+                       camera_heights[c] < 32768,
+                   "camera %d size %dx%d out of range", c, camera_widths[c], camera_heights[c]);
+    HC_TRY(hc_renderer_create(out, faces, n_faces, texture_coordinates, n_texcoords, number_of_vertices,
+                              number_of_cameras, camera_widths[0], camera_heights[0], albedo_mode, shading_mode,
+                              image_filter_size, texture_filter_size, compute_normal_map));
+    hc_renderer_s* r = *out;
+    r->ws.cam_w.assign(camera_widths, camera_widths + number_of_cameras);
+    r->ws.cam_h.assign(camera_heights, camera_heights + number_of_cameras);
+    return HC_OK;
+}
+
+extern "C" hc_status hc_renderer_frame_pixels(hc_renderer h, int64_t* pixels) {
+    clear_error();
+    HC_REQUIRE(h && pixels, "invalid arguments");
+    *pixels = frame_pixels(h);
     return HC_OK;
 }

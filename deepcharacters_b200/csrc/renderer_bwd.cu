@@ -24,16 +24,20 @@
 
 namespace hc {
 
-__global__ void k_view_setup(int V, const float* __restrict__ extr, const float* __restrict__ intr,
-                             ViewCam* __restrict__ cams);
+__global__ void k_view_setup(int V, int C, const float* __restrict__ extr, const float* __restrict__ intr,
+                             const CamLayout* __restrict__ layout, long long P_frame, long long T_frame,
+                             long long Tb_frame, ViewCam* __restrict__ cams);
 
 namespace {
 
 constexpr int BT = 16;           // backward tile edge
 constexpr int BNT = BT * BT;     // threads per CTA
+static_assert(BT == kAdjointTile, "the adjoint tile grid of the layout");
 
 struct BwdArgs {
-    int B, C, N, F, W, H;
+    int B, C, N, F;
+    long long Tb_frame;      // adjoint tiles per frame (all cameras)
+    const int* tile_cam_b;   // camera of each adjoint tile of a frame
     int albedo, shading;
     int ifs, tfs;
     int tex_w, tex_h;
@@ -177,10 +181,10 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
 
 // Albedo classes of the adjoint: vertex colours, texture, and the modes
 // whose albedo has no parameters (normal, lighting, mask, position, depth, uv).
-enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2 };
+enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2, kAlbTexBilinear = 3 };
 
 template <bool SHADED, int ALB, bool PARITY>
-__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, int tiles_x, const ViewCam* __restrict__ cams) {
+__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams) {
     constexpr int NVV = SHADED ? 9 : 6;               // values per vertex
     constexpr int NROW = (3 * NVV + 3) / 4 * 4;       // per-lane row, padded for float4 loads
     __shared__ __align__(16) float s_red[BNT / 32][32][NROW];
@@ -188,16 +192,22 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
     __shared__ float4 s_tgt[TILE_S * TILE_S];
     __shared__ float2 s_tap[MAXTAPS];  // image-gradient tap weights (i, j) / (i^2 + j^2)
     __shared__ float s_norm;
-    const int tile = blockIdx.x, view = blockIdx.y;
-    const int b = view / A.C;
+    // one CTA per 16x16 tile of the call; the frame's cameras are concatenated
+    const long long g = blockIdx.x;
+    const int b = (int)(g / A.Tb_frame);
+    const int view = b * A.C + A.tile_cam_b[g % A.Tb_frame];
+    const ViewCam& cam = cams[view];
+    const int tile = (int)(g - cam.tile_base_b);
+    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x_b;
     constexpr bool shaded = SHADED;
     constexpr bool vcol = ALB == kAlbVcol;
     constexpr bool textured = ALB == kAlbTex;
+    constexpr bool bilinear = ALB == kAlbTexBilinear;
     const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
     const int px = tx0 + threadIdx.x % BT;
     const int py = ty0 + threadIdx.x / BT;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const float* tgt = A.target + (long long)view * A.H * A.W * 3;
+    const float* tgt = A.target + cam.pix_base * 3;
     // stage the target tile with the filter halo (clipped to the image)
     const bool staged = A.ifs <= MAXFS;
     if (staged) {
@@ -206,8 +216,8 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
             const int yy = ty0 - A.ifs + i / e, xx = tx0 - A.ifs + i % e;
             // asynchronous copies: the pixel work below that does not read the
             // target overlaps them; they are waited for before the taps
-            if (xx >= 0 && yy >= 0 && xx < A.W && yy < A.H) {
-                const float* src = tgt + 3 * ((long long)yy * A.W + xx);
+            if (xx >= 0 && yy >= 0 && xx < W && yy < H) {
+                const float* src = tgt + 3 * ((long long)yy * W + xx);
                 const unsigned dst = (unsigned)__cvta_generic_to_shared(&s_tgt[i]);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4), "l"(src + 1));
@@ -238,8 +248,8 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
     float shg[SHADED ? 27 : 1];
 #pragma unroll
     for (int k = 0; k < (SHADED ? 27 : 1); ++k) shg[k] = 0.f;
-    const long long pix = ((long long)view * A.H + py) * A.W + px;
-    const int f = (px < A.W && py < A.H) ? A.face[pix] : -1;
+    const long long pix = cam.pix_base + (long long)py * W + px;
+    const int f = (px < W && py < H) ? A.face[pix] : -1;
     int vid[3] = {-1, -1, -1};
     float bw[3] = {0.f, 0.f, 0.f};
     float gp[9];
@@ -247,7 +257,6 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
     for (int k = 0; k < 9; ++k) gp[k] = 0.f;
     float3 gA = make_float3(0.f, 0.f, 0.f), gnu = make_float3(0.f, 0.f, 0.f);
     // carried from the first half of the pixel work (no target reads) to the second
-    const ViewCam& cam = cams[view];
     float3 d = make_float3(0.f, 0.f, 1.f), v0 = d, v1 = d, v2 = d, G = d, frag = d;
     float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
     if (f >= 0) {
@@ -288,6 +297,32 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
             const float3 c0 = ld3(Cc + 3 * id.x), c1 = ld3(Cc + 3 * id.y), c2 = ld3(Cc + 3 * id.z);
             alb = ba * c0 + bb * c1 + bc * c2;
             gbc = make_float3(dot(gA, c0), dot(gA, c1), dot(gA, c2));
+        } else if constexpr (bilinear) {
+            // bilinear sampling: texture gradient to the four texels, and the
+            // exact derivative of the sample w.r.t. the texel position
+            const float2 t0 = make_float2(tcp[0], 1.f - tcp[1]);
+            const float2 t1 = make_float2(tcp[2], 1.f - tcp[3]);
+            const float2 t2 = make_float2(tcp[4], 1.f - tcp[5]);
+            const float2 uv = t0 * ba + t1 * bb + t2 * bc;
+            const BilinearTaps tp = bilinear_taps(uv.x * A.tex_w, uv.y * A.tex_h, A.tex_w, A.tex_h);
+            const float* T = A.texture + (long long)b * A.tex_h * A.tex_w * 3;
+            const float3 c00 = ld3(T + tp.o00), c10 = ld3(T + tp.o10), c01 = ld3(T + tp.o01), c11 = ld3(T + tp.o11);
+            const float w00 = (1.f - tp.fx) * (1.f - tp.fy), w10 = tp.fx * (1.f - tp.fy),
+                        w01 = (1.f - tp.fx) * tp.fy, w11 = tp.fx * tp.fy;
+            alb = c00 * w00 + c10 * w10 + c01 * w01 + c11 * w11;
+            float* tg = A.tex_grad + (long long)b * A.tex_h * A.tex_w * 3;
+            const long long off[4] = {tp.o00, tp.o10, tp.o01, tp.o11};
+            const float wt[4] = {w00, w10, w01, w11};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                atomicAdd(tg + off[q] + 0, gA.x * wt[q]);
+                atomicAdd(tg + off[q] + 1, gA.y * wt[q]);
+                atomicAdd(tg + off[q] + 2, gA.z * wt[q]);
+            }
+            const float3 dx = (c10 - c00) * (1.f - tp.fy) + (c11 - c01) * tp.fy;
+            const float3 dy = (c01 - c00) * (1.f - tp.fx) + (c11 - c10) * tp.fx;
+            const float gu = dot(gA, dx) * A.tex_w, gv = dot(gA, dy) * A.tex_h;
+            gbc = make_float3(gu * t0.x + gv * t0.y, gu * t1.x + gv * t1.y, gu * t2.x + gv * t2.y);
         } else if constexpr (textured) {
             const float2 t0 = make_float2(tcp[0], 1.f - tcp[1]);
             const float2 t1 = make_float2(tcp[2], 1.f - tcp[3]);
@@ -353,7 +388,7 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
         {
             const int fs = A.ifs;
             float gu = 0.f, gv = 0.f;
-            if (px >= fs + 1 && py >= fs + 1 && px < A.W - (fs + 1) && py < A.H - (fs + 1)) {
+            if (px >= fs + 1 && py >= fs + 1 && px < W - (fs + 1) && py < H - (fs + 1)) {
                 // taps weighted (x, y)/(x^2 + y^2), normalised by sum |x|/(x^2 + y^2)
                 // (imageGradient, RendererUtil.h:566-620), contracted with G
                 if (staged) {
@@ -381,7 +416,7 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
                         for (int i = -fs; i <= fs; ++i) {
                             const float den = (float)(i * i + j * j);
                             if (den == 0.f) continue;
-                            const float3 I = ld3(tgt + 3 * ((long long)(py + j) * A.W + (px + i)));
+                            const float3 I = ld3(tgt + 3 * ((long long)(py + j) * W + (px + i)));
                             const float gi = dot(G, I);
                             gu += gi * ((float)i / den);
                             gv += gi * ((float)j / den);
@@ -545,13 +580,16 @@ __global__ void k_normal_chain(int B, int N, const int3* __restrict__ faces, con
 
 }  // namespace
 
+hc_status raster_layout(RasterWorkspace& ws);
+
 hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
-                          int W, int H, int albedo, int shading, int ifs, int tfs, const float* grad,
+                          int albedo, int shading, int ifs, int tfs, const float* grad,
                           const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
                           const float* sh, const float* target, const float* vnormal, const float* bary,
                           const int* face, const float* extr, const float* intr, float* vpos_grad,
                           float* vcol_grad, float* tex_grad, float* sh_grad, int parity) {
     const int V = B * C, N = topo.N;
+    HC_TRY(raster_layout(ws));
     HC_TRY(ws.cams.ensure(sizeof(ViewCam) * (size_t)std::max(V, ws.cap_views)));
     const bool shaded = shading == kShaded;
     if (shaded) HC_TRY(nrm_ws.ensure(sizeof(float) * 3 * (size_t)B * N));
@@ -562,15 +600,16 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     if (sh_grad) HC_CUDA(cudaMemsetAsync(sh_grad, 0, sizeof(float) * 27 * (size_t)V, s));
     if (shaded) HC_CUDA(cudaMemsetAsync(nrm_ws.ptr, 0, sizeof(float) * 3 * (size_t)B * N, s));
     ViewCam* cams = ws.cams.as<ViewCam>();
-    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, extr, intr, cams);
+    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, C, extr, intr, ws.layout.as<CamLayout>(), ws.P_frame, ws.T_frame,
+                                              ws.Tb_frame, cams);
     HC_CHECK_LAUNCH();
     BwdArgs A;
     A.B = B;
     A.C = C;
     A.N = N;
     A.F = topo.F;
-    A.W = W;
-    A.H = H;
+    A.Tb_frame = ws.Tb_frame;
+    A.tile_cam_b = ws.tile_cam_b.as<int>();
     A.albedo = albedo;
     A.shading = shading;
     A.ifs = ifs;
@@ -593,14 +632,17 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.tex_grad = tex_grad;
     A.sh_grad = sh_grad;
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
-    const int tiles_x = div_up(W, BT), tiles_y = div_up(H, BT);
-    const dim3 grid(tiles_x * tiles_y, V);
+    const long long tiles = (long long)B * ws.Tb_frame;
+    HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
+    const unsigned grid = (unsigned)tiles;
     ws.clock.begin(kKRenderGrad, s);
-    const int alb = albedo == kVertexColor ? kAlbVcol : albedo == kTextured ? kAlbTex : kAlbNone;
-    const int sel = (shaded ? 6 : 0) + alb * 2 + (parity ? 1 : 0);
+    const int alb = albedo == kVertexColor ? kAlbVcol
+                    : albedo == kTextured ? kAlbTex
+                    : albedo == kTexturedBilinear ? kAlbTexBilinear : kAlbNone;
+    const int sel = (shaded ? 8 : 0) + alb * 2 + (parity ? 1 : 0);
     switch (sel) {
 #define HC_GRAD_CASE(SH, AL, PA) \
-    case (SH ? 6 : 0) + AL * 2 + PA: k_render_grad<SH, AL, PA><<<grid, BNT, 0, s>>>(A, tiles_x, cams); break;
+    case (SH ? 8 : 0) + AL * 2 + PA: k_render_grad<SH, AL, PA><<<grid, BNT, 0, s>>>(A, cams); break;
         HC_GRAD_CASE(false, kAlbVcol, false)
         HC_GRAD_CASE(false, kAlbVcol, true)
         HC_GRAD_CASE(false, kAlbTex, false)
@@ -613,6 +655,10 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
         HC_GRAD_CASE(true, kAlbTex, true)
         HC_GRAD_CASE(true, kAlbNone, false)
         HC_GRAD_CASE(true, kAlbNone, true)
+        HC_GRAD_CASE(false, kAlbTexBilinear, false)
+        HC_GRAD_CASE(false, kAlbTexBilinear, true)
+        HC_GRAD_CASE(true, kAlbTexBilinear, false)
+        HC_GRAD_CASE(true, kAlbTexBilinear, true)
 #undef HC_GRAD_CASE
     }
     HC_CHECK_LAUNCH();

@@ -22,10 +22,23 @@ namespace hc {
 // camera set-up: one thread per view (reference initializeCamerasDevice,
 // CUDABasedRasterization.cu:23-67, which runs <<<1,1>>> per frame)
 // ---------------------------------------------------------------------------
-__global__ void k_view_setup(int V, const float* __restrict__ extr, const float* __restrict__ intr,
-                             ViewCam* __restrict__ cams) {
+__global__ void k_view_setup(int V, int C, const float* __restrict__ extr, const float* __restrict__ intr,
+                             const CamLayout* __restrict__ layout, long long P_frame, long long T_frame,
+                             long long Tb_frame, ViewCam* __restrict__ cams) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= V) return;
+    {
+        const CamLayout L = layout[v % C];
+        const long long b = v / C;
+        ViewCam& c = cams[v];
+        c.W = L.W;
+        c.H = L.H;
+        c.tiles_x = L.tiles_x;
+        c.tiles_x_b = L.tiles_x_b;
+        c.pix_base = b * P_frame + L.pix;
+        c.tile_base = b * T_frame + L.tile;
+        c.tile_base_b = b * Tb_frame + L.tile_b;
+    }
     const float* e = extr + 12 * (long long)v;
     const float* k = intr + 9 * (long long)v;
     M44 E, K;
@@ -143,13 +156,13 @@ struct BinSink {
     int TS, cap;
     int2* tile_state;
     int* bins;
-    int4* spill;
+    int2* spill;  // (tile of the call, triangle)
     long long spill_cap;
     unsigned long long* spill_keys;
     int spill_tile_cap;
     RasterStats* stats;
 
-    __device__ __forceinline__ int place(int slot, long long key, int view, int T, int f) const {
+    __device__ __forceinline__ int place(int slot, long long key, int view, int local_tile, int f) const {
         if (slot < cap) {
             bins[key * cap + slot] = f;
             return 1;
@@ -166,7 +179,7 @@ struct BinSink {
         }
         const unsigned long long si = atomicAdd(&stats->spilled, 1ull);
         if ((long long)si < spill_cap) {
-            spill[si] = make_int4(view, (int)(key - (long long)view * T), f, 0);
+            spill[si] = make_int2((int)key, f);
         } else {
             atomicOr(&stats->overflow, 1);
         }
@@ -174,22 +187,28 @@ struct BinSink {
     }
 };
 
-__global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tiles_x, int tiles_y, int cap,
+__global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
                       const int3* __restrict__ faces, const float* __restrict__ verts,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
-                      int4* __restrict__ spill, long long spill_cap, unsigned long long* __restrict__ spill_keys,
+                      int2* __restrict__ spill, long long spill_cap, unsigned long long* __restrict__ spill_keys,
                       int spill_tile_cap, RasterStats* __restrict__ stats) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const bool live = i < (long long)V * F;
     int view = 0, f = 0;
     int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
+    int W = 0, H = 0, tiles_x = 1;
+    long long tile_base = 0;
     Footprint fp;
     if (live) {
         view = (int)(i / F);
         f = (int)(i % F);
         const int b = view / C;
         const ViewCam& cam = cams[view];
+        W = cam.W;
+        H = cam.H;
+        tiles_x = cam.tiles_x;
+        tile_base = cam.tile_base;
         const float* P = verts + (long long)b * N * 3;
         const int3 id = faces[f];
         const float3 p0 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.x));
@@ -225,7 +244,6 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         ty0 = y0 / TS;
         ty1 = y1 / TS;
     }
-    const int T = tiles_x * tiles_y;
     const int ntx = tx1 - tx0 + 1;
     const int nt = nonempty ? ntx * (ty1 - ty0 + 1) : 0;
     const bool big = nt > kBinSmall;
@@ -247,7 +265,7 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
             // tiles of the box that the triangle's footprint misses get no entry
             act = nt == 1 || footprint_overlaps(fp, max(tx * TS, x0), min(tx * TS + TS - 1, x1), max(ty * TS, y0),
                                                 min(ty * TS + TS - 1, y1));
-            if (act) key = (long long)view * T + ty * tiles_x + tx;
+            if (act) key = tile_base + ty * tiles_x + tx;
         }
         const unsigned same = __match_any_sync(0xffffffffu, key);
         if (!act) continue;
@@ -256,7 +274,7 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         int base = 0;
         if ((int)lane == leader) base = atomicAdd(&tile_state[key].x, __popc(same));
         base = __shfl_sync(same, base, leader);
-        nbinned += sink.place(base + rank, key, view, T, f);
+        nbinned += sink.place(base + rank, key, view, (int)(key - tile_base), f);
     }
     // larger boxes: the warp takes them one at a time, a tile per lane
     unsigned pending = __ballot_sync(0xffffffffu, big);
@@ -264,6 +282,8 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
         const int src = __ffs(pending) - 1;
         pending &= pending - 1;
         const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
+        const int qtiles_x = __shfl_sync(0xffffffffu, tiles_x, src);
+        const long long qbase = __shfl_sync(0xffffffffu, tile_base, src);
         const int qx0 = __shfl_sync(0xffffffffu, x0, src), qx1 = __shfl_sync(0xffffffffu, x1, src);
         const int qy0 = __shfl_sync(0xffffffffu, y0, src), qy1 = __shfl_sync(0xffffffffu, y1, src);
         Footprint qfp;
@@ -281,8 +301,8 @@ __global__ void k_bin(int V, int C, int F, int N, int W, int H, int TS, int tile
             if (!footprint_overlaps(qfp, max(tx * TS, qx0), min(tx * TS + TS - 1, qx1), max(ty * TS, qy0),
                                     min(ty * TS + TS - 1, qy1)))
                 continue;
-            const long long key = (long long)qv * T + ty * tiles_x + tx;
-            nbinned += sink.place(atomicAdd(&tile_state[key].x, 1), key, qv, T, qf);
+            const long long key = qbase + ty * qtiles_x + tx;
+            nbinned += sink.place(atomicAdd(&tile_state[key].x, 1), key, qv, (int)(key - qbase), qf);
         }
     }
     // one counter update per warp
@@ -304,20 +324,24 @@ __device__ __forceinline__ void unpack_bbox(const TriView& tv, int& x0, int& x1,
 // `count_depth` set (diagnostics) the pass instead counts, per pixel, the
 // spilled triangles that reach the final depth.
 // ---------------------------------------------------------------------------
-__global__ void k_spill(int C, int F, int W, int H, int TS, int tiles_x,
+__global__ void k_spill(int C, int F, int TS, long long T_frame, const int* __restrict__ tile_cam,
                         const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                         const TriView* __restrict__ tri_view, const int2* __restrict__ tile_state,
-                        const int4* __restrict__ spill, long long spill_cap, int spill_tile_cap,
+                        const int2* __restrict__ spill, long long spill_cap, int spill_tile_cap,
                         unsigned long long* __restrict__ spill_keys, const RasterStats* __restrict__ stats,
-                        const int* __restrict__ count_depth, int* __restrict__ tie_out, int T) {
+                        const int* __restrict__ count_depth, int* __restrict__ tie_out) {
     const long long n = min((long long)stats->spilled, spill_cap);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
-        const int4 it = spill[i];
-        const int view = it.x, tile = it.y, f = it.z;
-        const int ks = tile_state[(long long)view * T + tile].y - 1;
-        if (ks < 0 || ks >= spill_tile_cap) continue;
+        const int2 it = spill[i];
+        const long long g = it.x;
+        const int f = it.y;
+        const int view = (int)(g / T_frame) * C + tile_cam[g % T_frame];
         const ViewCam& cam = cams[view];
+        const int tile = (int)(g - cam.tile_base);
+        const int ks = tile_state[g].y - 1;
+        if (ks < 0 || ks >= spill_tile_cap) continue;
+        const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x;
         const TriView tv = tri_view[(long long)view * F + f];
         const TriS Tr = tri_from(tri_frame[(long long)(view / C) * F + f]);
         const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
@@ -334,7 +358,7 @@ __global__ void k_spill(int C, int F, int W, int H, int TS, int tiles_x,
                 if (!raster_hit(ro_s, dir, Tr, tv.num, dq, a, b)) continue;
                 const int local = (py - ty * TS) * TS + (px - tx * TS);
                 if (count_depth) {
-                    const long long pix = ((long long)view * H + py) * W + px;
+                    const long long pix = cam.pix_base + (long long)py * W + px;
                     if (dq == count_depth[pix]) atomicAdd(&tie_out[pix], 1);
                 } else {
                     const unsigned long long key = ((unsigned long long)(unsigned)dq << 32) | (unsigned)f;
@@ -348,7 +372,7 @@ __global__ void k_spill(int C, int F, int W, int H, int TS, int tiles_x,
 // tile resolve + shading
 // ---------------------------------------------------------------------------
 struct ShadeArgs {
-    int B, C, N, F, W, H;
+    int B, C, N, F;
     int albedo, shading;
     const int3* faces;
     const float* texcoords;
@@ -391,6 +415,16 @@ __device__ __forceinline__ float3 shade_pixel(const ShadeArgs& A, const ViewCam&
             const int lv = (int)(uv.y - 0.5f);
             const float* T = A.texture + (long long)b * A.tex_h * A.tex_w * 3;
             color = ld3(T + 3LL * A.tex_w * lv + 3 * lu);
+            break;
+        }
+        case kTexturedBilinear: {
+            const float* tc = A.texcoords + (long long)f * 6;
+            const float2 t0 = make_float2(tc[0], 1.f - tc[1]);
+            const float2 t1 = make_float2(tc[2], 1.f - tc[3]);
+            const float2 t2 = make_float2(tc[4], 1.f - tc[5]);
+            const float2 uv = t0 * a + t1 * bb + t2 * (1.f - a - bb);
+            const float* T = A.texture + (long long)b * A.tex_h * A.tex_w * 3;
+            color = bilinear_sample(T, bilinear_taps(uv.x * A.tex_w, uv.y * A.tex_h, A.tex_w, A.tex_h));
             break;
         }
         case kVertexColor: {
@@ -484,7 +518,8 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, int tiles_x, int T, int cap,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, long long T_frame,
+                                                   const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
                                                    const TriView* __restrict__ tri_view,
@@ -497,21 +532,24 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
     __shared__ TileTri s_tri[CHUNK];
     __shared__ unsigned long long s_key[CHUNK];  // facing | depth lower bound | slot
     __shared__ unsigned short s_order[CHUNK];    // slots in key order
-    const int tile = blockIdx.x;
-    const int view = blockIdx.y;
-    const int b = view / A.C;
+    // one CTA per tile of the call; the frame's cameras are concatenated
+    const long long g = blockIdx.x;
+    const int b = (int)(g / T_frame);
+    const int view = b * A.C + tile_cam[g % T_frame];
+    const ViewCam& cam = cams[view];
+    const int tile = (int)(g - cam.tile_base);
+    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int lx = threadIdx.x % TS, ly = threadIdx.x / TS;
     const int px = tx * TS + lx, py = ty * TS + ly;
     const unsigned col_bit = 1u << lx, row_bit = 1u << ly;
     const float cx = px + 0.5f, cy = py + 0.5f;
-    const bool valid = px < A.W && py < A.H;
-    const ViewCam& cam = cams[view];
+    const bool valid = px < W && py < H;
     const float3 ro_s = make_float3(cam.ro_s[0], cam.ro_s[1], cam.ro_s[2]);
     const float3 dir = pixel_ray(cam, px, py);
-    const int2 st = tile_state[(long long)view * T + tile];
+    const int2 st = tile_state[g];
     const int n = min(st.x, cap);
-    const int* tb = bins + ((long long)view * T + tile) * cap;
+    const int* tb = bins + g * cap;
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
@@ -633,7 +671,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
             }
         }
     }
-    const long long pix = ((long long)view * A.H + py) * A.W + px;
+    const long long pix = cam.pix_base + (long long)py * W + px;
     if (best_d == 0xffffffffu) {
         A.face[pix] = -1;
         A.bary[2 * pix + 0] = 0.f;
@@ -646,11 +684,11 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
         return;
     }
     // recompute the winner's barycentrics (same arithmetic as the hit test)
-    const TriS W = tri_from(tri_frame[(long long)b * A.F + best_f]);
+    const TriS Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
     const TriView wv = tri_view[(long long)view * A.F + best_f];
     int dq;
     float a = 0.f, bb = 0.f;
-    raster_hit(ro_s, dir, W, wv.num, dq, a, bb);
+    raster_hit(ro_s, dir, Tw, wv.num, dq, a, bb);
     A.face[pix] = best_f;
     A.bary[2 * pix + 0] = a;
     A.bary[2 * pix + 1] = bb;
@@ -665,24 +703,61 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H) {
+// Per-camera layout of a frame for the current tile size: each camera's
+// resolution, tile grids and offsets, and the camera of every tile (the tile
+// resolve and the adjoint launch one CTA per tile of the whole call).
+hc_status raster_layout(RasterWorkspace& ws) {
+    const int TS = ws.tile, C = (int)ws.cam_w.size();
+    if (ws.layout_tile == TS) return HC_OK;
+    std::vector<CamLayout> L(C);
+    std::vector<int> tc, tcb;
+    long long pix = 0, tile = 0, tile_b = 0;
+    for (int c = 0; c < C; ++c) {
+        CamLayout& l = L[c];
+        l.W = ws.cam_w[c];
+        l.H = ws.cam_h[c];
+        l.tiles_x = div_up(l.W, TS);
+        l.tiles_x_b = div_up(l.W, kAdjointTile);
+        l.pix = pix;
+        l.tile = tile;
+        l.tile_b = tile_b;
+        const long long nt = (long long)l.tiles_x * div_up(l.H, TS);
+        const long long ntb = (long long)l.tiles_x_b * div_up(l.H, kAdjointTile);
+        tc.insert(tc.end(), (size_t)nt, c);
+        tcb.insert(tcb.end(), (size_t)ntb, c);
+        pix += (long long)l.W * l.H;
+        tile += nt;
+        tile_b += ntb;
+    }
+    HC_TRY(upload(ws.layout, L.data(), L.size()));
+    HC_TRY(upload(ws.tile_cam, tc.data(), tc.size()));
+    HC_TRY(upload(ws.tile_cam_b, tcb.data(), tcb.size()));
+    ws.P_frame = pix;
+    ws.T_frame = tile;
+    ws.Tb_frame = tile_b;
+    ws.layout_tile = TS;
+    ws.cap_views = 0;  // bins depend on the tile count
+    return HC_OK;
+}
+
+hc_status raster_reserve(RasterWorkspace& ws, int views, int F) {
+    HC_TRY(raster_layout(ws));
     const int TS = ws.tile;
-    ws.tiles_x = div_up(W, TS);
-    ws.tiles_y = div_up(H, TS);
-    const long long T = (long long)ws.tiles_x * ws.tiles_y;
-    if (views > ws.cap_views || ws.bins.bytes < (size_t)views * T * ws.bin_cap * sizeof(int)) {
+    const int C = (int)ws.cam_w.size();
+    const long long tiles = (long long)(views / C) * ws.T_frame;  // all tiles of the call
+    if (views > ws.cap_views || ws.bins.bytes < (size_t)tiles * ws.bin_cap * sizeof(int)) {
         HC_TRY(ws.cams.ensure(sizeof(ViewCam) * views));
         HC_TRY(ws.tri_view.ensure(sizeof(TriView) * (size_t)views * F));
-        HC_TRY(ws.tile_state.ensure(sizeof(int2) * (size_t)views * T));
-        HC_TRY(ws.bins.ensure(sizeof(int) * (size_t)views * T * ws.bin_cap));
-        ws.spill_cap = std::max<long long>(1 << 20, (long long)views * F / 4);
-        HC_TRY(ws.spill.ensure(sizeof(int4) * (size_t)ws.spill_cap));
-        // one key block per spilled tile; every tile can get one while that
-        // stays under 256 MB, beyond it a sixteenth of the tiles
-        const long long all_tiles = views * T;
+        HC_TRY(ws.tile_state.ensure(sizeof(int2) * (size_t)tiles));
+        HC_TRY(ws.bins.ensure(sizeof(int) * (size_t)tiles * ws.bin_cap));
+        // crumpled meshes overflow many bins: room for four spilled pairs per
+        // (view, triangle), and a key block for every tile while that stays
+        // under 4 GB (a quarter of the tiles beyond); overflow is reported by
+        // hc_renderer_stats
+        ws.spill_cap = std::max<long long>(1 << 22, 4ll * views * F);
+        HC_TRY(ws.spill.ensure(sizeof(int2) * (size_t)ws.spill_cap));
         const long long per_tile = (long long)TS * TS * sizeof(unsigned long long);
-        ws.spill_tile_cap = (int)(all_tiles * per_tile <= (256ll << 20) ? all_tiles
-                                                                         : std::max<long long>(256, all_tiles / 16));
+        ws.spill_tile_cap = (int)(tiles * per_tile <= (4ll << 30) ? tiles : std::max<long long>(256, tiles / 4));
         HC_TRY(ws.spill_keys.ensure(sizeof(unsigned long long) * (size_t)ws.spill_tile_cap * TS * TS));
         HC_TRY(ws.stats.ensure(sizeof(RasterStats)));
         ws.cap_views = views;
@@ -690,26 +765,27 @@ hc_status raster_reserve(RasterWorkspace& ws, int views, int F, int W, int H) {
     return HC_OK;
 }
 
-hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int W, int H,
-                         int albedo, int shading, const float* verts, const float* colors, const float* texture,
-                         int tex_h, int tex_w, const float* sh, const float* extr, const float* intr, float* bary,
-                         int* face, float* render, float* vnormal, int* depth_q, int* tie_count) {
+hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int albedo,
+                         int shading, const float* verts, const float* colors, const float* texture, int tex_h,
+                         int tex_w, const float* sh, const float* extr, const float* intr, float* bary, int* face,
+                         float* render, float* vnormal, int* depth_q, int* tie_count) {
     const int V = B * C;
     const int N = topo.N, F = topo.F;
-    HC_TRY(raster_reserve(ws, V, F, W, H));
+    HC_TRY(raster_reserve(ws, V, F));
     HC_TRY(ws.tri_frame.ensure(sizeof(TriFrame) * (size_t)B * F));
     const int TS = ws.tile;
-    const int T = ws.tiles_x * ws.tiles_y;
+    const long long tiles = (long long)B * ws.T_frame;
     ViewCam* cams = ws.cams.as<ViewCam>();
     TriFrame* tf = ws.tri_frame.as<TriFrame>();
     TriView* tv = ws.tri_view.as<TriView>();
     int2* tstate = ws.tile_state.as<int2>();
     RasterStats* stats = ws.stats.as<RasterStats>();
 
-    HC_CUDA(cudaMemsetAsync(tstate, 0, sizeof(int2) * (size_t)V * T, s));
+    HC_CUDA(cudaMemsetAsync(tstate, 0, sizeof(int2) * (size_t)tiles, s));
     HC_CUDA(cudaMemsetAsync(stats, 0, sizeof(RasterStats), s));
     ws.clock.begin(kKViewSetup, s);
-    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, extr, intr, cams);
+    k_view_setup<<<div_up(V, 64), 64, 0, s>>>(V, C, extr, intr, ws.layout.as<CamLayout>(), ws.P_frame, ws.T_frame,
+                                              ws.Tb_frame, cams);
     HC_CHECK_LAUNCH();
     ws.clock.end(kKViewSetup, s);
     ws.clock.begin(kKVertexNormals, s);
@@ -723,15 +799,15 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     ws.clock.end(kKTriFrame, s);
     ws.clock.begin(kKBin, s);
     k_bin<<<div_up((long long)V * F, 256), 256, 0, s>>>(
-        V, C, F, N, W, H, TS, ws.tiles_x, ws.tiles_y, ws.bin_cap, topo.faces.as<int3>(), verts, cams, tf, tv, tstate,
-        ws.bins.as<int>(), ws.spill.as<int4>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(),
-        ws.spill_tile_cap, stats);
+        V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), verts, cams, tf, tv, tstate, ws.bins.as<int>(),
+        ws.spill.as<int2>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap, stats);
     HC_CHECK_LAUNCH();
     ws.clock.end(kKBin, s);
     ws.clock.begin(kKSpill, s);
-    k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
-                                    ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(), stats,
-                                    nullptr, nullptr, T);
+    k_spill<<<148 * 4, 128, 0, s>>>(C, F, TS, ws.T_frame, ws.tile_cam.as<int>(), cams, tf, tv, tstate,
+                                    ws.spill.as<int2>(), ws.spill_cap,
+                                    ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(), stats, nullptr,
+                                    nullptr);
     HC_CHECK_LAUNCH();
     ws.clock.end(kKSpill, s);
     ShadeArgs A;
@@ -739,8 +815,6 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.C = C;
     A.N = N;
     A.F = F;
-    A.W = W;
-    A.H = H;
     A.albedo = albedo;
     A.shading = shading;
     A.faces = topo.faces.as<int3>();
@@ -757,19 +831,23 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.render = render;
     A.depth_q = depth_q;
     A.tie_count = tie_count;
-    const dim3 grid(T, V);
+    const int* tcam = ws.tile_cam.as<int>();
+    HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
+    const unsigned grid = (unsigned)tiles;
     ws.clock.begin(kKResolve, s);
     switch (TS) {
         case 8:
-            k_resolve<8><<<grid, 64, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate, ws.bins.as<int>(),
-                                             ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap);
+            k_resolve<8><<<grid, 64, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
+                                             ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
+                                             ws.spill_tile_cap);
             break;
         case 16:
-            k_resolve<16><<<grid, 256, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate, ws.bins.as<int>(),
-                                               ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap);
+            k_resolve<16><<<grid, 256, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
+                                               ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
+                                               ws.spill_tile_cap);
             break;
         case 32:
-            k_resolve<32><<<grid, 1024, 0, s>>>(A, ws.tiles_x, T, ws.bin_cap, cams, tf, tv, tstate,
+            k_resolve<32><<<grid, 1024, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
                                                 ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
                                                 ws.spill_tile_cap);
             break;
@@ -779,9 +857,10 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     HC_CHECK_LAUNCH();
     ws.clock.end(kKResolve, s);
     if (tie_count && depth_q) {
-        k_spill<<<148 * 4, 128, 0, s>>>(C, F, W, H, TS, ws.tiles_x, cams, tf, tv, tstate, ws.spill.as<int4>(),
-                                        ws.spill_cap, ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(),
-                                        stats, depth_q, tie_count, T);
+        k_spill<<<148 * 4, 128, 0, s>>>(C, F, TS, ws.T_frame, ws.tile_cam.as<int>(), cams, tf, tv, tstate,
+                                    ws.spill.as<int2>(), ws.spill_cap,
+                                        ws.spill_tile_cap, ws.spill_keys.as<unsigned long long>(), stats, depth_q,
+                                        tie_count);
         HC_CHECK_LAUNCH();
     }
     return HC_OK;

@@ -137,13 +137,13 @@ __global__ void k_vertex_normals(int B, int C, int N, const int3* __restrict__ f
                                  const int2* __restrict__ vf_id, const float* __restrict__ verts,
                                  float* __restrict__ out);
 
-hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, int W, int H, int mode,
+hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, long long P_frame, int mode,
                          const float* verts, int tex_h, int tex_w, float* bary, int* face, float* render,
                          float* vnormal, float* uv_map) {
     HC_REQUIRE(topo.has_texcoords, "compute_normal_map needs texture_coordinates");
     HC_REQUIRE(tex_h > 0 && tex_w > 0, "compute_normal_map needs the texture size");
     HC_REQUIRE(uv_map, "compute_normal_map needs the normal_map output");
-    const long long px = (long long)B * C * H * W;
+    const long long px = (long long)B * P_frame;
     HC_CUDA(cudaMemsetAsync(face, 0xff, sizeof(int) * px, s));
     HC_CUDA(cudaMemsetAsync(bary, 0, sizeof(float) * 2 * px, s));
     HC_CUDA(cudaMemsetAsync(render, 0, sizeof(float) * 3 * px, s));

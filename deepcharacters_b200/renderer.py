@@ -3,7 +3,8 @@
 Mirrors the reference Python class (Projects/CudaRenderer/CudaRendererGPU.py:25-237)
 and its op attributes (CudaRenderer/cpp/src/TensorflowOperators/CudaRenderer/
 CudaRenderer.cpp:5-31): same constructor arguments, same outputs and
-getters, same gradient rule (only ``vertexColor`` and ``textured`` produce
+getters, same gradient rule (only ``vertexColor`` and ``textured`` -- and the
+added ``texturedBilinear`` -- produce
 gradients; target image and cameras always get zeros).  Tensors are torch
 CUDA tensors; the work runs in ``libhc.so`` on the current CUDA stream.
 """
@@ -17,7 +18,8 @@ import torch
 
 from . import _lib
 
-ALBEDO_MODES = ("vertexColor", "textured", "normal", "lighting", "foregroundMask", "position", "depth", "uv")
+ALBEDO_MODES = ("vertexColor", "textured", "normal", "lighting", "foregroundMask", "position", "depth", "uv",
+                "texturedBilinear")  # the last: bilinear texture sampling, no reference counterpart
 SHADING_MODES = ("shaded", "shadeless")
 NORMAL_MAP_MODES = ("none", "normal", "position", "face")
 
@@ -48,8 +50,16 @@ class RendererEngine:
         self.F = f.size // 3
         self.N = int(n_vertices)
         self.C = int(n_cameras)
-        self.W = int(width)
-        self.H = int(height)
+        # width / height: one size for all cameras, or one per camera (views of
+        # different sizes then share one launch; image buffers are flat
+        # [B, pixels of a frame, ...] with the frame's cameras concatenated)
+        ws = np.broadcast_to(np.asarray(width, np.int32), (self.C,)).copy()
+        hs = np.broadcast_to(np.asarray(height, np.int32), (self.C,)).copy()
+        self.multires = not (np.all(ws == ws[0]) and np.all(hs == hs[0]))
+        self.widths, self.heights = ws, hs
+        self.W = int(ws[0])
+        self.H = int(hs[0])
+        self.P_frame = int((ws.astype(np.int64) * hs).sum())
         self.albedo_mode = albedo_mode
         self.shading_mode = shading_mode
         self.image_filter_size = int(image_filter_size)
@@ -58,11 +68,31 @@ class RendererEngine:
         self.faces = f
         self.tex_coords = tc
         h = C.c_void_p()
-        _lib.call("hc_renderer_create", C.byref(h), f.ctypes.data, self.F,
-                  None if tc is None else tc.ctypes.data, 0 if tc is None else tc.size,
-                  self.N, self.C, self.W, self.H, albedo_mode.encode(), shading_mode.encode(),
-                  self.image_filter_size, self.texture_filter_size, compute_normal_map.encode())
+        if self.multires:
+            _lib.call("hc_renderer_create_multires", C.byref(h), f.ctypes.data, self.F,
+                      None if tc is None else tc.ctypes.data, 0 if tc is None else tc.size, self.N, self.C,
+                      ws.ctypes.data, hs.ctypes.data, albedo_mode.encode(), shading_mode.encode(),
+                      self.image_filter_size, self.texture_filter_size, compute_normal_map.encode())
+        else:
+            _lib.call("hc_renderer_create", C.byref(h), f.ctypes.data, self.F,
+                      None if tc is None else tc.ctypes.data, 0 if tc is None else tc.size,
+                      self.N, self.C, self.W, self.H, albedo_mode.encode(), shading_mode.encode(),
+                      self.image_filter_size, self.texture_filter_size, compute_normal_map.encode())
         self._h = h
+
+    def image_shape(self, B: int) -> tuple:
+        """Leading shape of the per-pixel buffers: [B, C, H, W] or, with
+        per-camera sizes, [B, pixels of a frame]."""
+        return (B, self.P_frame) if self.multires else (B, self.C, self.H, self.W)
+
+    def split_views(self, img: torch.Tensor) -> list:
+        """[B, P_frame, ...] buffer -> per camera [B, H_c, W_c, ...] views (no copy)."""
+        out, o = [], 0
+        for w, h in zip(self.widths, self.heights):
+            n = int(w) * int(h)
+            out.append(img[:, o:o + n].reshape((img.shape[0], int(h), int(w)) + tuple(img.shape[2:])))
+            o += n
+        return out
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -118,19 +148,19 @@ class RendererEngine:
         TH = int(tex.shape[1]) if tex is not None and tex.dim() == 4 else 0
         TW = int(tex.shape[2]) if tex is not None and tex.dim() == 4 else 0
         o = out or {}
+        img = self.image_shape(B)
         bary = o.get("bary") if o.get("bary") is not None else torch.empty(
-            (B, self.C, self.H, self.W, 2), device=dev, dtype=torch.float32)
-        face = o.get("face") if o.get("face") is not None else torch.empty(
-            (B, self.C, self.H, self.W), device=dev, dtype=torch.int32)
+            img + (2,), device=dev, dtype=torch.float32)
+        face = o.get("face") if o.get("face") is not None else torch.empty(img, device=dev, dtype=torch.int32)
         render = o.get("render") if o.get("render") is not None else torch.empty(
-            (B, self.C, self.H, self.W, 3), device=dev, dtype=torch.float32)
+            img + (3,), device=dev, dtype=torch.float32)
         vnormal = o.get("vnormal") if o.get("vnormal") is not None else torch.empty(
             (B, self.C, self.N, 3), device=dev, dtype=torch.float32)
         normal_map = torch.zeros((B, max(TH, 1), max(TW, 1), 3), device=dev, dtype=torch.float32)
         depth_q = tie = None
         if diagnostics:
-            depth_q = torch.empty((B, self.C, self.H, self.W), device=dev, dtype=torch.int32)
-            tie = torch.empty((B, self.C, self.H, self.W), device=dev, dtype=torch.int32)
+            depth_q = torch.empty(img, device=dev, dtype=torch.int32)
+            tie = torch.empty(img, device=dev, dtype=torch.int32)
         P = _lib.ptr
         _lib.call("hc_renderer_forward_ex", self._h, _stream(), B, P(vp), P(vc), P(tex), TH, TW, P(sh), P(ex), P(it),
                   P(bary), P(face), P(render), P(vnormal),
@@ -179,7 +209,7 @@ class _RenderFn(torch.autograd.Function):
         eng: RendererEngine = ctx.engine
         zeros = [torch.zeros_like(t) if t is not None else None
                  for t in (vertex_pos, vertex_color, texture, sh_coeff)]
-        if eng.albedo_mode in ("vertexColor", "textured") and g_render is not None:
+        if eng.albedo_mode in ("vertexColor", "textured", "texturedBilinear") and g_render is not None:
             grads = renderer_backward(eng, g_render, vertex_pos, vertex_color, texture, sh_coeff, target_image,
                                       vnormal, bary, face, extrinsics, intrinsics)
         else:

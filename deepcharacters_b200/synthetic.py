@@ -229,13 +229,25 @@ def rest_joint_positions(sk: Skeleton) -> np.ndarray:
     return p
 
 
-def skinning_weights(verts: np.ndarray, sk: Skeleton, k: int, rng: np.random.Generator):
+def skinning_weights(verts: np.ndarray, sk: Skeleton, k: int, rng: np.random.Generator, smooth: bool = False):
     """Per vertex the ``k`` nearest skinning joints (Euclidean, rest pose) with
-    Dirichlet(1) weights.  Returns ``(indices[N,k] int32, weights[N,k] float32)``."""
+    Dirichlet(1) weights, or with ``smooth`` weights that are continuous over
+    the surface (neighbouring vertices get nearly equal blends, so large joint
+    angles fold the surface instead of tearing it).
+    Returns ``(indices[N,k] int32, weights[N,k] float32)``."""
     jp = rest_joint_positions(sk)[sk.skin_joint]
     d = np.linalg.norm(verts[:, None, :].astype(np.float64) - jp[None], axis=2)
     idx = np.argsort(d, axis=1, kind="stable")[:, :k].astype(np.int32)
-    w = rng.dirichlet(np.ones(k), size=verts.shape[0]).astype(np.float32)
+    if smooth:
+        # w_k proportional to (distance of the (k+1)-th nearest joint - own
+        # distance): a joint's weight falls to zero exactly where it leaves
+        # the k nearest, so the weights are continuous over the surface
+        order = np.argsort(d, axis=1, kind="stable")
+        dk = np.take_along_axis(d, order[:, :k + 1], axis=1)
+        w = dk[:, k:k + 1] - dk[:, :k] + 1e-6
+        w = (w / w.sum(axis=1, keepdims=True)).astype(np.float32)
+    else:
+        w = rng.dirichlet(np.ones(k), size=verts.shape[0]).astype(np.float32)
     return idx, w
 
 

@@ -73,6 +73,21 @@ hc_status hc_renderer_create(hc_renderer* out, const int32_t* faces, int32_t n_f
                              const char* albedo_mode, const char* shading_mode,
                              int32_t image_filter_size, int32_t texture_filter_size,
                              const char* compute_normal_map);
+/* hc_renderer_create with one resolution per camera (camera_widths /
+ * camera_heights [C], host; no reference counterpart: the reference op has
+ * one render_resolution_u/v).  Views of different sizes are rasterised in
+ * one launch.  Every per-pixel buffer of a call is then [B, P, ...] with P
+ * the pixels of a frame (hc_renderer_frame_pixels), the frame's cameras
+ * concatenated in order, each row-major H_c x W_c. */
+hc_status hc_renderer_create_multires(hc_renderer* out, const int32_t* faces, int32_t n_faces,
+                                      const float* texture_coordinates, int32_t n_texcoords,
+                                      int32_t number_of_vertices, int32_t number_of_cameras,
+                                      const int32_t* camera_widths, const int32_t* camera_heights,
+                                      const char* albedo_mode, const char* shading_mode,
+                                      int32_t image_filter_size, int32_t texture_filter_size,
+                                      const char* compute_normal_map);
+/* pixels of one frame (sum over cameras of W_c * H_c) */
+hc_status hc_renderer_frame_pixels(hc_renderer h, int64_t* pixels);
 hc_status hc_renderer_destroy(hc_renderer h);
 
 /* Pre-size the workspace for up to `batch` frames (no allocation afterwards). */

@@ -1,0 +1,141 @@
+"""Stress case at full size: icosphere subdivision 8 (655,362 vertices /
+1,310,720 triangles) folded into self-occlusion, 5 % of the triangles
+duplicated with vertex offsets of 0 or 1 ulp (every duplicate is a
+quantised-depth tie with its original), 8 frames x 8 views at 2048x2048.
+
+The synthetic character's joint angles are U(-0.75, 0.75) with skinning
+weights that are continuous over the surface.  With the nominal U(-1.5, 1.5)
+the random 24-joint tree stretches triangles across the whole image: ~2e7 tile
+bin entries and ~4e9 bounding-box pixels per view, a 2.4e11-test workload for
+the reference's own per-triangle loops at 64 views.
+
+The face buffer must equal the reference kernels' everywhere except pixels
+where two triangles share the minimum quantised depth (the reference picks
+one of them by a race); barycentrics and colours must be bit-identical where
+the faces agree.  The spill-over rate of the tile bins and the tie counts are
+printed (pytest -s)."""
+import numpy as np
+import pytest
+import torch
+
+from deepcharacters_b200 import synthetic as S
+from deepcharacters_b200.renderer import RendererEngine
+from deepcharacters_b200.skinning import Character, SkinningEngine
+from oracle import oracle as O
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not O.ref_available(), reason="reference kernels (oracle/_ref) not built")]
+DEV = "cuda:0"
+FRAMES, VIEWS, RES = 8, 8, 2048
+
+
+def stress_scene(seed=5):
+    rng = S.rng_for(seed)
+    verts, faces = S.sphere_mesh(8, rng)
+    sk = S.random_skeleton(24, rng)
+    idx, w = S.skinning_weights(verts, sk, 4, rng, smooth=True)
+    dofs = np.stack([S.random_pose(sk, S.rng_for(seed, b), 0.75) for b in range(FRAMES)])
+    ch = Character.from_synthetic(sk, verts, faces, idx)
+    eng = SkinningEngine(ch)
+    wt = torch.from_numpy(np.ascontiguousarray(np.tile(w[None], (FRAMES, 1, 1)))).to(DEV)
+    v = eng.dq_forward(torch.from_numpy(dofs).to(DEV), wt)[0].cpu().numpy()
+    # 5 % of the faces again, on copies of their vertices nudged by 0 or 1 ulp
+    F, N = faces.shape[0], verts.shape[0]
+    dup = rng.choice(F, size=F // 20, replace=False)
+    dv = v[:, faces[dup].reshape(-1)]
+    step = rng.integers(0, 2, size=dv.shape).astype(bool)
+    direction = np.where(rng.integers(0, 2, size=dv.shape) == 1, np.inf, -np.inf).astype(np.float32)
+    dv = np.where(step, np.nextafter(dv, direction), dv).astype(np.float32)
+    verts_all = np.concatenate([v, dv], axis=1)
+    faces_all = np.concatenate([faces, (N + np.arange(3 * len(dup))).reshape(-1, 3)]).astype(np.int32)
+    ex, it = S.camera_ring(VIEWS, 3000.0, 600.0 * RES / 512, RES, RES)
+    colors = rng.uniform(0, 1, size=(FRAMES, verts_all.shape[1], 3)).astype(np.float32)
+    return dict(verts=verts_all, faces=faces_all, colors=colors, extr=np.tile(ex[None], (FRAMES, 1)),
+                intr=np.tile(it[None], (FRAMES, 1)), n_dup=len(dup))
+
+
+def test_stress_face_buffer_bit_exact_outside_ties():
+    sc = stress_scene()
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    N = sc["verts"].shape[1]
+    verts, colors, extr, intr = t(sc["verts"]), t(sc["colors"]), t(sc["extr"]), t(sc["intr"])
+    tex = torch.zeros((FRAMES, 1, 1, 3), device=DEV)
+    sh = torch.zeros((FRAMES, VIEWS, 27), device=DEV)
+    eng = RendererEngine(sc["faces"], None, N, VIEWS, RES, RES, "vertexColor", "shadeless", 2, 2)
+    eng.set_tuning(16, 2048)
+    bary, face, render, _, _, dq, tie = eng.forward(verts, colors, tex, sh, extr, intr, diagnostics=True)
+    binned, spilled = eng.stats()
+    ref = O.RefRenderer(sc["faces"], None, N, VIEWS, RES, RES, "vertexColor", "shadeless")
+    r = ref.forward(FRAMES, verts, colors, tex, sh, extr, intr, depth=False, sync_each=0)
+    torch.cuda.synchronize()
+    ties = tie >= 2
+    mism = face != r["face"]
+    covered = int((r["face"] >= 0).sum())
+    print(f"\nstress: {FRAMES}x{VIEWS} views {RES}^2, {sc['faces'].shape[0]} triangles ({sc['n_dup']} duplicated); "
+          f"covered px {covered}, tie px {int(ties.sum())} ({ties.sum().item() / max(covered, 1):.4f}), "
+          f"face mismatches {int(mism.sum())} (all at ties: {not bool((mism & ~ties).any())}); "
+          f"bin entries {binned}, spilled {spilled} ({spilled / max(binned + spilled, 1):.2e})")
+    assert covered > 10 ** 7
+    assert int(ties.sum()) > 0
+    assert not bool((mism & ~ties).any()), int((mism & ~ties).sum())
+    # at ties the reference's buffers can also be torn (F2), so compare elsewhere
+    same = (~mism) & (~ties) & (face >= 0)
+    assert torch.equal(bary[same], r["bary"][same])
+    assert torch.equal(render[same], r["render"][same])
+
+
+def test_c4_textured_dq_lbs_blend_matches_reference():
+    """Config 4 at full size: icosphere subdivision 7 (327,680 triangles) with
+    spherical UVs and a 1024x1024 texture, skinned by 0.5 DQ + 0.5 LBS, 4 views
+    at 2048x2048, nearest-texel textured mode (the reference's) against the
+    reference kernels, and its adjoint in parity mode."""
+    rng = S.rng_for(4)
+    verts, faces = S.sphere_mesh(7, rng)
+    sk = S.random_skeleton(24, rng)
+    idx, w = S.skinning_weights(verts, sk, 4, rng)
+    dofs = S.random_pose(sk, S.rng_for(4, 0), 0.5)[None]
+    ch = Character.from_synthetic(sk, verts, faces, idx)
+    eng = SkinningEngine(ch)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(DEV)  # noqa: E731
+    wt = t(w[None])
+    v_dq = eng.dq_forward(t(dofs), wt)[0]
+    v_lbs = eng.lbs_forward(t(dofs), wt, torch.zeros((1, verts.shape[0], 3), device=DEV))[0]
+    v = (0.5 * v_dq + 0.5 * v_lbs).contiguous()
+    N = verts.shape[0]
+    ex, it = S.camera_ring(4, 3000.0, 600.0 * RES / 512, RES, RES)
+    extr, intr = t(ex[None]), t(it[None])
+    tex = t(rng.uniform(0, 1, size=(1, 1024, 1024, 3)).astype(np.float32))
+    texcoords = S.spherical_uvs(verts, faces)
+    sh = t(S.sh_coefficients(4, rng).reshape(1, 4, 27))
+    colors = torch.zeros((1, N, 3), device=DEV)
+    ours = RendererEngine(faces, texcoords, N, 4, RES, RES, "textured", "shaded", 2, 2)
+    ours.set_tuning(16, 2048)  # the crumpled 2048^2 views overflow smaller bins heavily
+    bary, face, render, vn, _, dq, tie = ours.forward(v, colors, tex, sh, extr, intr, diagnostics=True)
+    binned, spilled = ours.stats()  # raises on spill overflow
+    ref = O.RefRenderer(faces, texcoords, N, 4, RES, RES, "textured", "shaded")
+    r = ref.forward(1, v, colors, tex, sh, extr, intr, depth=False, sync_each=0)
+    torch.cuda.synchronize()
+    ties = tie >= 2
+    mism = face != r["face"]
+    assert int((r["face"] >= 0).sum()) > 10 ** 6
+    assert not bool((mism & ~ties).any()), int((mism & ~ties).sum())
+    same = (~mism) & (~ties) & (face >= 0)
+    assert float((render[same] - r["render"][same]).abs().max()) < 1e-5
+    # adjoint in parity mode on the reference forward's buffers
+    g = torch.randn(render.shape, device=DEV, generator=torch.Generator(DEV).manual_seed(2))
+    target = t(rng.uniform(0, 1, size=tuple(render.shape)).astype(np.float32))
+    rg = ref.backward(1, g, v, colors, tex, sh, target, r["vnormal"], r["bary"], r["face"], extr, intr)
+    ours.set_gradient_parity(True)
+    from deepcharacters_b200.renderer import renderer_backward
+    gpos, _, gtex, gsh = renderer_backward(ours, g, v, colors, tex, sh, target, r["vnormal"], r["bary"], r["face"],
+                                           extr, intr)
+    torch.cuda.synchronize()
+
+    def nrel(a, b):
+        return float((a.double() - b.double()).norm() / b.double().norm())
+
+    print(f"\nc4: covered {int((face >= 0).sum())}, ties {int(ties.sum())}, spilled {spilled}/{binned + spilled}, pos-grad {nrel(gpos, rg['vertex_pos_grad']):.2e}, "
+          f"tex-grad {nrel(gtex, rg['texture_grad']):.2e}, sh-grad {nrel(gsh, rg['sh_coeff_grad']):.2e}")
+    assert nrel(gpos, rg["vertex_pos_grad"]) < 1e-5
+    assert nrel(gtex, rg["texture_grad"]) < 1e-5
+    assert nrel(gsh, rg["sh_coeff_grad"]) < 1e-5
