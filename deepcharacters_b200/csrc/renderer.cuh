@@ -345,6 +345,7 @@ struct RasterWorkspace {
     long long spill_cap = 0;
     int spill_tile_cap = 0;
     DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;
+    DevBuf proj;  // float4 [V,N]: projected vertices of the current call
     KernelClock clock;
 };
 

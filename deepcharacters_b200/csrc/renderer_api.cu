@@ -175,7 +175,7 @@ static void release_all(hc_renderer_s* r) {
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
                       &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
-                      &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b};
+                      &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b, &r->ws.proj};
     for (DevBuf* b : bufs) b->release();
 }
 
@@ -192,6 +192,7 @@ extern "C" hc_status hc_renderer_reserve(hc_renderer h, int32_t batch) {
     HC_REQUIRE(h && batch > 0, "invalid handle or batch");
     HC_TRY(raster_reserve(h->ws, batch * h->C, h->topo.F));
     HC_TRY(h->ws.tri_frame.ensure(sizeof(TriFrame) * (size_t)batch * h->topo.F));
+    HC_TRY(h->ws.proj.ensure(sizeof(float4) * (size_t)batch * h->C * h->topo.N));
     return HC_OK;
 }
 

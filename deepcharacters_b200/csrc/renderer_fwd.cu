@@ -138,6 +138,21 @@ __global__ void k_tri_frame(int B, int F, int N, const int3* __restrict__ faces,
 }
 
 // ---------------------------------------------------------------------------
+// per-view vertex projection (reference projectVerticesDevice,
+// CUDABasedRasterization.cu:98-115): once per (view, vertex) instead of three
+// times per (view, triangle); the same function, so the same values
+// ---------------------------------------------------------------------------
+__global__ void k_project_vertices(int V, int C, int N, const float* __restrict__ verts,
+                                   const ViewCam* __restrict__ cams, float4* __restrict__ proj) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)V * N) return;
+    const int view = (int)(i / N), v = (int)(i % N);
+    const ViewCam& cam = cams[view];
+    const float3 p = project_point(cam.ext, cam.intr, ld3(verts + ((long long)(view / C) * N + v) * 3));
+    proj[i] = make_float4(p.x, p.y, p.z, 0.f);
+}
+
+// ---------------------------------------------------------------------------
 // per-view triangle set-up and screen-tile binning
 //
 // The pixel bbox is the reference's projectFacesDevice (CUDABasedRasterization.cu:
@@ -188,7 +203,7 @@ struct BinSink {
 };
 
 __global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
-                      const int3* __restrict__ faces, const float* __restrict__ verts,
+                      const int3* __restrict__ faces, const float4* __restrict__ proj,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
                       int2* __restrict__ spill, long long spill_cap, unsigned long long* __restrict__ spill_keys,
@@ -209,11 +224,11 @@ __global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
         H = cam.H;
         tiles_x = cam.tiles_x;
         tile_base = cam.tile_base;
-        const float* P = verts + (long long)b * N * 3;
         const int3 id = faces[f];
-        const float3 p0 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.x));
-        const float3 p1 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.y));
-        const float3 p2 = project_point(cam.ext, cam.intr, ld3(P + 3 * id.z));
+        const float4* PV = proj + (long long)view * N;
+        const float4 q0 = PV[id.x], q1 = PV[id.y], q2 = PV[id.z];
+        const float3 p0 = make_float3(q0.x, q0.y, q0.z), p1 = make_float3(q1.x, q1.y, q1.z),
+                     p2 = make_float3(q2.x, q2.y, q2.z);
         x0 = (int)fmaxf(fminf(p0.x, fminf(p1.x, p2.x)) - 0.5f, 0.f);
         y0 = (int)fmaxf(fminf(p0.y, fminf(p1.y, p2.y)) - 0.5f, 0.f);
         x1 = (int)fminf(fmaxf(p0.x, fmaxf(p1.x, p2.x)) + 0.5f, (float)(W - 1));
@@ -373,6 +388,7 @@ __global__ void k_spill(int C, int F, int TS, long long T_frame, const int* __re
 // ---------------------------------------------------------------------------
 struct ShadeArgs {
     int B, C, N, F;
+    const float4* proj;  // [V,N] projected vertices
     int albedo, shading;
     const int3* faces;
     const float* texcoords;
@@ -578,13 +594,11 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
                         const TriFrame tf = tri_frame[(long long)b * A.F + f];
                         const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
                         const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
-                        const float3 q0 =
-                            project_point(cam.ext, cam.intr, make_float3(tf.a.x, tf.a.y, tf.a.z) * 1000.f);
-                        const float3 q1 =
-                            project_point(cam.ext, cam.intr, make_float3(tf.b.x, tf.b.y, tf.b.z) * 1000.f);
-                        const float3 q2 =
-                            project_point(cam.ext, cam.intr, make_float3(tf.c.x, tf.c.y, tf.c.z) * 1000.f);
-                        const Footprint fp = footprint(q0, q1, q2);
+                        const int3 id = A.faces[f];
+                        const float4* PV = A.proj + (long long)view * A.N;
+                        const float4 r0 = PV[id.x], r1 = PV[id.y], r2 = PV[id.z];
+                        const Footprint fp = footprint(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z),
+                                                       make_float3(r2.x, r2.y, r2.z));
                         TileTri t;
                         t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
                                           (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
@@ -773,6 +787,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     const int N = topo.N, F = topo.F;
     HC_TRY(raster_reserve(ws, V, F));
     HC_TRY(ws.tri_frame.ensure(sizeof(TriFrame) * (size_t)B * F));
+    HC_TRY(ws.proj.ensure(sizeof(float4) * (size_t)V * N));
     const int TS = ws.tile;
     const long long tiles = (long long)B * ws.T_frame;
     ViewCam* cams = ws.cams.as<ViewCam>();
@@ -798,8 +813,11 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     HC_CHECK_LAUNCH();
     ws.clock.end(kKTriFrame, s);
     ws.clock.begin(kKBin, s);
+    k_project_vertices<<<div_up((long long)V * N, 256), 256, 0, s>>>(V, C, N, verts, cams, ws.proj.as<float4>());
+    HC_CHECK_LAUNCH();
     k_bin<<<div_up((long long)V * F, 256), 256, 0, s>>>(
-        V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), verts, cams, tf, tv, tstate, ws.bins.as<int>(),
+        V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), ws.proj.as<float4>(), cams, tf, tv, tstate,
+        ws.bins.as<int>(),
         ws.spill.as<int2>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap, stats);
     HC_CHECK_LAUNCH();
     ws.clock.end(kKBin, s);
@@ -815,6 +833,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.C = C;
     A.N = N;
     A.F = F;
+    A.proj = ws.proj.as<float4>();
     A.albedo = albedo;
     A.shading = shading;
     A.faces = topo.faces.as<int3>();
