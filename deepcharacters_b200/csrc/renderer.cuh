@@ -33,6 +33,8 @@ struct ViewCam {
     float intr[9];   // row-major 3x3
     float ro[3];     // ray origin (camera centre)
     float ro_s[3];   // ray origin / 1000
+    float KE[9];     // K * E[:, :3] (row-major): world -> homogeneous pixel, linear part
+    float Kt[3];     // K * E[:, 3]
     // the view's image: resolution, tile grids and where its pixels / tiles
     // start in the call's buffers (cameras of a frame may differ in size)
     int W, H, tiles_x, tiles_x_b;

@@ -427,26 +427,18 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
                 }
             }
             if (gu != 0.f || gv != 0.f) {
-                const float* e = cam.ext;
-                const float* k = cam.intr;
-                const float3 cs = make_float3(e[0] * frag.x + e[1] * frag.y + e[2] * frag.z + e[3],
-                                              e[4] * frag.x + e[5] * frag.y + e[6] * frag.z + e[7],
-                                              e[8] * frag.x + e[9] * frag.y + e[10] * frag.z + e[11]);
-                const float3 Pp = make_float3(k[0] * cs.x + k[1] * cs.y + k[2] * cs.z,
-                                              k[3] * cs.x + k[4] * cs.y + k[5] * cs.z,
-                                              k[6] * cs.x + k[7] * cs.y + k[8] * cs.z);
+                // pixel position of the fragment, P = K (E frag), and its
+                // Jacobian d(u, v)/d frag = (KE_0 - u KE_2, KE_1 - v KE_2) / P_z
+                const float* KE = cam.KE;
+                const float3 Pp = make_float3(KE[0] * frag.x + KE[1] * frag.y + KE[2] * frag.z + cam.Kt[0],
+                                              KE[3] * frag.x + KE[4] * frag.y + KE[5] * frag.z + cam.Kt[1],
+                                              KE[6] * frag.x + KE[7] * frag.y + KE[8] * frag.z + cam.Kt[2]);
                 if (fabsf(Pp.z) > 0.0001f) {
                     const float iz = 1.f / Pp.z;
-                    const float dx = -Pp.x / (Pp.z * Pp.z), dy = -Pp.y / (Pp.z * Pp.z);
-                    float KE[3][3];
-#pragma unroll
-                    for (int r = 0; r < 3; ++r)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            KE[r][c] = k[3 * r + 0] * e[c] + k[3 * r + 1] * e[4 + c] + k[3 * r + 2] * e[8 + c];
-                    m.x = -(gu * (iz * KE[0][0] + dx * KE[2][0]) + gv * (iz * KE[1][0] + dy * KE[2][0]));
-                    m.y = -(gu * (iz * KE[0][1] + dx * KE[2][1]) + gv * (iz * KE[1][1] + dy * KE[2][1]));
-                    m.z = -(gu * (iz * KE[0][2] + dx * KE[2][2]) + gv * (iz * KE[1][2] + dy * KE[2][2]));
+                    const float dx = -Pp.x * iz * iz, dy = -Pp.y * iz * iz;
+                    m.x = -(gu * (iz * KE[0] + dx * KE[6]) + gv * (iz * KE[3] + dy * KE[6]));
+                    m.y = -(gu * (iz * KE[1] + dx * KE[7]) + gv * (iz * KE[4] + dy * KE[7]));
+                    m.z = -(gu * (iz * KE[2] + dx * KE[8]) + gv * (iz * KE[5] + dy * KE[8]));
                 }
             }
         }

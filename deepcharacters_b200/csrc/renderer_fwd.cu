@@ -70,6 +70,13 @@ __global__ void k_view_setup(int V, int C, const float* __restrict__ extr, const
     for (int i = 0; i < 12; ++i) c.ext[i] = e[i];
 #pragma unroll
     for (int i = 0; i < 9; ++i) c.intr[i] = k[i];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+            c.KE[3 * r + cc] = k[3 * r + 0] * e[cc] + k[3 * r + 1] * e[4 + cc] + k[3 * r + 2] * e[8 + cc];
+        c.Kt[r] = k[3 * r + 0] * e[3] + k[3 * r + 1] * e[7] + k[3 * r + 2] * e[11];
+    }
     // camera centre: last column of inv(E), dehomogenised
     float4 o = make_float4(invE.e[3], invE.e[7], invE.e[11], invE.e[15]);
     const float w = o.w;
