@@ -184,49 +184,21 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
 enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2, kAlbTexBilinear = 3 };
 
 template <bool SHADED, int ALB, bool PARITY>
-__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams) {
+__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles) {
     constexpr int NVV = SHADED ? 9 : 6;               // values per vertex
     constexpr int NROW = (3 * NVV + 3) / 4 * 4;       // per-lane row, padded for float4 loads
     __shared__ __align__(16) float s_red[BNT / 32][32][NROW];
     __shared__ float s_sh[SHADED ? BNT / 32 : 1][27];
-    __shared__ float4 s_tgt[TILE_S * TILE_S];
+    __shared__ float4 s_tgt2[2][TILE_S * TILE_S];      // target tile + halo, double-buffered
     __shared__ float2 s_tap[MAXTAPS];  // image-gradient tap weights (i, j) / (i^2 + j^2)
     __shared__ float s_norm;
-    // one CTA per 16x16 tile of the call; the frame's cameras are concatenated
-    const long long g = blockIdx.x;
-    const int b = (int)(g / A.Tb_frame);
-    const int view = b * A.C + A.tile_cam_b[g % A.Tb_frame];
-    const ViewCam& cam = cams[view];
-    const int tile = (int)(g - cam.tile_base_b);
-    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x_b;
     constexpr bool shaded = SHADED;
     constexpr bool vcol = ALB == kAlbVcol;
     constexpr bool textured = ALB == kAlbTex;
     constexpr bool bilinear = ALB == kAlbTexBilinear;
-    const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
-    const int px = tx0 + threadIdx.x % BT;
-    const int py = ty0 + threadIdx.x / BT;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const float* tgt = A.target + cam.pix_base * 3;
-    // stage the target tile with the filter halo (clipped to the image)
     const bool staged = A.ifs <= MAXFS;
     if (staged) {
-        const int e = BT + 2 * A.ifs;
-        for (int i = threadIdx.x; i < e * e; i += BNT) {
-            const int yy = ty0 - A.ifs + i / e, xx = tx0 - A.ifs + i % e;
-            // asynchronous copies: the pixel work below that does not read the
-            // target overlaps them; they are waited for before the taps
-            if (xx >= 0 && yy >= 0 && xx < W && yy < H) {
-                const float* src = tgt + 3 * ((long long)yy * W + xx);
-                const unsigned dst = (unsigned)__cvta_generic_to_shared(&s_tgt[i]);
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4), "l"(src + 1));
-                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8), "l"(src + 2));
-            } else {
-                s_tgt[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-        }
-        asm volatile("cp.async.commit_group;\n" ::);
         // tap weights and their normaliser, once per CTA: the same divisions
         // and the same summation order as evaluating them per pixel
         const int fs = A.ifs, ew = 2 * fs + 1;
@@ -245,6 +217,47 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
             s_norm = norm;
         }
     }
+    // Persistent CTAs walk the 16x16 tiles of the call (the frame's cameras
+    // concatenated).  The target tile + filter halo of the next tile is
+    // copied into the other shared buffer with cp.async while this tile's
+    // pixels are processed, so the copy latency is hidden.
+    auto stage = [&](long long gt, int buf) {
+        const int sb = (int)(gt / A.Tb_frame);
+        const ViewCam& sc = cams[sb * A.C + A.tile_cam_b[gt % A.Tb_frame]];
+        const int st = (int)(gt - sc.tile_base_b);
+        const int sx0 = (st % sc.tiles_x_b) * BT, sy0 = (st / sc.tiles_x_b) * BT;
+        const float* stg = A.target + sc.pix_base * 3;
+        const int e = BT + 2 * A.ifs;
+        for (int i = threadIdx.x; i < e * e; i += BNT) {
+            const int yy = sy0 - A.ifs + i / e, xx = sx0 - A.ifs + i % e;
+            if (xx >= 0 && yy >= 0 && xx < sc.W && yy < sc.H) {
+                const float* src = stg + 3 * ((long long)yy * sc.W + xx);
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(&s_tgt2[buf][i]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4), "l"(src + 1));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 8), "l"(src + 2));
+            } else {
+                s_tgt2[buf][i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    };
+    if (staged && (long long)blockIdx.x < n_tiles) stage(blockIdx.x, 0);
+    asm volatile("cp.async.commit_group;\n" ::);
+    int it = 0;
+    for (long long g = blockIdx.x; g < n_tiles; g += gridDim.x, ++it) {
+    const int buf = it & 1;
+    const float4* s_tgt = s_tgt2[buf];
+    if (staged && g + gridDim.x < n_tiles) stage(g + gridDim.x, buf ^ 1);
+    asm volatile("cp.async.commit_group;\n" ::);
+    const int b = (int)(g / A.Tb_frame);
+    const int view = b * A.C + A.tile_cam_b[g % A.Tb_frame];
+    const ViewCam& cam = cams[view];
+    const int tile = (int)(g - cam.tile_base_b);
+    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x_b;
+    const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
+    const int px = tx0 + threadIdx.x % BT;
+    const int py = ty0 + threadIdx.x / BT;
+    const float* tgt = A.target + cam.pix_base * 3;
     float shg[SHADED ? 27 : 1];
 #pragma unroll
     for (int k = 0; k < (SHADED ? 27 : 1); ++k) shg[k] = 0.f;
@@ -380,7 +393,7 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
             gbc += make_float3(dot(gnu, n0), dot(gnu, n1), dot(gnu, n2));
         }
     }
-    if (staged) asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile's copies (the next tile's stay in flight)
     __syncthreads();
     if (f >= 0) {
         // model -> data: -G^T dTarget/d(u,v) d(u,v)/d(frag) d(frag)/d(v)
@@ -540,6 +553,9 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
             if (v != 0.f) atomicAdd(A.sh_grad + (long long)view * 27 + threadIdx.x, v);
         }
     }
+    __syncthreads();  // the next iteration's prefetch reuses this tile's buffer
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 // Normal chain, per (frame, vertex): for every incident face g = (x, y, z)
@@ -571,6 +587,24 @@ __global__ void k_normal_chain(int B, int N, const int3* __restrict__ faces, con
 }
 
 }  // namespace
+
+// CTAs of a persistent launch: as many as fit on the GPU at once (each walks
+// tiles blockIdx.x, + gridDim.x, ...), never more than the tiles
+template <class K>
+static unsigned persistent_grid(K kernel, long long tiles) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BNT, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    const long long g = (long long)sms * per_sm;
+    return (unsigned)std::max<long long>(1, std::min(g, tiles));
+}
 
 hc_status raster_layout(RasterWorkspace& ws);
 
@@ -625,8 +659,6 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.sh_grad = sh_grad;
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
     const long long tiles = (long long)B * ws.Tb_frame;
-    HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
-    const unsigned grid = (unsigned)tiles;
     ws.clock.begin(kKRenderGrad, s);
     const int alb = albedo == kVertexColor ? kAlbVcol
                     : albedo == kTextured ? kAlbTex
@@ -634,7 +666,10 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     const int sel = (shaded ? 8 : 0) + alb * 2 + (parity ? 1 : 0);
     switch (sel) {
 #define HC_GRAD_CASE(SH, AL, PA) \
-    case (SH ? 8 : 0) + AL * 2 + PA: k_render_grad<SH, AL, PA><<<grid, BNT, 0, s>>>(A, cams); break;
+    case (SH ? 8 : 0) + AL * 2 + PA:                                                                    \
+        k_render_grad<SH, AL, PA><<<persistent_grid(k_render_grad<SH, AL, PA>, tiles), BNT, 0, s>>>(A, cams, \
+                                                                                              tiles);     \
+        break;
         HC_GRAD_CASE(false, kAlbVcol, false)
         HC_GRAD_CASE(false, kAlbVcol, true)
         HC_GRAD_CASE(false, kAlbTex, false)

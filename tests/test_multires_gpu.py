@@ -64,6 +64,6 @@ def test_mixed_resolution_views_match_single_camera_calls(tile):
         p1, c1, _, s1 = renderer_backward(one, g1, verts, colors, tex, sh[:, c:c + 1], tg, vn1, b1, f1, ex1, in1)
         sum_pos += p1
         sum_col += c1
-        assert nrel(gsh[:, c], s1[:, 0]) < 1e-6
+        assert nrel(gsh[:, c], s1[:, 0]) < 1e-5  # float sums in a different order
     torch.cuda.synchronize()
     assert nrel(gpos, sum_pos) < 1e-5 and nrel(gcol, sum_col) < 1e-5
