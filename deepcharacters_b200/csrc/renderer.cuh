@@ -196,6 +196,7 @@ constexpr float kEdgeMargin = 0.125f;
 
 struct Footprint {
     float a[3], b[3], c[3];  // edge k: a*x + b*y + c >= 0 inside (margin included)
+    float m[3];              // the margin folded into c[k] (0 when disabled)
 };
 // A pixel centre whose three footprint values are all >= kEdgeInterior lies
 // inside the (unwidened) projected triangle by more than kEdgeMargin px: the
@@ -225,6 +226,7 @@ __device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, 
         fp.a[k] = -ey * inv;
         fp.b[k] = ex * inv;
         fp.c[k] = (ey * u.x - ex * u.y) * inv + margin;
+        fp.m[k] = ok ? margin : 0.f;
     }
     if (!ok) {  // disabled: every pixel is on the boundary band (passes, never "inside")
 #pragma unroll
@@ -232,6 +234,7 @@ __device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, 
             fp.a[k] = 0.f;
             fp.b[k] = 0.f;
             fp.c[k] = 0.f;
+            fp.m[k] = 0.f;
         }
     }
     return fp;

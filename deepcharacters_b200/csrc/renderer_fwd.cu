@@ -552,9 +552,11 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
                                                    int spill_tile_cap) {
     constexpr int NT = TS * TS;
     constexpr int CHUNK = NT > 256 ? 256 : NT;  // triangles staged per round
-    __shared__ TileTri s_tri[CHUNK];
-    __shared__ unsigned long long s_key[CHUNK];  // facing | depth lower bound | slot
-    __shared__ unsigned short s_order[CHUNK];    // slots in key order
+    constexpr int SB = CHUNK == 64 ? 6 : 8;     // slot bits of a sort key
+    constexpr unsigned kNoKey = 0xffffffffu;
+    __shared__ TileTri s_tri[CHUNK];             // staged triangles in key order
+    __shared__ unsigned s_key[CHUNK];            // per warp: its keys, sorted
+    __shared__ unsigned char s_rank[CHUNK];       // position of each slot in key order
     // one CTA per tile of the call; the frame's cameras are concatenated
     const long long g = blockIdx.x;
     const int b = (int)(g / T_frame);
@@ -576,67 +578,90 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
-    // Each staged chunk is sorted by (back-facing, depth lower bound).  All
-    // front faces are tested first, nearest bound first, then the back faces.
-    // A triangle whose depth lower bound exceeds the pixel's current best
-    // depth can neither win nor tie, and neither can any triangle after it in
-    // the same run, so a pixel stops scanning a run there.  The result is the
-    // same minimum (depth, id) as one unordered pass.  Per pixel a triangle
-    // is only tested when the pixel lies in its bounding box (a column and a
-    // row bit mask relative to the tile) and in its conservative footprint.
+    // Each staged chunk is sorted by (back-facing, depth lower bound rounded
+    // down to a multiple of 2^SB).  All front faces are tested first, nearest
+    // bound first, then the back faces.  A triangle whose rounded bound
+    // exceeds the pixel's current best depth can neither win nor tie, and
+    // neither can any triangle after it in the same run (their bounds are at
+    // least as large), so a pixel stops scanning a run there.  The result is
+    // the same minimum (depth, id) as one unordered pass.  Per pixel a
+    // triangle is only tested when the pixel lies in its bounding box (a
+    // column and a row bit mask relative to the tile) and in its conservative
+    // footprint.
+    //
+    // Sort: 32-bit keys (facing | rounded bound | slot) are distinct; each
+    // warp sorts its 32 keys with a shuffle bitonic network, and a key's rank
+    // in the chunk is its lane plus its lower bound in every other warp's
+    // sorted keys (5-step binary searches).
     int n_front = 0;
+    const int lane = threadIdx.x & 31;
     for (int pass = 0; pass < 2; ++pass) {
         for (int base = 0; base < n; base += CHUNK) {
             const int m = min(CHUNK, n - base);
             if (pass == 0 || n > CHUNK) {
-                __syncthreads();
-                const int k = base + threadIdx.x;
+                __syncthreads();  // the previous chunk's readers are done
                 bool front = false;
-                if (threadIdx.x < CHUNK) {
-                    unsigned long long key = ~0ull;
-                    if (k < m + base) {
-                        const int f = tb[k];
-                        const TriView tv = tri_view[(long long)view * A.F + f];
-                        front = tv.dqmin >= 0;
-                        const TriFrame tf = tri_frame[(long long)b * A.F + f];
-                        const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
-                        const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
-                        const int3 id = A.faces[f];
-                        const float4* PV = A.proj + (long long)view * A.N;
-                        const float4 r0 = PV[id.x], r1 = PV[id.y], r2 = PV[id.z];
-                        const Footprint fp = footprint(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z),
-                                                       make_float3(r2.x, r2.y, r2.z));
-                        TileTri t;
-                        t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
-                                          (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
-                                          tv.dqmin & 0x7fffffff, f);
-                        t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
-                        t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
-                        t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
-                        t.a = tf.a;
-                        t.b = tf.b;
-                        t.c = tf.c;
-                        s_tri[threadIdx.x] = t;
-                        key = ((unsigned long long)(front ? 0u : 1u) << 62) |
-                              ((unsigned long long)(unsigned)(tv.dqmin & 0x7fffffff) << 16) | threadIdx.x;
+                unsigned key = kNoKey;
+                TileTri t;
+                if ((int)threadIdx.x < m) {
+                    const int f = tb[base + threadIdx.x];
+                    const TriView tv = tri_view[(long long)view * A.F + f];
+                    front = tv.dqmin >= 0;
+                    const TriFrame tf = tri_frame[(long long)b * A.F + f];
+                    const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
+                    const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
+                    const int3 id = A.faces[f];
+                    const float4* PV = A.proj + (long long)view * A.N;
+                    const float4 r0 = PV[id.x], r1 = PV[id.y], r2 = PV[id.z];
+                    const Footprint fp = footprint(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z),
+                                                   make_float3(r2.x, r2.y, r2.z));
+                    // rounded bound, kept below the all-ones key of an empty slot
+                    const unsigned coarse = min((unsigned)(tv.dqmin & 0x7fffffff) >> SB, (1u << (31 - SB)) - 2u);
+                    t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
+                                      (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
+                                      (int)(coarse << SB), f);
+                    t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
+                    t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
+                    t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
+                    t.a = tf.a;
+                    t.b = tf.b;
+                    t.c = tf.c;
+                    key = (front ? 0u : 0x80000000u) | (coarse << SB) | threadIdx.x;
+                }
+                if (threadIdx.x < CHUNK) {  // whole warps
+#pragma unroll
+                    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+                        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                            const unsigned o = __shfl_xor_sync(0xffffffffu, key, stride);
+                            const bool keep_min = ((lane & stride) == 0) == ((lane & size) == 0);
+                            key = keep_min ? min(key, o) : max(key, o);
+                        }
                     }
-                    s_key[threadIdx.x] = key;  // unused keys (beyond m) are never ranked or read
+                    s_key[threadIdx.x] = key;
                 }
                 n_front = __syncthreads_count(front);
-                // sort by rank: keys are distinct (the slot is part of the key)
-                if ((int)threadIdx.x < m) {
-                    const unsigned long long mine = s_key[threadIdx.x];
-                    int rank = 0;
-                    for (int q = 0; q < m; ++q) rank += s_key[q] < mine;
-                    s_order[rank] = (unsigned short)threadIdx.x;
+                if (threadIdx.x < CHUNK && key != kNoKey) {
+                    int r = lane;
+                    const int me = threadIdx.x >> 5, nw = (m + 31) >> 5;
+                    for (int w = 0; w < nw; ++w) {
+                        if (w == me) continue;
+                        const unsigned* L = s_key + 32 * w;
+                        int lo = 0;
+#pragma unroll
+                        for (int step = 16; step > 0; step >>= 1) lo += L[lo + step] < key ? step : 0;
+                        r += lo + (L[lo] < key ? 1 : 0);
+                    }
+                    s_rank[key & (CHUNK - 1)] = (unsigned char)r;
                 }
+                __syncthreads();
+                if ((int)threadIdx.x < m) s_tri[s_rank[threadIdx.x]] = t;
                 __syncthreads();
             }
             const int j0 = pass == 0 ? 0 : n_front;
             const int j1 = pass == 0 ? n_front : m;
             if (valid) {
-                for (int j = j0; j < j1; ++j) {
-                    const int slot = s_order[j];
+                for (int slot = j0; slot < j1; ++slot) {
                     // one 16-byte header load decides whether the ray test runs
                     const int4 h = s_tri[slot].hdr;
                     if ((unsigned)h.z > best_d) break;  // neither this nor a later one can reach the best depth

@@ -289,6 +289,7 @@ struct CovTileTri {
     float4 e2;  // c2, d1, d2, -
     float4 ab;  // a.x, a.y, b.x, b.y
     float2 c;
+    int2 bb;  // pixel box: x0 | x1 << 16, y0 | y1 << 16
 };
 
 // one CTA per (tile, view): a pixel stops at the first binned triangle that covers it
@@ -307,7 +308,7 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int N, const in
     const float pu = px + 0.5f, pv = py + 0.5f;
     for (int base = 0; base < n; base += kCovTile * kCovTile) {
         const int m = min(kCovTile * kCovTile, n - base);
-        __syncthreads();
+        if (__syncthreads_and(covered)) break;  // every pixel of the tile is covered: stop staging
         if ((int)threadIdx.x < m) {
             const int f = cb.bins[key * kCovCap + base + threadIdx.x];
             CoverTri t;
@@ -316,17 +317,31 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int N, const in
             CovTileTri e;
             e.e0 = make_float4(fp.a[0], fp.b[0], fp.c[0], fp.a[1]);
             e.e1 = make_float4(fp.b[1], fp.c[1], fp.a[2], fp.b[2]);
-            e.e2 = make_float4(fp.c[2], t.d1, t.d2, 0.f);
+            // interior threshold: a pixel centre inside every edge by three
+            // margins passes the exact test whatever its rounding (the error
+            // of e0 = 1 - e1 - e2 adds those of e1 and e2); disabled
+            // footprints get an unreachable threshold
+            const float mmax = fmaxf(fp.m[0], fmaxf(fp.m[1], fp.m[2]));
+            e.e2 = make_float4(fp.c[2], t.d1, t.d2, mmax > 0.f ? 4.f * mmax : 3.0e38f);
             e.ab = make_float4(t.a.x, t.a.y, t.b.x, t.b.y);
             e.c = t.c;
+            e.bb = make_int2(t.x0 | (t.x1 << 16), t.y0 | (t.y1 << 16));
             s_t[threadIdx.x] = e;
         }
         __syncthreads();
         for (int j = 0; j < m && !covered; ++j) {
+            // the reference tests only the pixels of the triangle's box
+            // (a tile pixel outside it can pass the widened barycentric test)
+            const int2 bb = s_t[j].bb;
+            if (px < (bb.x & 0xffff) || px > (bb.x >> 16) || py < (bb.y & 0xffff) || py > (bb.y >> 16)) continue;
             const float4 e0 = s_t[j].e0, e1 = s_t[j].e1, e2 = s_t[j].e2;
-            if (e0.x * pu + e0.y * pv + e0.z < 0.f || e0.w * pu + e1.x * pv + e1.y < 0.f ||
-                e1.z * pu + e1.w * pv + e2.x < 0.f)
-                continue;
+            const float f0 = e0.x * pu + e0.y * pv + e0.z, f1 = e0.w * pu + e1.x * pv + e1.y,
+                        f2 = e1.z * pu + e1.w * pv + e2.x;
+            if (f0 < 0.f || f1 < 0.f || f2 < 0.f) continue;
+            if (f0 >= e2.w && f1 >= e2.w && f2 >= e2.w) {  // clearly inside
+                covered = true;
+                break;
+            }
             CoverTri t;
             const float4 ab = s_t[j].ab;
             t.a = make_float2(ab.x, ab.y);
@@ -666,7 +681,8 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
                                               const float* extrinsics, const float* intrinsics,
                                               const float* points_image_space, uint8_t* is_boundary) {
     clear_error();
-    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 2 && height > 2, "bad sizes");
+    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 2 && height > 2 && width < 32768 && height < 32768,
+               "bad sizes");
     HC_REQUIRE(is_boundary && (points_image_space || (points_global_space && extrinsics && intrinsics)),
                "NULL pointer");
     HC_TRY(hc_mesh_boundary_reserve(h, batch, n_cameras, width, height));

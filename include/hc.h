@@ -360,7 +360,7 @@ typedef struct hc_mesh_boundary_s* hc_mesh_boundary;
  * image-space coverage of the mesh at width x height (render_u x render_v)
  * and flags a vertex of a view when a pixel of the 3x3 window around its
  * truncated projection is uncovered.  is_boundary [B,C,N] uint8 (TF bool).
- * Bit-identical to the reference op. */
+ * width and height lie in [3, 32767].  Bit-identical to the reference op. */
 hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
                                   int32_t n_vertices);
 hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h);

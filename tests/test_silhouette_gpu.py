@@ -136,3 +136,48 @@ def test_mesh_boundary_matches_fp64_oracle(scene):
     # -0.001 / 1.001 barycentric tolerance
     assert ora.sum() > 0
     assert (ours != ora).mean() < 1e-3
+
+
+def _box(P, F, x0, y0, x1, y1):
+    i = len(P)
+    P += [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
+    F += [(i, i + 1, i + 2), (i, i + 2, i + 3)]
+
+
+def test_mesh_boundary_tests_only_the_triangle_box():
+    """A long sliver whose sharp vertex sits 1.1 px right of a pixel centre:
+    that centre passes the widened barycentric test (-0.001 / 1.001) but lies
+    outside the sliver's clamped pixel box, so the reference leaves it
+    uncovered.  Three boxes cover the rest of a probe vertex's 3x3 window,
+    making the probe's flag depend on that one pixel alone."""
+    from deepcharacters_b200.silhouette import MeshBoundaryEngine
+    W = H = 64
+    P, F, probes = [], [], []
+    for x, y in ((13, 20), (29, 40), (45, 12), (16, 52)):  # (16, 52): the pixel sits in the tile before the sliver's
+        i = len(P)
+        P += [(x + 0.6, y + 0.5), (x + 2000.0, y + 0.5 - 10.0), (x + 2000.0, y + 0.5 + 10.0)]
+        F.append((i, i + 1, i + 2))
+        _box(P, F, x - 3.0, y - 1.0, x - 1.05, y + 2.0)
+        _box(P, F, x - 1.0, y - 1.0, x + 0.0, y - 0.05)
+        _box(P, F, x - 1.0, y + 1.05, x + 0.0, y + 2.0)
+        probes.append(len(P))
+        P.append((x - 1.5, y + 0.5))
+        # the pixel (x-1, y) passes the sliver's barycentric test in FP64
+        a, b, c = np.array(P[i]), np.array(P[i + 1]), np.array(P[i + 2])
+        pu, pv = x - 0.5, y + 0.5
+        d2 = (a[1] - b[1]) * c[0] + (b[0] - a[0]) * c[1] + a[0] * b[1] - b[0] * a[1]
+        d1 = (a[1] - c[1]) * b[0] + (c[0] - a[0]) * b[1] + a[0] * c[1] - c[0] * a[1]
+        e2 = ((a[1] - b[1]) * pu + (b[0] - a[0]) * pv + a[0] * b[1] - b[0] * a[1]) / d2
+        e1 = ((a[1] - c[1]) * pu + (c[0] - a[0]) * pv + a[0] * c[1] - c[0] * a[1]) / d1
+        e = np.array([1 - e1 - e2, e1, e2])
+        assert (e >= -0.001).all() and (e <= 1.001).all() and e.max() > 1.0
+    p2d = np.asarray(P, np.float32)[None, None]
+    faces = np.asarray(F, np.int32)
+    N = p2d.shape[2]
+    ora = SO.mesh_boundary(faces, p2d, W, H)
+    assert all(ora[0, 0, k] == 1 for k in probes)
+    eng = MeshBoundaryEngine(faces, N)
+    zeros = torch.zeros((1, N, 3), device=DEV)
+    ours = eng.forward(zeros, torch.zeros((1, 12), device=DEV), torch.zeros((1, 9), device=DEV), W, H,
+                       points_image_space=_t(p2d))
+    assert np.array_equal(ours.cpu().numpy(), ora)
