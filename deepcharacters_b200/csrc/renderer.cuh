@@ -55,11 +55,14 @@ struct TriFrame {    // 48 bytes: s0.xyz n.x | s1.xyz n.y | s2.xyz n.z
     float4 a, b, c;
 };
 
-struct TriView {     // 16 bytes
+struct TriView {     // 64 bytes per (view, triangle), written by the binning pass
     float num;       // dot(s0, n) - dot(ro_s, n)
     int x01;         // bbox x0 | x1 << 16
     int y01;         // bbox y0 | y1 << 16
     int dqmin;       // lower bound of the quantised depth; bit 31 set = back-facing
+    float4 e01;      // 2-D footprint edges 0 and 1: (a0, b0, a1, b1)
+    float4 e2c;      // edge 2 and two offsets: (a2, b2, c0, c1)
+    float4 e2o;      // (c2, 0, 0, 0)
 };
 
 struct TriS;

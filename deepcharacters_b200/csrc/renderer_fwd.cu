@@ -255,8 +255,12 @@ __global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
         tv.y01 = (cy0 & 0xffff) | (cy1 << 16);
         // front-facing: the plane normal points towards the camera (num < 0)
         tv.dqmin = depth_lower_bound(tv.num, T.n, T, ro_s) | (tv.num < 0.f ? 0 : (int)0x80000000);
-        tri_view[i] = tv;
         fp = footprint(p0, p1, p2);
+        // the tile resolve stages this record as it is (no vertex gathers there)
+        tv.e01 = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
+        tv.e2c = make_float4(fp.a[2], fp.b[2], fp.c[0], fp.c[1]);
+        tv.e2o = make_float4(fp.c[2], 0.f, 0.f, 0.f);
+        tri_view[i] = tv;
     }
     const bool nonempty = live && x1 >= x0 && y1 >= y0;
     int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
@@ -610,19 +614,14 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
                     const TriFrame tf = tri_frame[(long long)b * A.F + f];
                     const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
                     const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
-                    const int3 id = A.faces[f];
-                    const float4* PV = A.proj + (long long)view * A.N;
-                    const float4 r0 = PV[id.x], r1 = PV[id.y], r2 = PV[id.z];
-                    const Footprint fp = footprint(make_float3(r0.x, r0.y, r0.z), make_float3(r1.x, r1.y, r1.z),
-                                                   make_float3(r2.x, r2.y, r2.z));
                     // rounded bound, kept below the all-ones key of an empty slot
                     const unsigned coarse = min((unsigned)(tv.dqmin & 0x7fffffff) >> SB, (1u << (31 - SB)) - 2u);
                     t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
                                       (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
                                       (int)(coarse << SB), f);
-                    t.ea = make_float4(fp.a[0], fp.b[0], fp.a[1], fp.b[1]);
-                    t.nm = make_float4(tv.num, fp.c[0], fp.c[1], fp.c[2]);
-                    t.eb = make_float4(fp.a[2], fp.b[2], 0.f, 0.f);
+                    t.ea = tv.e01;
+                    t.nm = make_float4(tv.num, tv.e2c.z, tv.e2c.w, tv.e2o.x);
+                    t.eb = make_float4(tv.e2c.x, tv.e2c.y, 0.f, 0.f);
                     t.a = tf.a;
                     t.b = tf.b;
                     t.c = tf.c;
