@@ -155,11 +155,6 @@ __device__ __forceinline__ bool cover_test(const CoverTri& t, float pu, float pv
     return e0 >= -0.001f && e1 >= -0.001f && e2 >= -0.001f && e0 <= 1.001f && e1 <= 1.001f && e2 <= 1.001f;
 }
 
-__device__ __forceinline__ bool fp_inside(const Footprint& fp, float pu, float pv) {
-    return fp.a[0] * pu + fp.b[0] * pv + fp.c[0] >= 0.f && fp.a[1] * pu + fp.b[1] * pv + fp.c[1] >= 0.f &&
-           fp.a[2] * pu + fp.b[2] * pv + fp.c[2] >= 0.f;
-}
-
 __device__ __forceinline__ Footprint cover_footprint(const CoverTri& t, int W, int H) {
     const float M = fmaxf(fmaxf(fmaxf(fabsf(t.a.x), fabsf(t.a.y)), fmaxf(fabsf(t.b.x), fabsf(t.b.y))),
                           fmaxf(fmaxf(fabsf(t.c.x), fabsf(t.c.y)), (float)max(W, H)));
@@ -193,36 +188,93 @@ __device__ __forceinline__ void cover_tri(int view, int f, int N, int W, int H, 
     t.d1 = (a.y - c.y) * b.x + (c.x - a.x) * b.y + a.x * c.y - c.x * a.y;
 }
 
+// What the coverage tile stages per (view, triangle), written once by the
+// binning pass: the footprint, the exact test's operands and the pixel box.
+struct CovTileTri {
+    float4 e0;  // footprint a0, b0, c0, a1
+    float4 e1;  // b1, c1, a2, b2
+    float4 e2;  // c2, d1, d2, interior threshold
+    float4 ab;  // a.x, a.y, b.x, b.y
+    float2 c;
+    int2 bb;  // pixel box: x0 | x1 << 16, y0 | y1 << 16
+};
+
+__device__ __forceinline__ CovTileTri cover_record(const CoverTri& t, const Footprint& fp) {
+    CovTileTri e;
+    e.e0 = make_float4(fp.a[0], fp.b[0], fp.c[0], fp.a[1]);
+    e.e1 = make_float4(fp.b[1], fp.c[1], fp.a[2], fp.b[2]);
+    // interior threshold: a pixel centre inside every edge by three margins
+    // passes the exact test whatever its rounding (the error of
+    // e0 = 1 - e1 - e2 adds those of e1 and e2); disabled footprints get an
+    // unreachable threshold
+    const float mmax = fmaxf(fp.m[0], fmaxf(fp.m[1], fp.m[2]));
+    e.e2 = make_float4(fp.c[2], t.d1, t.d2, mmax > 0.f ? 4.f * mmax : 3.0e38f);
+    e.ab = make_float4(t.a.x, t.a.y, t.b.x, t.b.y);
+    e.c = t.c;
+    e.bb = make_int2(t.x0 | (t.x1 << 16), t.y0 | (t.y1 << 16));
+    return e;
+}
+
+__device__ __forceinline__ Footprint record_footprint(const CovTileTri& e) {
+    Footprint fp;
+    fp.a[0] = e.e0.x;
+    fp.b[0] = e.e0.y;
+    fp.c[0] = e.e0.z;
+    fp.a[1] = e.e0.w;
+    fp.b[1] = e.e1.x;
+    fp.c[1] = e.e1.y;
+    fp.a[2] = e.e1.z;
+    fp.b[2] = e.e1.w;
+    fp.c[2] = e.e2.x;
+    return fp;
+}
+
+// the reference's test of one pixel centre (only pixels of the triangle's
+// clamped box are tested: a centre just outside the box can pass the widened
+// barycentric test), with the footprint cull and the interior shortcut first
+__device__ __forceinline__ bool cover_record_test(const CovTileTri& e, int px, int py) {
+    if (px < (e.bb.x & 0xffff) || px > (e.bb.x >> 16) || py < (e.bb.y & 0xffff) || py > (e.bb.y >> 16)) return false;
+    const float pu = px + 0.5f, pv = py + 0.5f;
+    const float f0 = e.e0.x * pu + e.e0.y * pv + e.e0.z, f1 = e.e0.w * pu + e.e1.x * pv + e.e1.y,
+                f2 = e.e1.z * pu + e.e1.w * pv + e.e2.x;
+    if (f0 < 0.f || f1 < 0.f || f2 < 0.f) return false;
+    if (f0 >= e.e2.w && f1 >= e.e2.w && f2 >= e.e2.w) return true;  // clearly inside
+    CoverTri t;
+    t.a = make_float2(e.ab.x, e.ab.y);
+    t.b = make_float2(e.ab.z, e.ab.w);
+    t.c = e.c;
+    t.d1 = e.e2.y;
+    t.d2 = e.e2.z;
+    return cover_test(t, pu, pv);
+}
+
 struct CovBins {
     int tiles_x, T;
-    int* count;  // [V*T]
-    int* bins;   // [V*T*kCovCap]
+    int* count;        // [V*T]
+    int* bins;         // [V*T*kCovCap]
+    CovTileTri* rec;   // [V*F]
     unsigned char* cover;
     int W, H;
 };
 
-// append (tile, triangle) or, beyond the bin capacity, sweep the pair now
-__device__ __forceinline__ void cov_place(const CovBins& cb, int view, int tile, int f, const CoverTri& t,
-                                          const Footprint& fp) {
-    const long long key = (long long)view * cb.T + tile;
-    const int slot = atomicAdd(cb.count + key, 1);
-    if (slot < kCovCap) {
-        cb.bins[key * kCovCap + slot] = f;
-        return;
-    }
+// the pixels of one tile that a triangle covers, written at once (a pair
+// beyond the tile's bin capacity)
+__device__ void cov_sweep(const CovBins& cb, int view, int tile, const CovTileTri& e) {
     const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
     unsigned char* img = cb.cover + (long long)view * cb.H * cb.W;
-    for (int v = max(t.y0, ty * kCovTile); v <= min(t.y1, ty * kCovTile + kCovTile - 1); ++v)
-        for (int u = max(t.x0, tx * kCovTile); u <= min(t.x1, tx * kCovTile + kCovTile - 1); ++u) {
-            const float pu = u + 0.5f, pv = v + 0.5f;
-            if (fp_inside(fp, pu, pv) && cover_test(t, pu, pv)) img[(long long)v * cb.W + u] = 1;
-        }
+    for (int v = ty * kCovTile; v < min(ty * kCovTile + kCovTile, cb.H); ++v)
+        for (int u = tx * kCovTile; u < min(tx * kCovTile + kCovTile, cb.W); ++u)
+            if (cover_record_test(e, u, v)) img[(long long)v * cb.W + u] = 1;
 }
 
+// One thread per (view, triangle): its record, then its tiles.  Boxes of up
+// to 4 tiles are binned by their own thread, lanes that hit the same tile
+// sharing one counter atomic; larger boxes are taken by the whole warp, a
+// tile per lane, reading the record back from global memory.
 __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
                           CovBins cb) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
+    const unsigned lane = threadIdx.x & 31;
     const bool live = i < (long long)V * F;
     int view = 0, f = 0;
     CoverTri t;
@@ -235,66 +287,74 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
         view = (int)(i / F);
         f = (int)(i % F);
         cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
-        fp = cover_footprint(t, cb.W, cb.H);
     }
     const bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
+    if (nonempty) {
+        fp = cover_footprint(t, cb.W, cb.H);
+        cb.rec[i] = cover_record(t, fp);
+    }
     const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
     const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
     const int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
     const bool big = nt > 4;
-    if (nonempty && !big) {
-        for (int k = 0; k < nt; ++k) {
+    const int my_nt = big ? 0 : nt;
+    int maxnt = my_nt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
+    for (int k = 0; k < maxnt; ++k) {
+        bool act = k < my_nt;
+        long long key = -1;
+        int tile = 0;
+        if (act) {
             const int tx = tx0 + k % ntx, ty = ty0 + k / ntx;
-            if (nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
-                                              max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1)))
-                cov_place(cb, view, ty * cb.tiles_x + tx, f, t, fp);
+            act = nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
+                                                max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1));
+            tile = ty * cb.tiles_x + tx;
+            if (act) key = (long long)view * cb.T + tile;
         }
+        const unsigned same = __match_any_sync(0xffffffffu, key);
+        if (!act) continue;
+        const int leader = __ffs(same) - 1;
+        const int rank = __popc(same & ((1u << lane) - 1u));
+        int base = 0;
+        if ((int)lane == leader) base = atomicAdd(cb.count + key, __popc(same));
+        base = __shfl_sync(same, base, leader);
+        const int slot = base + rank;
+        if (slot < kCovCap)
+            cb.bins[key * kCovCap + slot] = f;
+        else
+            cov_sweep(cb, view, tile, cb.rec[i]);
     }
+    __syncwarp();  // the records of big triangles are read back by the other lanes
     unsigned pending = __ballot_sync(0xffffffffu, big);
     while (pending) {
         const int src = __ffs(pending) - 1;
         pending &= pending - 1;
-        CoverTri q;
-        q.a = make_float2(__shfl_sync(0xffffffffu, t.a.x, src), __shfl_sync(0xffffffffu, t.a.y, src));
-        q.b = make_float2(__shfl_sync(0xffffffffu, t.b.x, src), __shfl_sync(0xffffffffu, t.b.y, src));
-        q.c = make_float2(__shfl_sync(0xffffffffu, t.c.x, src), __shfl_sync(0xffffffffu, t.c.y, src));
-        q.d1 = __shfl_sync(0xffffffffu, t.d1, src);
-        q.d2 = __shfl_sync(0xffffffffu, t.d2, src);
-        q.x0 = __shfl_sync(0xffffffffu, t.x0, src);
-        q.x1 = __shfl_sync(0xffffffffu, t.x1, src);
-        q.y0 = __shfl_sync(0xffffffffu, t.y0, src);
-        q.y1 = __shfl_sync(0xffffffffu, t.y1, src);
         const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
-        Footprint qfp;
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-            qfp.a[e] = __shfl_sync(0xffffffffu, fp.a[e], src);
-            qfp.b[e] = __shfl_sync(0xffffffffu, fp.b[e], src);
-            qfp.c[e] = __shfl_sync(0xffffffffu, fp.c[e], src);
-        }
-        const int qtx0 = q.x0 / kCovTile, qty0 = q.y0 / kCovTile, qntx = q.x1 / kCovTile - qtx0 + 1;
-        const int qnt = qntx * (q.y1 / kCovTile - qty0 + 1);
+        const CovTileTri q = cb.rec[(long long)qv * F + qf];
+        const Footprint qfp = record_footprint(q);
+        const int qx0 = q.bb.x & 0xffff, qx1 = q.bb.x >> 16, qy0 = q.bb.y & 0xffff, qy1 = q.bb.y >> 16;
+        const int qtx0 = qx0 / kCovTile, qty0 = qy0 / kCovTile, qntx = qx1 / kCovTile - qtx0 + 1;
+        const int qnt = qntx * (qy1 / kCovTile - qty0 + 1);
         for (int k = lane; k < qnt; k += 32) {
             const int tx = qtx0 + k % qntx, ty = qty0 + k / qntx;
-            if (footprint_overlaps(qfp, max(tx * kCovTile, q.x0), min(tx * kCovTile + kCovTile - 1, q.x1),
-                                   max(ty * kCovTile, q.y0), min(ty * kCovTile + kCovTile - 1, q.y1)))
-                cov_place(cb, qv, ty * cb.tiles_x + tx, qf, q, qfp);
+            if (!footprint_overlaps(qfp, max(tx * kCovTile, qx0), min(tx * kCovTile + kCovTile - 1, qx1),
+                                    max(ty * kCovTile, qy0), min(ty * kCovTile + kCovTile - 1, qy1)))
+                continue;
+            const int tile = ty * cb.tiles_x + tx;
+            const long long key = (long long)qv * cb.T + tile;
+            const int slot = atomicAdd(cb.count + key, 1);
+            if (slot < kCovCap)
+                cb.bins[key * kCovCap + slot] = qf;
+            else
+                cov_sweep(cb, qv, tile, q);
         }
     }
 }
 
-struct CovTileTri {
-    float4 e0;  // footprint a0, b0, c0, a1
-    float4 e1;  // b1, c1, a2, b2
-    float4 e2;  // c2, d1, d2, -
-    float4 ab;  // a.x, a.y, b.x, b.y
-    float2 c;
-    int2 bb;  // pixel box: x0 | x1 << 16, y0 | y1 << 16
-};
-
-// one CTA per (tile, view): a pixel stops at the first binned triangle that covers it
-__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int N, const int* __restrict__ faces,
-                                                                 const float2* __restrict__ p2d, CovBins cb) {
+// one CTA per (tile, view): a pixel stops at the first binned triangle that
+// covers it, the tile at the chunk after which all its pixels are covered
+__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, CovBins cb) {
     __shared__ CovTileTri s_t[kCovTile * kCovTile];
     const int tile = blockIdx.x, view = blockIdx.y;
     const long long key = (long long)view * cb.T + tile;
@@ -305,52 +365,13 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int N, const in
     const bool valid = px < cb.W && py < cb.H;
     unsigned char* pix = cb.cover + ((long long)view * cb.H + py) * cb.W + px;
     bool covered = !valid || *pix;
-    const float pu = px + 0.5f, pv = py + 0.5f;
+    const CovTileTri* R = cb.rec + (long long)view * F;
     for (int base = 0; base < n; base += kCovTile * kCovTile) {
         const int m = min(kCovTile * kCovTile, n - base);
         if (__syncthreads_and(covered)) break;  // every pixel of the tile is covered: stop staging
-        if ((int)threadIdx.x < m) {
-            const int f = cb.bins[key * kCovCap + base + threadIdx.x];
-            CoverTri t;
-            cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
-            const Footprint fp = cover_footprint(t, cb.W, cb.H);
-            CovTileTri e;
-            e.e0 = make_float4(fp.a[0], fp.b[0], fp.c[0], fp.a[1]);
-            e.e1 = make_float4(fp.b[1], fp.c[1], fp.a[2], fp.b[2]);
-            // interior threshold: a pixel centre inside every edge by three
-            // margins passes the exact test whatever its rounding (the error
-            // of e0 = 1 - e1 - e2 adds those of e1 and e2); disabled
-            // footprints get an unreachable threshold
-            const float mmax = fmaxf(fp.m[0], fmaxf(fp.m[1], fp.m[2]));
-            e.e2 = make_float4(fp.c[2], t.d1, t.d2, mmax > 0.f ? 4.f * mmax : 3.0e38f);
-            e.ab = make_float4(t.a.x, t.a.y, t.b.x, t.b.y);
-            e.c = t.c;
-            e.bb = make_int2(t.x0 | (t.x1 << 16), t.y0 | (t.y1 << 16));
-            s_t[threadIdx.x] = e;
-        }
+        if ((int)threadIdx.x < m) s_t[threadIdx.x] = R[cb.bins[key * kCovCap + base + threadIdx.x]];
         __syncthreads();
-        for (int j = 0; j < m && !covered; ++j) {
-            // the reference tests only the pixels of the triangle's box
-            // (a tile pixel outside it can pass the widened barycentric test)
-            const int2 bb = s_t[j].bb;
-            if (px < (bb.x & 0xffff) || px > (bb.x >> 16) || py < (bb.y & 0xffff) || py > (bb.y >> 16)) continue;
-            const float4 e0 = s_t[j].e0, e1 = s_t[j].e1, e2 = s_t[j].e2;
-            const float f0 = e0.x * pu + e0.y * pv + e0.z, f1 = e0.w * pu + e1.x * pv + e1.y,
-                        f2 = e1.z * pu + e1.w * pv + e2.x;
-            if (f0 < 0.f || f1 < 0.f || f2 < 0.f) continue;
-            if (f0 >= e2.w && f1 >= e2.w && f2 >= e2.w) {  // clearly inside
-                covered = true;
-                break;
-            }
-            CoverTri t;
-            const float4 ab = s_t[j].ab;
-            t.a = make_float2(ab.x, ab.y);
-            t.b = make_float2(ab.z, ab.w);
-            t.c = s_t[j].c;
-            t.d1 = e2.y;
-            t.d2 = e2.z;
-            covered = cover_test(t, pu, pv);
-        }
+        for (int j = 0; j < m && !covered; ++j) covered = cover_record_test(s_t[j], px, py);
     }
     if (valid && covered && !*pix) *pix = 1;
 }
@@ -630,7 +651,7 @@ extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover, count, bins;
+    DevBuf faces, p2d, cover, count, bins, rec;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -673,6 +694,7 @@ extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch,
     const size_t tiles = (size_t)div_up(width, kCovTile) * div_up(height, kCovTile);
     HC_TRY(h->count.ensure(sizeof(int) * views * tiles));
     HC_TRY(h->bins.ensure(sizeof(int) * views * tiles * kCovCap));
+    HC_TRY(h->rec.ensure(sizeof(CovTileTri) * views * h->F));
     return HC_OK;
 }
 
@@ -704,14 +726,14 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
     cb.count = h->count.as<int>();
     cb.bins = h->bins.as<int>();
     cb.cover = h->cover.as<unsigned char>();
+    cb.rec = h->rec.as<CovTileTri>();
     cb.W = width;
     cb.H = height;
     HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)views * cb.T, s));
     k_cov_bin<<<div_up(nt, 256), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
                                               reinterpret_cast<const float2*>(p2d), cb);
     HC_CHECK_LAUNCH();
-    k_cov_tile<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(
-        h->N, h->faces.as<int>(), reinterpret_cast<const float2*>(p2d), cb);
+    k_cov_tile<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(h->F, cb);
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
                                                      h->cover.as<unsigned char>(), is_boundary);
