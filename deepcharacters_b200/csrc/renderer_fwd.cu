@@ -416,14 +416,19 @@ struct ShadeArgs {
     int* tie_count;
 };
 
+// colour of a pixel hit by face f at barycentrics (a, bb)
 __device__ __forceinline__ float3 shade_pixel(const ShadeArgs& A, const ViewCam& cam, int view, int b, int f,
                                               float a, float bb, float3 dir) {
     const int3 id = A.faces[f];
-    const float* VN = A.vnormal + ((long long)view * A.N) * 3;
-    const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
-    float3 pn = n0 * a + n1 * bb + n2 * (1.f - a - bb);
-    pn = pn / length3(pn);
-    if (dot(pn, dir) > 0.f) pn = -pn;
+    // the interpolated normal, only where the albedo or the shading reads it
+    float3 pn = make_float3(0.f, 0.f, 0.f);
+    if (A.albedo == kNormal || A.albedo == kLighting || A.shading == kShaded) {
+        const float* VN = A.vnormal + ((long long)view * A.N) * 3;
+        const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
+        pn = n0 * a + n1 * bb + n2 * (1.f - a - bb);
+        pn = pn / length3(pn);
+        if (dot(pn, dir) > 0.f) pn = -pn;
+    }
     float3 color = make_float3(0.f, 0.f, 0.f);
     switch (A.albedo) {
         case kTextured: {
