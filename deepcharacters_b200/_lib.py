@@ -60,8 +60,11 @@ _SIGS: dict[str, list] = {
     "hc_mesh_boundary_destroy": [vp],
     "hc_mesh_boundary_reserve": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
     "hc_mesh_boundary_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp],
+    "hc_mesh_boundary_forward_hinted": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp,
+                                        vp],
     "hc_sum_squares_loss": [vp, C.c_int64, vp, C.c_float, vp, vp, vp],
     "hc_add_inplace": [vp, C.c_int64, vp, vp],
+    "hc_image_u8_to_f32": [vp, C.c_int64, vp, vp],
     "hc_gaussian_smooth": [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_float, vp, vp],
     "hc_renderer_set_kernel_timing": [vp, C.c_int32],
     "hc_renderer_create_multires": [vp, vp, C.c_int32, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_char_p,

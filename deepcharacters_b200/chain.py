@@ -115,8 +115,9 @@ class DeformRenderChain:
         L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), None, P(i["extr"]), P(i["intr"]), 1, P(o["p2d"]))
         L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), P(o["n"]), P(i["extr"]), P(i["intr"]), 0,
           P(o["n2d"]))
-        L("hc_mesh_boundary_forward", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]), P(i["intr"]),
-          P(o["p2d"]), P(o["isb"]))
+        # the renderer's face buffer of the same views is the coverage hint
+        L("hc_mesh_boundary_forward_hinted", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]), P(i["intr"]),
+          P(o["p2d"]), P(o["face"]), P(o["isb"]))
         L("hc_silhouette_forward", self.sil.handle, s, B, C, N, W, H, P(o["p2d"]), P(o["n2d"]), P(o["isb"]),
           P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
         L("hc_sum_squares_loss", s, B * C * N, P(o["res"]), self.w_sil, self.ws.data_ptr() + 16,

@@ -109,6 +109,21 @@ __global__ void k_add_inplace(long long n, float* __restrict__ dst, const float*
         dst[i] += src[i];
 }
 
+// 8-bit image values -> float32 in [0, 1] (k / 255, IEEE division); four
+// bytes per thread and step
+__global__ void k_u8_to_f32(long long n, const unsigned char* __restrict__ src, float* __restrict__ dst) {
+    const long long n4 = n / 4;
+    const uchar4* s4 = reinterpret_cast<const uchar4*>(src);
+    float4* d4 = reinterpret_cast<float4*>(dst);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const uchar4 q = s4[i];
+        d4[i] = make_float4((float)q.x / 255.f, (float)q.y / 255.f, (float)q.z / 255.f, (float)q.w / 255.f);
+    }
+    for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
+        dst[i] = (float)src[i] / 255.f;
+}
+
 // Gaussian smoothing of images (Projects/CustomTFOperators/GaussianSmoothingGpu.py:12-37):
 // a depthwise (2s+1)^2 convolution with the normalised outer product of a
 // sampled normal density, zero padding ("SAME").  The kernel is separable, so
@@ -217,6 +232,19 @@ extern "C" hc_status hc_add_inplace(void* stream, int64_t n, float* dst, const f
     if (n == 0) return HC_OK;
     const long long blocks = n / 1024 + 1 < 148 * 8 ? n / 1024 + 1 : 148 * 8;
     k_add_inplace<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, dst, src);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
+extern "C" hc_status hc_image_u8_to_f32(void* stream, int64_t n, const uint8_t* src, float* dst) {
+    clear_error();
+    HC_REQUIRE(n >= 0, "n < 0");
+    HC_REQUIRE(src && dst, "NULL pointer");
+    HC_REQUIRE(((uintptr_t)src & 3) == 0 && ((uintptr_t)dst & 15) == 0,
+               "src must be 4-byte and dst 16-byte aligned");
+    if (n == 0) return HC_OK;
+    const long long blocks = n / 4096 + 1 < 148 * 8 ? n / 4096 + 1 : 148 * 8;
+    k_u8_to_f32<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(n, src, dst);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }

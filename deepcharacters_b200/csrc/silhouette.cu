@@ -254,6 +254,7 @@ struct CovBins {
     int* bins;         // [V*T*kCovCap]
     CovTileTri* rec;   // [V*F]
     unsigned char* cover;
+    const unsigned char* need;  // [V*T] tiles with a pixel still open (NULL: every tile)
     int W, H;
 };
 
@@ -265,6 +266,35 @@ __device__ void cov_sweep(const CovBins& cb, int view, int tile, const CovTileTr
     for (int v = ty * kCovTile; v < min(ty * kCovTile + kCovTile, cb.H); ++v)
         for (int u = tx * kCovTile; u < min(tx * kCovTile + kCovTile, cb.W); ++u)
             if (cover_record_test(e, u, v)) img[(long long)v * cb.W + u] = 1;
+}
+
+// Coverage from a per-pixel face hint (a renderer face buffer of the same
+// views): a pixel is covered when the reference's 2-D test passes for its hint
+// face, which is checked here exactly; every other pixel stays open for the
+// binned passes, and a tile is marked as needing them when it has an open
+// pixel.  Any hint gives the same coverage; a good one only saves work.
+__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_hint(int N, int F, const int* __restrict__ faces,
+                                                                 const float2* __restrict__ p2d,
+                                                                 const int* __restrict__ hint, CovBins cb,
+                                                                 unsigned char* __restrict__ need) {
+    const int tile = blockIdx.x, view = blockIdx.y;
+    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+    const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
+    const bool valid = px < cb.W && py < cb.H;
+    bool covered = true;
+    if (valid) {
+        const long long pix = ((long long)view * cb.H + py) * cb.W + px;
+        const int f = hint[pix];
+        covered = false;
+        if (f >= 0 && f < F) {
+            CoverTri t;
+            cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
+            covered = px >= t.x0 && px <= t.x1 && py >= t.y0 && py <= t.y1 && cover_test(t, px + 0.5f, py + 0.5f);
+        }
+        cb.cover[pix] = covered ? 1 : 0;
+    }
+    const bool all = __syncthreads_and(covered);
+    if (threadIdx.x == 0) need[(long long)view * cb.T + tile] = all ? 0 : 1;
 }
 
 // One thread per (view, triangle): its record, then its tiles.  Boxes of up
@@ -288,14 +318,23 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
         f = (int)(i % F);
         cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
     }
-    const bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
+    bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
+    const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
+    const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
+    int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
+    if (cb.need && nt > 0 && nt <= 4) {  // a small box whose tiles are all covered already needs nothing
+        bool any = false;
+        for (int k = 0; k < nt; ++k)
+            any = any || cb.need[(long long)view * cb.T + (ty0 + k / ntx) * cb.tiles_x + tx0 + k % ntx];
+        if (!any) {
+            nonempty = false;
+            nt = 0;
+        }
+    }
     if (nonempty) {
         fp = cover_footprint(t, cb.W, cb.H);
         cb.rec[i] = cover_record(t, fp);
     }
-    const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
-    const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
-    const int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
     const bool big = nt > 4;
     const int my_nt = big ? 0 : nt;
     int maxnt = my_nt;
@@ -310,6 +349,7 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
             act = nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
                                                 max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1));
             tile = ty * cb.tiles_x + tx;
+            if (act && cb.need && !cb.need[(long long)view * cb.T + tile]) act = false;
             if (act) key = (long long)view * cb.T + tile;
         }
         const unsigned same = __match_any_sync(0xffffffffu, key);
@@ -343,6 +383,7 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
                 continue;
             const int tile = ty * cb.tiles_x + tx;
             const long long key = (long long)qv * cb.T + tile;
+            if (cb.need && !cb.need[key]) continue;
             const int slot = atomicAdd(cb.count + key, 1);
             if (slot < kCovCap)
                 cb.bins[key * kCovCap + slot] = qf;
@@ -651,7 +692,7 @@ extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover, count, bins, rec;
+    DevBuf faces, p2d, cover, count, bins, rec, need;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -680,6 +721,8 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     h->cover.release();
     h->count.release();
     h->bins.release();
+    h->rec.release();
+    h->need.release();
     delete h;
     return HC_OK;
 }
@@ -695,14 +738,14 @@ extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch,
     HC_TRY(h->count.ensure(sizeof(int) * views * tiles));
     HC_TRY(h->bins.ensure(sizeof(int) * views * tiles * kCovCap));
     HC_TRY(h->rec.ensure(sizeof(CovTileTri) * views * h->F));
+    HC_TRY(h->need.ensure(views * tiles));
     return HC_OK;
 }
 
-extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
-                                              int32_t width, int32_t height, const float* points_global_space,
-                                              const float* extrinsics, const float* intrinsics,
-                                              const float* points_image_space, uint8_t* is_boundary) {
-    clear_error();
+static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                   int32_t width, int32_t height, const float* points_global_space,
+                                   const float* extrinsics, const float* intrinsics, const float* points_image_space,
+                                   const int32_t* face_hint, uint8_t* is_boundary) {
     HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 2 && height > 2 && width < 32768 && height < 32768,
                "bad sizes");
     HC_REQUIRE(is_boundary && (points_image_space || (points_global_space && extrinsics && intrinsics)),
@@ -718,7 +761,6 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
         p2d = h->p2d.as<float>();
     }
     const long long views = (long long)batch * n_cameras;
-    HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
     const long long nt = views * h->F;
     CovBins cb;
     cb.tiles_x = div_up(width, kCovTile);
@@ -727,8 +769,18 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
     cb.bins = h->bins.as<int>();
     cb.cover = h->cover.as<unsigned char>();
     cb.rec = h->rec.as<CovTileTri>();
+    cb.need = nullptr;
     cb.W = width;
     cb.H = height;
+    if (face_hint) {  // writes every pixel of the coverage image and the per-tile flags
+        k_cov_hint<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(
+            h->N, h->F, h->faces.as<int>(), reinterpret_cast<const float2*>(p2d), face_hint, cb,
+            h->need.as<unsigned char>());
+        HC_CHECK_LAUNCH();
+        cb.need = h->need.as<unsigned char>();
+    } else {
+        HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
+    }
     HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)views * cb.T, s));
     k_cov_bin<<<div_up(nt, 256), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
                                               reinterpret_cast<const float2*>(p2d), cb);
@@ -739,6 +791,26 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
                                                      h->cover.as<unsigned char>(), is_boundary);
     HC_CHECK_LAUNCH();
     return HC_OK;
+}
+
+extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                              int32_t width, int32_t height, const float* points_global_space,
+                                              const float* extrinsics, const float* intrinsics,
+                                              const float* points_image_space, uint8_t* is_boundary) {
+    clear_error();
+    return mesh_boundary_run(h, stream, batch, n_cameras, width, height, points_global_space, extrinsics, intrinsics,
+                             points_image_space, nullptr, is_boundary);
+}
+
+extern "C" hc_status hc_mesh_boundary_forward_hinted(hc_mesh_boundary h, void* stream, int32_t batch,
+                                                     int32_t n_cameras, int32_t width, int32_t height,
+                                                     const float* points_global_space, const float* extrinsics,
+                                                     const float* intrinsics, const float* points_image_space,
+                                                     const int32_t* face_hint, uint8_t* is_boundary) {
+    clear_error();
+    HC_REQUIRE(face_hint, "face_hint is NULL");
+    return mesh_boundary_run(h, stream, batch, n_cameras, width, height, points_global_space, extrinsics, intrinsics,
+                             points_image_space, face_hint, is_boundary);
 }
 
 struct hc_silhouette_s {

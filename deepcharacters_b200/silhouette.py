@@ -107,7 +107,10 @@ class MeshBoundaryEngine:
         _lib.call("hc_mesh_boundary_reserve", self._h, B, Cn, int(width), int(height))
 
     def forward(self, points_global_space, extrinsics, intrinsics, width: int, height: int,
-                points_image_space=None, out=None):
+                points_image_space=None, out=None, face_hint=None):
+        """is_boundary [B,C,N] (uint8).  ``face_hint`` [B,C,H,W] int32 (a renderer
+        face buffer of the same views) only saves work: the flags are the same
+        for any hint."""
         p = _f32(points_global_space, "points_global_space")
         ex, it = _f32(extrinsics, "extrinsics"), _f32(intrinsics, "intrinsics")
         B = p.shape[0]
@@ -118,8 +121,15 @@ class MeshBoundaryEngine:
             out = torch.empty((B, Cn, self.N), device=p.device, dtype=torch.uint8)
         pis = _f32(points_image_space, "points_image_space") if points_image_space is not None else None
         P = _lib.ptr
-        _lib.call("hc_mesh_boundary_forward", self._h, _stream(), B, Cn, int(width), int(height), P(p), P(ex), P(it),
-                  P(pis) if pis is not None else None, P(out))
+        if face_hint is None:
+            _lib.call("hc_mesh_boundary_forward", self._h, _stream(), B, Cn, int(width), int(height), P(p), P(ex),
+                      P(it), P(pis) if pis is not None else None, P(out))
+            return out
+        if (face_hint.dtype != torch.int32 or not face_hint.is_contiguous()
+                or face_hint.numel() != B * Cn * int(width) * int(height)):
+            raise ValueError("face_hint must be a contiguous int32 [B,C,H,W] tensor")
+        _lib.call("hc_mesh_boundary_forward_hinted", self._h, _stream(), B, Cn, int(width), int(height), P(p), P(ex),
+                  P(it), P(pis) if pis is not None else None, P(face_hint), P(out))
         return out
 
 

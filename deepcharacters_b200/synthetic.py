@@ -485,9 +485,10 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
     nodes, K nearest nodes per vertex) and a random ``n_skel``-joint tree with
     K-nearest-joint skinning weights; per frame an independent pose (joint
     angles U(-a, a)) and node deltas (Euler N(0, 0.05) rad, translation
-    N(0, 10) mm); 8 markers on random nodes; cameras on a ring; vertex colours U[0,1]; target images
-    U[0,1]; silhouette distance-transform images of seeded random ellipses
-    (``n_masks`` distinct ones, default one per view, reused across frames)."""
+    N(0, 10) mm); 8 markers on random nodes; cameras on a ring; vertex colours U[0,1]; 8-bit target
+    images (``target_u8`` uniform bytes, ``target`` = byte / 255 in float32, the value
+    ``hc_image_u8_to_f32`` computes on the device); silhouette distance-transform images of
+    seeded random ellipses (``n_masks`` distinct ones, default one per view, reused across frames)."""
     rng = rng_for(seed)
     verts, faces = sphere_mesh(subdiv, rng)
     N = verts.shape[0]
@@ -504,6 +505,7 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
     nm = views if n_masks is None else n_masks
     masks = silhouette_masks(1, nm, width, height, seed=seed, scale=min(width, height) / 512.0)[0]
     dt = np.stack([masks[np.arange(views) % nm]] * frames)
+    target_u8 = rng.integers(0, 256, size=(frames, views, height, width, 3), dtype=np.uint8)
     return dict(verts=verts, faces=faces, graph=graph, markers=markers, marker_node=mk_nodes, skeleton=sk,
                 skin_index=skin_idx, skin_weights=skin_w,
                 dofs=dofs, dT=f(delta_t_std, (frames, n_nodes, 3)), dA=f(delta_rot_std, (frames, n_nodes, 3)),
@@ -513,6 +515,6 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
                 sh=sh_coefficients(frames * views, rng).reshape(frames, views, 27),
                 extr=np.tile(ex[None], (frames, 1)), intr=np.tile(it[None], (frames, 1)),
                 texcoords=spherical_uvs(verts, faces),
-                target=rng.uniform(0.0, 1.0, size=(frames, views, height, width, 3)).astype(np.float32),
+                target=target_u8.astype(np.float32) / np.float32(255.0), target_u8=target_u8,
                 dt=dt, crops=identity_crops(frames, views, width, height),
                 N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=width, H=height)

@@ -370,6 +370,19 @@ hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t bat
                                    int32_t width, int32_t height, const float* points_global_space,
                                    const float* extrinsics, const float* intrinsics,
                                    const float* points_image_space, uint8_t* is_boundary);
+/* hc_mesh_boundary_forward with a per-pixel face hint: face_hint [B,C,H,W]
+ * int32, e.g. the face buffer of hc_renderer_forward for the same vertices,
+ * cameras and resolution.  A pixel whose hint face passes the op's own 2-D
+ * coverage test (checked exactly) is covered; every other pixel and the tiles
+ * that hold one go through the full binned coverage.  The flags are
+ * bit-identical to hc_mesh_boundary_forward for every hint (out-of-range ids
+ * count as no hint); a hint that matches the coverage only saves work.  No
+ * reference counterpart (the reference op rasterises the whole mesh again). */
+hc_status hc_mesh_boundary_forward_hinted(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                          int32_t width, int32_t height, const float* points_global_space,
+                                          const float* extrinsics, const float* intrinsics,
+                                          const float* points_image_space, const int32_t* face_hint,
+                                          uint8_t* is_boundary);
 /* The same boundary test with coverage taken from a renderer face buffer
  * [B,C,H,W] (-1 = empty) instead of the op's own 2-D raster.  No separate
  * reference counterpart: the renderer's ray test and the 2-D barycentric test
@@ -472,6 +485,12 @@ hc_status hc_gaussian_smooth(void* stream, int32_t n_images, int32_t height, int
  * branches meet on one tensor (e.g. vertex positions, fed by the renderer
  * and by the silhouette's camera projection). */
 hc_status hc_add_inplace(void* stream, int64_t n, float* dst, const float* src);
+
+/* dst[i] = src[i] / 255 (float32, IEEE division) over n values: 8-bit target
+ * images uploaded as bytes and widened on the device, a quarter of the
+ * host-to-device traffic of float32 images.  src 4-byte and dst 16-byte
+ * aligned.  No reference counterpart. */
+hc_status hc_image_u8_to_f32(void* stream, int64_t n, const uint8_t* src, float* dst);
 
 #ifdef __cplusplus
 }

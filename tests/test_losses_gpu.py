@@ -56,3 +56,18 @@ def test_l1_and_sum_squares():
     l2, g2 = sum_squares_loss(torch.from_numpy(x).to(DEV), 0.5)
     assert abs(float(l2) - 0.5 * (x.astype(np.float64) ** 2).sum()) < 1e-5 * (x.astype(np.float64) ** 2).sum()
     assert torch.allclose(g2.cpu(), torch.from_numpy(x), rtol=1e-6)
+
+
+def test_u8_images_widen_to_the_host_values():
+    """hc_image_u8_to_f32 gives byte / 255 exactly as float32 division on the
+    host does (every byte value; a length that is not a multiple of 4)."""
+    from deepcharacters_b200 import _lib
+    rng = np.random.default_rng(4)
+    for n in (256, 1000003):
+        src = np.arange(n, dtype=np.int64) % 256 if n == 256 else rng.integers(0, 256, n)
+        src = src.astype(np.uint8)
+        s = torch.from_numpy(src).to(DEV)
+        d = torch.empty(n, dtype=torch.float32, device=DEV)
+        _lib.call("hc_image_u8_to_f32", torch.cuda.current_stream().cuda_stream, n, s.data_ptr(), d.data_ptr())
+        want = src.astype(np.float32) / np.float32(255.0)
+        assert np.array_equal(d.cpu().numpy(), want)

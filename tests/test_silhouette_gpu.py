@@ -144,6 +144,11 @@ def _box(P, F, x0, y0, x1, y1):
     F += [(i, i + 1, i + 2), (i, i + 2, i + 3)]
 
 
+# sharp corners of the slivers below; at (16, 52) the pixel left of the corner
+# lies in the tile before the sliver's
+CORNERS = ((13, 20), (29, 40), (45, 12), (16, 52))
+
+
 def test_mesh_boundary_tests_only_the_triangle_box():
     """A long sliver whose sharp vertex sits 1.1 px right of a pixel centre:
     that centre passes the widened barycentric test (-0.001 / 1.001) but lies
@@ -152,10 +157,11 @@ def test_mesh_boundary_tests_only_the_triangle_box():
     making the probe's flag depend on that one pixel alone."""
     from deepcharacters_b200.silhouette import MeshBoundaryEngine
     W = H = 64
-    P, F, probes = [], [], []
-    for x, y in ((13, 20), (29, 40), (45, 12), (16, 52)):  # (16, 52): the pixel sits in the tile before the sliver's
+    P, F, probes, slivers = [], [], [], []
+    for x, y in CORNERS:
         i = len(P)
         P += [(x + 0.6, y + 0.5), (x + 2000.0, y + 0.5 - 10.0), (x + 2000.0, y + 0.5 + 10.0)]
+        slivers.append(len(F))
         F.append((i, i + 1, i + 2))
         _box(P, F, x - 3.0, y - 1.0, x - 1.05, y + 2.0)
         _box(P, F, x - 1.0, y - 1.0, x + 0.0, y - 0.05)
@@ -178,6 +184,36 @@ def test_mesh_boundary_tests_only_the_triangle_box():
     assert all(ora[0, 0, k] == 1 for k in probes)
     eng = MeshBoundaryEngine(faces, N)
     zeros = torch.zeros((1, N, 3), device=DEV)
-    ours = eng.forward(zeros, torch.zeros((1, 12), device=DEV), torch.zeros((1, 9), device=DEV), W, H,
-                       points_image_space=_t(p2d))
+    ex, it = torch.zeros((1, 12), device=DEV), torch.zeros((1, 9), device=DEV)
+    ours = eng.forward(zeros, ex, it, W, H, points_image_space=_t(p2d))
     assert np.array_equal(ours.cpu().numpy(), ora)
+    # a hint naming the sliver at every pixel must not cover the pixel outside its box
+    hint = torch.full((1, 1, H, W), -1, dtype=torch.int32, device=DEV)
+    for (x, y), f in zip(CORNERS, slivers):
+        hint[0, 0, y - 2:y + 3, x - 4:x + 2] = f
+    hinted = eng.forward(zeros, ex, it, W, H, points_image_space=_t(p2d), face_hint=hint)
+    assert np.array_equal(hinted.cpu().numpy(), ora)
+
+
+def test_mesh_boundary_hint_changes_no_flag(scene):
+    """The hinted coverage gives the same flags as the full one for the
+    renderer's face buffer of the same views, for no hint at all (-1), and for
+    random face ids (in and out of range)."""
+    from deepcharacters_b200.silhouette import MeshBoundaryEngine
+    sc = scene["sc"]
+    ex, it = _t(sc["extr"]), _t(sc["intr"])
+    eng = MeshBoundaryEngine(sc["faces"], sc["N"])
+    for width, height in ((RES, RES), (RES, RES // 2)):
+        full = eng.forward(scene["verts"], ex, it, width, height).clone()
+        assert int(full.sum()) > 0
+        g = torch.Generator(DEV).manual_seed(7)
+        F = len(sc["faces"])
+        hints = [torch.full((2, 3, height, width), -1, dtype=torch.int32, device=DEV),
+                 torch.randint(-2, F + 5, (2, 3, height, width), generator=g, device=DEV, dtype=torch.int32)]
+        if height == RES:
+            hints.append(scene["face"].contiguous())
+        for k, hint in enumerate(hints):
+            for _ in range(2):  # two calls in a row on the same handle
+                hinted = eng.forward(scene["verts"], ex, it, width, height, face_hint=hint)
+                torch.cuda.synchronize()
+                assert torch.equal(hinted, full), (width, height, k, int((hinted != full).sum()))
