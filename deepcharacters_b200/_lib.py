@@ -36,6 +36,10 @@ _SIGS: dict[str, list] = {
     "hc_eg_set_full_skinned_gradient": [vp, C.c_int32],
     "hc_eg_forward": [vp, vp, C.c_int32] + [vp] * 11,
     "hc_eg_backward": [vp, vp, C.c_int32] + [vp] * 11,
+    "hc_arap_create": [C.POINTER(vp), C.c_int32, vp, C.c_int32, vp, vp, vp, vp, vp, C.c_int32],
+    "hc_arap_destroy": [vp],
+    "hc_arap_forward": [vp, vp, C.c_int32, vp, vp, vp, vp, vp],
+    "hc_arap_backward": [vp, vp, C.c_int32, vp, vp, vp, vp],
     "hc_skin_create": [C.POINTER(vp), C.c_int32, vp, vp, vp, vp, vp, C.c_int32, vp, vp, vp, C.c_int32, vp, vp,
                        C.c_int32, vp, vp, C.c_int32, vp],
     "hc_skin_destroy": [vp],

@@ -419,6 +419,56 @@ def render_scene(subdiv: int, batch: int, views: int, width: int, height: int, s
                 N=N, F=faces.shape[0], B=batch, C=views, W=width, H=height)
 
 
+@dataclasses.dataclass
+class NodeGraph:
+    """Node -> node neighbours and rigidity weights of an embedded graph, the
+    arrays the ARAP regulariser reads (Skeletool/Mesh/EmbeddedGraph.cpp:
+    155-167, 327-436, 460-490): per node an ascending neighbour list (the
+    reference keeps them in a std::set) as a CSR, and the mean segmentation
+    weight of the vertices connected to the node."""
+    n2n_offsets: np.ndarray
+    n2n_sizes: np.ndarray
+    n2n_indices: np.ndarray
+    rigidity: np.ndarray
+    max_connections: int
+
+
+def node_graph(verts: np.ndarray, graph: EmbeddedGraph, k: int, rng: np.random.Generator,
+               refinement: bool = False, seg_weights: np.ndarray | None = None) -> NodeGraph:
+    """Neighbours: the ``k`` nearest other nodes of every node, made
+    symmetric (the reference takes the edges of its graph mesh, which are
+    symmetric).  Rigidity: per-vertex segmentation weights (U[1, 40] unless
+    given) averaged over each node's vertex connections, the ones below 20
+    divided by 10 in the refinement mode (EmbeddedGraph.cpp:460-490)."""
+    M = graph.n_nodes
+    g = verts[graph.node_vertex].astype(np.float64)
+    d = np.linalg.norm(g[:, None] - g[None], axis=2)
+    np.fill_diagonal(d, np.inf)
+    near = np.argsort(d, axis=1, kind="stable")[:, :k]
+    nb = [set() for _ in range(M)]
+    for j in range(M):
+        for q in near[j]:
+            nb[j].add(int(q))
+            nb[int(q)].add(j)
+    lists = [sorted(x) for x in nb]
+    sizes = np.array([len(x) for x in lists], np.int32)
+    offsets = np.zeros(M, np.int32)
+    offsets[1:] = np.cumsum(sizes)[:-1]
+    indices = np.array([q for x in lists for q in x], np.int32)
+    if seg_weights is None:
+        seg_weights = rng.uniform(1.0, 40.0, size=verts.shape[0]).astype(np.float32)
+    rig = np.zeros(M, np.float32)
+    cnt = np.zeros(M, np.float32)
+    for v in range(verts.shape[0]):  # the reference's loop order: vertices, then their connections
+        o, n = graph.v2n_offsets[v], graph.v2n_sizes[v]
+        for e in graph.v2n_indices[o:o + n]:
+            w = seg_weights[v]
+            rig[e] = np.float32(rig[e] + (w / np.float32(10.0) if refinement and w < 20.0 else w))
+            cnt[e] += 1
+    rig = (rig / np.maximum(cnt, 1)).astype(np.float32)
+    return NodeGraph(offsets, sizes, indices, rig, int(sizes.max()))
+
+
 def eg_scene(subdiv: int, n_nodes: int, batch: int, seed: int, k: int = 4, n_markers: int = 8,
              delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, skinned_rot_std: float = 0.1,
              skinned_t_std: float = 0.02 * MM, disp_std: float = 0.001 * MM):

@@ -240,6 +240,48 @@ hc_status hc_eg_backward(hc_eg h, void* stream, int32_t batch, const float* defo
                          const float* nodes_delta_translation, const float* vertex_displacements);
 
 /* ------------------------------------------------------------------------ */
+/* Embedded-graph ARAP regulariser                                           */
+/* ------------------------------------------------------------------------ */
+
+typedef struct hc_arap_s* hc_arap;
+
+/*
+ * EmbeddedGraphArapGpu (EmbeddedGraphArapGPUOp.cpp:5-16, kernels
+ * EmbeddedGraphArapGPUOp.cu:10-97).  The handle holds what the op's
+ * constructor reads from the character and graph files
+ * (EmbeddedGraphArapGPUOp.cpp:38-53): base vertices [N,3] (mm), node -> base
+ * vertex [M], the node -> node CSR (offsets, sizes, indices; the graph mesh's
+ * neighbours in ascending order, EmbeddedGraph.cpp:155-167, 420-436) and the
+ * per-node rigidity weights [M] (EmbeddedGraph.cpp:460-490).
+ * max_connections is the op attr max_number_of_node_connections (every node's
+ * list must fit).
+ */
+hc_status hc_arap_create(hc_arap* out, int32_t n_vertices, const float* base_vertices, int32_t n_nodes,
+                         const int32_t* node_to_base_vertex, const int32_t* n2n_offsets, const int32_t* n2n_sizes,
+                         const int32_t* n2n_indices, const float* rigidity_weights, int32_t max_connections);
+hc_status hc_arap_destroy(hc_arap h);
+/*
+ * nodes_translation, nodes_rotation (Euler, rad) [B,M,3] -> nodes_arap_loss
+ * [B,M,max_connections,3] (R_j (g_k - g_j) + g_j + t_j - (g_k + t_k), zeros in
+ * the padding slots), d_connection_weights [B,M,max_connections]
+ * ((rho_j + rho_k) / 2, 0 in padding), d_rotation [B,M,3] (the rotation
+ * input, for the gradient op).
+ */
+hc_status hc_arap_forward(hc_arap h, void* stream, int32_t batch, const float* nodes_translation,
+                          const float* nodes_rotation, float* nodes_arap_loss, float* connection_weights,
+                          float* rotation);
+/*
+ * EmbeddedGraphArapGpuGrad (EmbeddedGraphArapGPUOpGrad.cpp:5-15, kernel
+ * EmbeddedGraphArapGPUOpGrad.cu:9-96): nodes_arap_loss gradient
+ * [B,M,max_connections,3] and d_a [B,M,3] -> nodes_t_grad, nodes_r_grad
+ * [B,M,3].  As the reference, the connection weights get no gradient and the
+ * translation gradient of a pair takes the neighbour's slot that names this
+ * node (the last one if it appears twice; none if it is missing).
+ */
+hc_status hc_arap_backward(hc_arap h, void* stream, int32_t batch, const float* nodes_arap_loss_grad,
+                           const float* nodes_rotation, float* nodes_translation_grad, float* nodes_rotation_grad);
+
+/* ------------------------------------------------------------------------ */
 /* Forward kinematics + dual-quaternion / linear-blend skinning              */
 /* ------------------------------------------------------------------------ */
 

@@ -259,6 +259,48 @@ def eg_backward(d, gv, gm, dT, dA, sA, disp, full=False, precision="f64"):
     return out
 
 
+class RefArap:
+    """The reference ARAP regulariser kernels (GPU), on torch CUDA tensors
+    (EmbeddedGraphArapGPUOp.cu:10-97, EmbeddedGraphArapGPUOpGrad.cu:9-104)."""
+
+    def __init__(self, base, node_vertex, off, size, idx, rigid, maxc, device):
+        import torch
+        t = lambda x, dt: torch.from_numpy(np.ascontiguousarray(np.asarray(x, dt))).to(device)  # noqa: E731
+        self.d = {"base": t(base, np.float32), "nv": t(node_vertex, np.int32), "off": t(off, np.int32),
+                  "size": t(size, np.int32), "idx": t(idx, np.int32), "rigid": t(rigid, np.float32)}
+        self.M, self.maxc = len(node_vertex), int(maxc)
+        L = ref_lib()
+        L.hcref_arap_forward.restype = C.c_int
+        L.hcref_arap_forward.argtypes = [C.c_int] * 3 + [C.c_void_p] * 11
+        L.hcref_arap_backward.restype = C.c_int
+        L.hcref_arap_backward.argtypes = [C.c_int] * 3 + [C.c_void_p] * 10
+
+    def forward(self, T, A):
+        import torch
+        B, dev, d = T.shape[0], T.device, self.d
+        loss = torch.zeros((B, self.M, self.maxc, 3), device=dev)
+        w = torch.zeros((B, self.M, self.maxc), device=dev)
+        rot = torch.zeros((B, self.M, 3), device=dev)
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_arap_forward(B, self.M, self.maxc, _p(d["size"]), _p(d["idx"]), _p(d["off"]),
+                                          _p(d["rigid"]), _p(d["nv"]), _p(d["base"]), _p(T), _p(A), _p(loss), _p(w),
+                                          _p(rot))
+        assert st == 0, st
+        return loss, w, rot
+
+    def backward(self, gloss, A):
+        import torch
+        B, dev, d = A.shape[0], A.device, self.d
+        gT = torch.zeros((B, self.M, 3), device=dev)
+        gA = torch.zeros((B, self.M, 3), device=dev)
+        torch.cuda.synchronize()
+        st = ref_lib().hcref_arap_backward(B, self.M, self.maxc, _p(d["size"]), _p(d["idx"]), _p(d["off"]),
+                                           _p(d["rigid"]), _p(d["nv"]), _p(d["base"]), _p(gloss), _p(A), _p(gT),
+                                           _p(gA))
+        assert st == 0, st
+        return gT, gA
+
+
 class RefEG:
     """The reference embedded-graph kernels (GPU), on torch CUDA tensors."""
 

@@ -123,9 +123,28 @@ def uv(out):
                         verts=sc["verts"], extr=sc["extr"], intr=sc["intr"], **res)
 
 
+def arap(out):
+    sc = S.eg_scene(2, 40, batch=2, seed=21, n_markers=0)
+    ng = S.node_graph(sc["verts"], sc["graph"], 4, np.random.default_rng(22))
+    ref = O.RefArap(sc["verts"], sc["graph"].node_vertex, ng.n2n_offsets, ng.n2n_sizes, ng.n2n_indices, ng.rigidity,
+                    ng.max_connections, DEV)
+    T = (sc["dT"] * 3.0).astype(np.float32)
+    A = (sc["dA"] * 4.0).astype(np.float32)
+    loss, w, rot = ref.forward(t(T), t(A))
+    g = np.random.default_rng(23).normal(size=tuple(loss.shape)).astype(np.float32)
+    gT, gA = ref.backward(t(g), rot)
+    np.savez_compressed(os.path.join(out, "arap.npz"), base=sc["verts"], node_vertex=sc["graph"].node_vertex,
+                        off=ng.n2n_offsets, size=ng.n2n_sizes, idx=ng.n2n_indices, rigid=ng.rigidity,
+                        maxc=ng.max_connections, T=T, A=A, g=g, out_loss=n(loss), out_w=n(w), out_rot=n(rot),
+                        grad_T=n(gT), grad_A=n(gA))
+
+
 if __name__ == "__main__":
     out = sys.argv[1] if len(sys.argv) > 1 else HERE
+    only = set(sys.argv[2:])  # optional: names of the fixtures to (re)make
     os.makedirs(out, exist_ok=True)
-    for fn in (render, eg, skin, silhouette, uv):
+    for fn in (render, eg, skin, silhouette, uv, arap):
+        if only and fn.__name__ not in only:
+            continue
         fn(out)
         print("wrote", fn.__name__)

@@ -112,3 +112,16 @@ def test_uv_table_matches_reference_golden():
     idx = tab[..., 0].astype(int)
     pos = (v[f[idx, 0]] * tab[..., 1:2] + v[f[idx, 1]] * tab[..., 2:3] + v[f[idx, 2]] * tab[..., 3:4])
     assert np.abs(pos[same] - g["out_position"][0][same]).max() < 1e-2
+
+
+def test_arap_oracle_matches_reference_golden():
+    from oracle import arap_oracle as AO
+    z = load("arap.npz")
+    args = (z["base"], z["node_vertex"], z["off"], z["size"], z["idx"])
+    loss, w, rot = AO.arap_forward(*args, z["rigid"], int(z["maxc"]), z["T"], z["A"])
+    assert nrel(loss, z["out_loss"]) < 1e-6
+    assert np.array_equal(w.astype(np.float32), z["out_w"])
+    assert np.array_equal(rot.astype(np.float32), z["out_rot"])
+    gT, gA = AO.arap_backward(*args, int(z["maxc"]), z["g"], z["A"])
+    assert nrel(gT, z["grad_T"]) < 1e-6
+    assert nrel(gA, z["grad_A"]) < 1e-5
