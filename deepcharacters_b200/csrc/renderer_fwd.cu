@@ -215,16 +215,18 @@ __global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
                       int2* __restrict__ spill, long long spill_cap, unsigned long long* __restrict__ spill_keys,
                       int spill_tile_cap, RasterStats* __restrict__ stats) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const bool live = i < (long long)V * F;
-    int view = 0, f = 0;
+    // grid (triangle blocks, views): no 64-bit division per thread
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = fi < F;
+    const int view = blockIdx.y;
+    const long long i = (long long)view * F + fi;
+    int f = 0;
     int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
     int W = 0, H = 0, tiles_x = 1;
     long long tile_base = 0;
     Footprint fp;
     if (live) {
-        view = (int)(i / F);
-        f = (int)(i % F);
+        f = fi;
         const int b = view / C;
         const ViewCam& cam = cams[view];
         W = cam.W;
@@ -851,7 +853,8 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     ws.clock.begin(kKBin, s);
     k_project_vertices<<<div_up((long long)V * N, 256), 256, 0, s>>>(V, C, N, verts, cams, ws.proj.as<float4>());
     HC_CHECK_LAUNCH();
-    k_bin<<<div_up((long long)V * F, 256), 256, 0, s>>>(
+    HC_REQUIRE(V <= 65535, "too many views in one call (%d)", V);
+    k_bin<<<dim3(div_up(F, 256), V), 256, 0, s>>>(
         V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), ws.proj.as<float4>(), cams, tf, tv, tstate,
         ws.bins.as<int>(),
         ws.spill.as<int2>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap, stats);

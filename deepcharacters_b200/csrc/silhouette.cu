@@ -303,10 +303,13 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_hint(int N, int F, c
 // tile per lane, reading the record back from global memory.
 __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
                           CovBins cb) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    // grid (triangle blocks, views): no 64-bit division per thread
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned lane = threadIdx.x & 31;
-    const bool live = i < (long long)V * F;
-    int view = 0, f = 0;
+    const bool live = fi < F;
+    const int view = blockIdx.y;
+    const long long i = (long long)view * F + fi;
+    int f = 0;
     CoverTri t;
     t.x0 = 0;
     t.x1 = -1;
@@ -314,8 +317,7 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
     t.y1 = -1;
     Footprint fp;
     if (live) {
-        view = (int)(i / F);
-        f = (int)(i % F);
+        f = fi;
         cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
     }
     bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
@@ -559,10 +561,12 @@ __global__ void k_grid_fill(int B, int C, int N, int U, int V, SilGrid g, const 
 __global__ void k_sil_pixels(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
                              const unsigned char* __restrict__ dt, const float* __restrict__ crops,
                              float* __restrict__ residual1, float* __restrict__ closest) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * C * U * V) return;
-    const long long view = i / ((long long)U * V);
-    const int vid = (int)((i / U) % V), uid = (int)(i % U);
+    // grid (pixel blocks of one view, views): 32-bit index arithmetic per pixel
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= U * V) return;
+    const long long view = blockIdx.y;
+    const long long i = view * U * V + p;
+    const int vid = p / U, uid = p - vid * U;
     const unsigned char* D = dt + view * (long long)U * V;
     int best = -1;
     float2 imgpos = make_float2(0.f, 0.f);
@@ -761,7 +765,7 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
         p2d = h->p2d.as<float>();
     }
     const long long views = (long long)batch * n_cameras;
-    const long long nt = views * h->F;
+    HC_REQUIRE(views <= 65535, "too many views in one call (%lld)", views);
     CovBins cb;
     cb.tiles_x = div_up(width, kCovTile);
     cb.T = cb.tiles_x * div_up(height, kCovTile);
@@ -782,8 +786,8 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
         HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
     }
     HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)views * cb.T, s));
-    k_cov_bin<<<div_up(nt, 256), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
-                                              reinterpret_cast<const float2*>(p2d), cb);
+    k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
+                                                                       reinterpret_cast<const float2*>(p2d), cb);
     HC_CHECK_LAUNCH();
     k_cov_tile<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(h->F, cb);
     HC_CHECK_LAUNCH();
@@ -863,6 +867,7 @@ extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_
     cudaStream_t s = (cudaStream_t)stream;
     const int U = resolution_u, V = resolution_v, N = n_points;
     const long long views = (long long)batch * n_cameras;
+    HC_REQUIRE(views <= 65535 && (long long)U * V < (1ll << 31), "too many views or pixels in one call");
     SilGrid g;
     g.gx = div_up(U, 30) + 3;
     g.gy = div_up(V, 30) + 3;
@@ -888,8 +893,8 @@ extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_
     k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
-    const long long npx = views * U * V;
-    k_sil_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space,
+    k_sil_pixels<<<dim3(div_up((long long)U * V, 256), (unsigned)views), 256, 0, s>>>(batch, n_cameras, N, U, V, g,
+                                                                                      points_image_space,
                                                   distance_transform_image, multi_view_crops, mv_dt_residual_1,
                                                   closest_vertex_id);
     HC_CHECK_LAUNCH();
@@ -968,6 +973,7 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
                "NULL pointer");
     const int U = resolution_u, V = resolution_v, N = n_points;
     const long long views = (long long)batch * n_cameras;
+    HC_REQUIRE(views <= 65535 && (long long)U * V < (1ll << 31), "too many views or pixels in one call");
     SilGrid g;
     g.gx = div_up(U, 30) + 3;
     g.gy = div_up(V, 30) + 3;
@@ -999,8 +1005,8 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
     k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
-    const long long npx = views * U * V;
-    k_sil_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space,
+    k_sil_pixels<<<dim3(div_up((long long)U * V, 256), (unsigned)views), 256, 0, s>>>(batch, n_cameras, N, U, V, g,
+                                                                                      points_image_space,
                                                   distance_transform_image, multi_view_crops, mv_dt_residual_1,
                                                   closest_vertex_id);
     HC_CHECK_LAUNCH();
