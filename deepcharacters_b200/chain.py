@@ -193,6 +193,31 @@ class DeformRenderChain:
         self.silhouette_backward()
         self.backward()
 
+    def capture_step(self, inputs: dict | None = None) -> torch.cuda.CUDAGraph:
+        """Capture one step (forward, silhouette, both adjoints) in a CUDA
+        graph that reads the tensors of ``inputs`` (keys and shapes of
+        ``self.inp``; the current inputs by default).  A replay runs the step
+        on what those tensors hold at that time.  Run one eager step first: it
+        sizes every workspace, and no allocation may happen during capture."""
+        saved = dict(self.inp)
+        if inputs:
+            for k, v in inputs.items():
+                if k not in self.inp or v.shape != self.inp[k].shape or v.dtype != self.inp[k].dtype:
+                    raise ValueError(f"input {k!r} must match the chain's {k} tensor")
+            self.inp.update(inputs)
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(device=self.loss.device)
+        s.wait_stream(torch.cuda.current_stream())
+        try:
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(g, stream=s):
+                    self.step()
+        finally:
+            torch.cuda.current_stream().wait_stream(s)
+            self.inp.clear()
+            self.inp.update(saved)
+        return g
+
     def stages(self):
         return (("deform_render_forward", self.forward), ("silhouette_forward", self.silhouette_forward),
                 ("silhouette_backward", self.silhouette_backward), ("render_eg_backward", self.backward))

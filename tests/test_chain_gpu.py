@@ -89,3 +89,27 @@ def test_graph_replay_matches_eager(scene):
         assert nrel(ch.buf[k], eager[k]) < 1e-5, k
     assert nrel(ch.loss, loss) < 1e-6
     assert int(ch.buf["isb"].sum()) > 0 and float(ch.buf["gT"].abs().sum()) > 0
+
+
+def test_capture_step_reads_the_given_input_buffers(scene):
+    """capture_step on a second set of input tensors: replaying it after
+    filling them gives the eager step's results, and the chain's own inputs
+    are left in place."""
+    ch = DeformRenderChain(scene, DEV, B, C, RES, RES)
+    ch.step()
+    torch.cuda.synchronize()
+    eager = {k: ch.buf[k].clone() for k in ("face", "render", "isb", "gT", "gcol")}
+    own = {k: v.data_ptr() for k, v in ch.inp.items()}
+    other = {k: torch.zeros_like(v) for k, v in ch.inp.items()}
+    g = ch.capture_step(other)
+    assert {k: v.data_ptr() for k, v in ch.inp.items()} == own
+    for k, v in other.items():
+        v.copy_(ch.inp[k])
+    for k in eager:
+        ch.buf[k].zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    for k in ("face", "render", "isb"):
+        assert torch.equal(ch.buf[k], eager[k]), k
+    for k in ("gT", "gcol"):
+        assert nrel(ch.buf[k], eager[k]) < 1e-5, k
