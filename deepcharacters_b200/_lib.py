@@ -25,6 +25,10 @@ _SIGS: dict[str, list] = {
     "hc_renderer_reserve": [vp, C.c_int32],
     "hc_renderer_set_tuning": [vp, C.c_int32, C.c_int32],
     "hc_renderer_forward": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp],
+    "hc_renderer_forward_l1": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp,
+                               vp, vp, vp],
+    "hc_renderer_backward_l1": [vp, vp, C.c_int32, vp, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp,
+                                vp, vp, vp, vp, vp, vp],
     "hc_renderer_forward_ex": [vp, vp, C.c_int32, vp, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp,
                                vp, vp, vp],
     "hc_renderer_stats": [vp, vp, c_i64_p, c_i64_p],

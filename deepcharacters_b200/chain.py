@@ -51,7 +51,7 @@ class DeformRenderChain:
 
     def __init__(self, sc, dev, frames: int, views: int, width: int, height: int, w_sil: float = 1e-3,
                  w_sil1: float = 1e-3, tile: int = 8, bin_capacity: int = 256, gradient_parity: bool = False,
-                 joint_gradients: bool = True):
+                 joint_gradients: bool = True, fused_l1: bool = True):
         B, C, H, W, N = frames, views, height, width, int(sc["verts"].shape[0])
         M = int(sc["graph"].n_nodes)
         Mk = int(len(sc["markers"]))
@@ -60,6 +60,10 @@ class DeformRenderChain:
         self.skin = SkinningEngine(character(sc))
         self.skin.reserve(B)
         self.joint_gradients = bool(joint_gradients)
+        # the image L1 inside the raster's tile pass and adjoint
+        # (hc_renderer_forward_l1 / _backward_l1) or as its own op
+        # (hc_image_l1_loss + hc_renderer_backward on the gradient image)
+        self.fused_l1 = bool(fused_l1)
         self.eg = EmbeddedGraphEngine(eg_data(sc), full_skinned_gradient=self.joint_gradients)
         self.eg.reserve(B)
         self.rend = RendererEngine(sc["faces"], sc["texcoords"], N, C, W, H, "vertexColor", "shadeless", 2, 2)
@@ -83,7 +87,7 @@ class DeformRenderChain:
             sT=e(B, M, 3), sA=e(B, M, 3), dq=e(B, self.skin.S, 8),
             v=e(B, N, 3), n=e(B, N, 3), mk=e(B, Mk, 3), graph=e(B, M, 3), da=e(B, M, 3), sa=e(B, M, 3),
             bary=e(B, C, H, W, 2), face=e(B, C, H, W, dt=torch.int32), render=e(B, C, H, W, 3),
-            vnormal=e(B, C, N, 3), grad_img=e(B, C, H, W, 3),
+            vnormal=e(B, C, N, 3), grad_img=None if fused_l1 else e(B, C, H, W, 3),
             p2d=e(B, C, N, 2), n2d=e(B, C, N, 2), isb=e(B, C, N, dt=torch.uint8),
             res=e(B, C, N), res1=e(B, C, H, W, 2), dtg=e(B, C, N, 2), cid=e(B, C, H, W),
             g_res=e(B, C, N), g_res1=e(B, C, H, W, 2), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
@@ -102,6 +106,11 @@ class DeformRenderChain:
           P(o["sT"]), P(o["sA"]), P(o["dq"]))
         L("hc_eg_forward", self.eg.handle, s, B, P(i["dT"]), P(i["dA"]), P(o["sT"]), P(o["sA"]), P(i["disp"]),
           P(o["v"]), P(o["n"]), P(o["mk"]), P(o["graph"]), P(o["da"]), P(o["sa"]))
+        if self.fused_l1:
+            L("hc_renderer_forward_l1", self.rend.handle, s, B, P(o["v"]), P(i["colors"]), P(i["texture"]),
+              *self.tex_hw, P(i["sh"]), P(i["extr"]), P(i["intr"]), P(o["bary"]), P(o["face"]), P(o["render"]),
+              P(o["vnormal"]), P(i["target"]), None, P(self.ws), P(self.loss))
+            return
         L("hc_renderer_forward", self.rend.handle, s, B, P(o["v"]), P(i["colors"]), P(i["texture"]), *self.tex_hw,
           P(i["sh"]), P(i["extr"]), P(i["intr"]), P(o["bary"]), P(o["face"]), P(o["render"]), P(o["vnormal"]), None)
         L("hc_image_l1_loss", s, B * C * H * W, P(o["render"]), P(i["target"]), P(o["face"]), None, P(self.ws),
@@ -141,9 +150,14 @@ class DeformRenderChain:
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
         B, N = self.B, self.N
-        L("hc_renderer_backward", self.rend.handle, s, B, P(o["grad_img"]), P(o["v"]), P(i["colors"]),
-          P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]), P(o["bary"]), P(o["face"]),
-          P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
+        if self.fused_l1:
+            L("hc_renderer_backward_l1", self.rend.handle, s, B, P(self.ws), P(o["render"]), None, P(o["v"]),
+              P(i["colors"]), P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]),
+              P(o["bary"]), P(o["face"]), P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
+        else:
+            L("hc_renderer_backward", self.rend.handle, s, B, P(o["grad_img"]), P(o["v"]), P(i["colors"]),
+              P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]), P(o["bary"]),
+              P(o["face"]), P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
         L("hc_add_inplace", s, B * N * 3, P(o["gv"]), P(o["gv_sil"]))
         full = self.joint_gradients
         L("hc_eg_backward", self.eg.handle, s, B, P(o["gv"]), P(o["gm"]), P(o["da"]), P(o["sa"]), P(o["gT"]),

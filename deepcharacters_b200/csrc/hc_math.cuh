@@ -106,3 +106,20 @@ HC_HD M44 inverse44(const M44& m) {
     for (int i = 0; i < 16; ++i) r.e[i] = inv[i] * rdet;
     return r;
 }
+
+// Masked image L1 of the training step (Projects/HoloportedCharacters/
+// HPCMeshDL.py:642-688).  One channel's difference: render and target scaled
+// by 255 and then subtracted, each product rounded on its own as the separate
+// TF ops do (no fused multiply-add).
+__device__ __forceinline__ float l1_diff(float r, float t) {
+    return __fsub_rn(__fmul_rn(255.f, r), __fmul_rn(255.f, t));
+}
+// d loss / d render of one channel: 255 sign(difference) / count, scale = 255 / count
+__device__ __forceinline__ float l1_grad(float d, float scale) { return d > 0.f ? scale : (d < 0.f ? -scale : 0.f); }
+
+// Running L1 state (16 bytes, the workspace of the L1 entry points): the sum
+// of |difference| and the number of non-zero differences.
+struct L1State {
+    double sum;
+    unsigned long long count;
+};

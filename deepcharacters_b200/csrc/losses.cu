@@ -7,14 +7,12 @@
 #include <math.h>
 
 #include "hc_common.cuh"
+#include "hc_math.cuh"
 
 namespace hc {
 namespace {
 
-struct L1Acc {
-    double sum;
-    unsigned long long count;
-};
+using L1Acc = L1State;
 
 __global__ void k_l1_reduce(long long n_px, const float* __restrict__ render, const float* __restrict__ target,
                             const int* __restrict__ face, const unsigned char* __restrict__ mask,
@@ -27,7 +25,7 @@ __global__ void k_l1_reduce(long long n_px, const float* __restrict__ render, co
         if (!m) continue;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const float d = 255.f * render[3 * p + c] - 255.f * target[3 * p + c];
+            const float d = l1_diff(render[3 * p + c], target[3 * p + c]);
             s += fabsf(d);
             cnt += d != 0.f;
         }
@@ -70,8 +68,7 @@ __global__ void k_l1_grad(long long n_px, const float* __restrict__ render, cons
         for (int c = 0; c < 3; ++c) {
             float g = 0.f;
             if (m) {
-                const float d = 255.f * render[3 * p + c] - 255.f * target[3 * p + c];
-                g = d > 0.f ? scale : (d < 0.f ? -scale : 0.f);
+                g = l1_grad(l1_diff(render[3 * p + c], target[3 * p + c]), scale);
             }
             grad[3 * p + c] = g;
         }

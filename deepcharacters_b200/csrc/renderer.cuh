@@ -341,6 +341,18 @@ struct KernelClock {
     }
 };
 
+// The masked image L1 fused into the raster (hc_renderer_forward_l1 /
+// hc_renderer_backward_l1): the forward's tile pass accumulates the loss of
+// the pixels it shades, the adjoint forms the image gradient inline instead
+// of reading it.
+struct L1Fuse {
+    const float* target = nullptr;        // [B, P_frame, 3]
+    const unsigned char* mask = nullptr;  // [B, P_frame] foreground mask, or NULL
+    L1State* state = nullptr;             // written by the forward, read by the adjoint
+    float* loss = nullptr;                // forward: sum / count, or NULL
+    const float* render = nullptr;        // adjoint: the forward's render buffer
+};
+
 struct RasterWorkspace {
     int cap_views = 0;   // views the buffers are sized for
     int tile = 16;
@@ -354,6 +366,7 @@ struct RasterWorkspace {
     int spill_tile_cap = 0;
     DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;
     DevBuf proj;  // float4 [V,N]: projected vertices of the current call
+    DevBuf l1_part;  // per raster tile: float L1 sum, unsigned count (fused L1 only)
     KernelClock clock;
 };
 

@@ -11,7 +11,8 @@ namespace hc {
 hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int albedo,
                          int shading, const float* verts, const float* colors, const float* texture, int tex_h,
                          int tex_w, const float* sh, const float* extr, const float* intr, float* bary, int* face,
-                         float* render, float* vnormal, int* depth_q, int* tie_count);
+                         float* render, float* vnormal, int* depth_q, int* tie_count,
+                         const L1Fuse* l1 = nullptr);
 hc_status raster_reserve(RasterWorkspace& ws, int views, int F);
 hc_status raster_uv_maps(const Topology& topo, UvTable& tab, cudaStream_t s, int B, int C, long long P_frame, int mode,
                          const float* verts, int tex_h, int tex_w, float* bary, int* face, float* render,
@@ -21,7 +22,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
                           const float* colors, const float* texture, int tex_h, int tex_w, const float* sh,
                           const float* target, const float* vnormal, const float* bary, const int* face,
                           const float* extr, const float* intr, float* vpos_grad, float* vcol_grad, float* tex_grad,
-                          float* sh_grad, int parity);
+                          float* sh_grad, int parity, const L1Fuse* l1 = nullptr);
 
 static int parse_albedo(const char* m) {
     if (!m) return -1;
@@ -291,6 +292,70 @@ extern "C" hc_status hc_renderer_backward(hc_renderer h, void* stream, int32_t b
                            vertex_color, texture, texture_height, texture_width, sh_coeff, target_image,
                            vertex_normal, barycentric_buffer, face_buffer, extrinsics, intrinsics, vertex_pos_grad,
                            vertex_color_grad, texture_grad, sh_coeff_grad, h->grad_parity);
+}
+
+extern "C" hc_status hc_renderer_forward_l1(hc_renderer h, void* stream, int32_t batch, const float* vertex_pos,
+                                            const float* vertex_color, const float* texture,
+                                            int32_t texture_height, int32_t texture_width, const float* sh_coeff,
+                                            const float* extrinsics, const float* intrinsics,
+                                            float* barycentric_buffer, int32_t* face_buffer, float* render_buffer,
+                                            float* vertex_normal, const float* target_image,
+                                            const uint8_t* foreground_mask, void* l1_state, float* loss) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    HC_REQUIRE(batch > 0, "batch must be positive (%d)", batch);
+    HC_REQUIRE(h->normal_map == kNmNone, "the fused L1 needs compute_normal_map = none");
+    HC_REQUIRE(vertex_pos && extrinsics && intrinsics && barycentric_buffer && face_buffer && render_buffer &&
+                   vertex_normal && target_image && l1_state,
+               "NULL input/output pointer");
+    if (h->albedo == kVertexColor) HC_REQUIRE(vertex_color, "vertexColor mode needs vertex_color");
+    if (h->albedo == kTextured || h->albedo == kTexturedBilinear) {
+        HC_REQUIRE(texture && texture_width > 0 && texture_height > 0, "textured mode needs a texture");
+        HC_REQUIRE(h->topo.has_texcoords, "textured mode needs texture_coordinates");
+    }
+    const bool needs_sh = (h->shading == kShaded && h->albedo != kNormal) || h->albedo == kLighting;
+    if (needs_sh) HC_REQUIRE(sh_coeff, "shading needs sh_coeff");
+    L1Fuse l1;
+    l1.target = target_image;
+    l1.mask = foreground_mask;
+    l1.state = static_cast<L1State*>(l1_state);
+    l1.loss = loss;
+    return raster_forward(h->topo, h->ws, (cudaStream_t)stream, batch, h->C, h->albedo, h->shading, vertex_pos,
+                          vertex_color, texture, texture_height, texture_width, sh_coeff, extrinsics, intrinsics,
+                          barycentric_buffer, face_buffer, render_buffer, vertex_normal, nullptr, nullptr, &l1);
+}
+
+extern "C" hc_status hc_renderer_backward_l1(hc_renderer h, void* stream, int32_t batch, const void* l1_state,
+                                             const float* render_buffer, const uint8_t* foreground_mask,
+                                             const float* vertex_pos, const float* vertex_color,
+                                             const float* texture, int32_t texture_height, int32_t texture_width,
+                                             const float* sh_coeff, const float* target_image,
+                                             const float* vertex_normal, const float* barycentric_buffer,
+                                             const int32_t* face_buffer, const float* extrinsics,
+                                             const float* intrinsics, float* vertex_pos_grad,
+                                             float* vertex_color_grad, float* texture_grad, float* sh_coeff_grad) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    HC_REQUIRE(batch > 0, "batch must be positive (%d)", batch);
+    HC_REQUIRE(h->albedo == kVertexColor || h->albedo == kTextured || h->albedo == kTexturedBilinear,
+               "renderer gradients exist only for vertexColor and textured albedo");
+    HC_REQUIRE(l1_state && render_buffer && vertex_pos && target_image && vertex_normal && barycentric_buffer &&
+                   face_buffer && extrinsics && intrinsics && vertex_pos_grad,
+               "NULL input/output pointer");
+    if (h->albedo == kVertexColor) HC_REQUIRE(vertex_color && vertex_color_grad, "vertexColor mode needs colours");
+    if (h->albedo == kTextured || h->albedo == kTexturedBilinear)
+        HC_REQUIRE(texture && texture_grad && texture_width > 0 && texture_height > 0, "textured mode needs a texture");
+    if (h->shading == kShaded) HC_REQUIRE(sh_coeff && sh_coeff_grad, "shaded mode needs sh_coeff");
+    L1Fuse l1;
+    l1.target = target_image;
+    l1.mask = foreground_mask;
+    l1.state = const_cast<L1State*>(static_cast<const L1State*>(l1_state));
+    l1.render = render_buffer;
+    return raster_backward(h->topo, h->ws, h->nrm_grad, (cudaStream_t)stream, batch, h->C, h->albedo,
+                           h->shading, h->image_filter, h->texture_filter, nullptr, vertex_pos, vertex_color, texture,
+                           texture_height, texture_width, sh_coeff, target_image, vertex_normal, barycentric_buffer,
+                           face_buffer, extrinsics, intrinsics, vertex_pos_grad, vertex_color_grad, texture_grad,
+                           sh_coeff_grad, h->grad_parity, &l1);
 }
 
 extern "C" hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t parity) {

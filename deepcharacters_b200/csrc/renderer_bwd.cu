@@ -57,6 +57,11 @@ struct BwdArgs {
     float* tex_grad;        // [B,TH,TW,3]
     float* sh_grad;         // [V,27]
     float* nrm_grad;        // [B,N,3] workspace: d loss / d (unnormalised vertex normal)
+    // fused image L1: the image gradient is formed from the render and the
+    // target instead of read from grad (NULL state: not fused)
+    const L1State* l1_state;
+    const float* l1_render;          // [V,H,W,3]
+    const unsigned char* l1_mask;    // [V,H,W] or NULL
 };
 
 __device__ __forceinline__ float3 unit3(int k) {
@@ -198,6 +203,11 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
     constexpr bool bilinear = ALB == kAlbTexBilinear;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const bool staged = A.ifs <= MAXFS;
+    float l1_scale = 0.f;  // 255 / count of the fused L1
+    if (A.l1_state) {
+        const unsigned long long cnt = A.l1_state->count;
+        l1_scale = cnt ? 255.f / (float)cnt : 0.f;
+    }
     if (staged) {
         // tap weights and their normaliser, once per CTA: the same divisions
         // and the same summation order as evaluating them per pixel
@@ -289,7 +299,16 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, 
         v2 = ld3(P + 3 * id.z);
         const float* VN = A.vnormal + (long long)view * A.N * 3;
         const float3 n0 = ld3(VN + 3 * id.x), n1 = ld3(VN + 3 * id.y), n2 = ld3(VN + 3 * id.z);
-        G = ld3(A.grad + 3 * pix);
+        if (A.l1_state) {  // d L1 / d render (k_l1_grad's arithmetic)
+            G = make_float3(0.f, 0.f, 0.f);
+            if (!A.l1_mask || A.l1_mask[pix]) {
+                const float3 r = ld3(A.l1_render + 3 * pix), t = ld3(A.target + 3 * pix);
+                G = make_float3(l1_grad(l1_diff(r.x, t.x), l1_scale), l1_grad(l1_diff(r.y, t.y), l1_scale),
+                                l1_grad(l1_diff(r.z, t.z), l1_scale));
+            }
+        } else {
+            G = ld3(A.grad + 3 * pix);
+        }
         frag = ba * v0 + bb * v1 + bc * v2;
         const float3 pnu = ba * n0 + bb * n1 + bc * n2;
         const float pnv = sqrtf(pnu.x * pnu.x + pnu.y * pnu.y + pnu.z * pnu.z);
@@ -613,7 +632,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
                           const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
                           const float* sh, const float* target, const float* vnormal, const float* bary,
                           const int* face, const float* extr, const float* intr, float* vpos_grad,
-                          float* vcol_grad, float* tex_grad, float* sh_grad, int parity) {
+                          float* vcol_grad, float* tex_grad, float* sh_grad, int parity, const L1Fuse* l1) {
     const int V = B * C, N = topo.N;
     HC_TRY(raster_layout(ws));
     HC_TRY(ws.cams.ensure(sizeof(ViewCam) * (size_t)std::max(V, ws.cap_views)));
@@ -658,6 +677,9 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.tex_grad = tex_grad;
     A.sh_grad = sh_grad;
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
+    A.l1_state = l1 ? l1->state : nullptr;
+    A.l1_render = l1 ? l1->render : nullptr;
+    A.l1_mask = l1 ? l1->mask : nullptr;
     const long long tiles = (long long)B * ws.Tb_frame;
     ws.clock.begin(kKRenderGrad, s);
     const int alb = albedo == kVertexColor ? kAlbVcol

@@ -416,6 +416,11 @@ struct ShadeArgs {
     float* render;
     int* depth_q;
     int* tie_count;
+    // fused image L1 (NULL sums: not fused)
+    const float* l1_target;
+    const unsigned char* l1_mask;
+    float* l1_sum;     // [tiles]
+    unsigned* l1_cnt;  // [tiles]
 };
 
 // colour of a pixel hit by face f at barycentrics (a, bb)
@@ -708,48 +713,106 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
             }
         }
     }
-    if (!valid) return;
-    if (st.x > cap && st.y > 0 && st.y <= spill_tile_cap) {
-        const unsigned long long key = spill_keys[(long long)(st.y - 1) * NT + threadIdx.x];
-        if (key != ~0ull) {
-            const unsigned kd = (unsigned)(key >> 32);
-            const int kf = (int)(key & 0xffffffffu);
-            if (kd < best_d) {
-                best_d = kd;
-                best_f = kf;
-                ties = 0;  // spilled ties are added by the diagnostics pass
-            } else if (kd == best_d) {
-                best_f = min(best_f, kf);
+    float l1s = 0.f;  // this pixel's image L1 terms (fused L1 only)
+    unsigned l1c = 0;
+    if (valid) {
+        if (st.x > cap && st.y > 0 && st.y <= spill_tile_cap) {
+            const unsigned long long key = spill_keys[(long long)(st.y - 1) * NT + threadIdx.x];
+            if (key != ~0ull) {
+                const unsigned kd = (unsigned)(key >> 32);
+                const int kf = (int)(key & 0xffffffffu);
+                if (kd < best_d) {
+                    best_d = kd;
+                    best_f = kf;
+                    ties = 0;  // spilled ties are added by the diagnostics pass
+                } else if (kd == best_d) {
+                    best_f = min(best_f, kf);
+                }
+            }
+        }
+        const long long pix = cam.pix_base + (long long)py * W + px;
+        if (best_d == 0xffffffffu) {
+            A.face[pix] = -1;
+            A.bary[2 * pix + 0] = 0.f;
+            A.bary[2 * pix + 1] = 0.f;
+            A.render[3 * pix + 0] = 0.f;
+            A.render[3 * pix + 1] = 0.f;
+            A.render[3 * pix + 2] = 0.f;
+            if (A.depth_q) A.depth_q[pix] = 0x7fffffff;
+            if (A.tie_count) A.tie_count[pix] = 0;
+        } else {
+            // recompute the winner's barycentrics (same arithmetic as the hit test)
+            const TriS Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
+            const TriView wv = tri_view[(long long)view * A.F + best_f];
+            int dq;
+            float a = 0.f, bb = 0.f;
+            raster_hit(ro_s, dir, Tw, wv.num, dq, a, bb);
+            A.face[pix] = best_f;
+            A.bary[2 * pix + 0] = a;
+            A.bary[2 * pix + 1] = bb;
+            const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
+            A.render[3 * pix + 0] = col.x;
+            A.render[3 * pix + 1] = col.y;
+            A.render[3 * pix + 2] = col.z;
+            if (A.depth_q) A.depth_q[pix] = (int)best_d;
+            if (A.tie_count) A.tie_count[pix] = ties;
+            if (A.l1_sum && (!A.l1_mask || A.l1_mask[pix])) {
+                const float* t = A.l1_target + 3 * pix;
+                const float d0 = l1_diff(col.x, t[0]), d1 = l1_diff(col.y, t[1]), d2 = l1_diff(col.z, t[2]);
+                l1s = fabsf(d0) + fabsf(d1) + fabsf(d2);
+                l1c = (d0 != 0.f) + (d1 != 0.f) + (d2 != 0.f);
             }
         }
     }
-    const long long pix = cam.pix_base + (long long)py * W + px;
-    if (best_d == 0xffffffffu) {
-        A.face[pix] = -1;
-        A.bary[2 * pix + 0] = 0.f;
-        A.bary[2 * pix + 1] = 0.f;
-        A.render[3 * pix + 0] = 0.f;
-        A.render[3 * pix + 1] = 0.f;
-        A.render[3 * pix + 2] = 0.f;
-        if (A.depth_q) A.depth_q[pix] = 0x7fffffff;
-        if (A.tie_count) A.tie_count[pix] = 0;
-        return;
+    if (A.l1_sum) {  // launch-uniform: the tile's partial L1 sum and count
+        __shared__ float s_l1s[NT / 32];
+        __shared__ unsigned s_l1c[NT / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            l1s += __shfl_xor_sync(0xffffffffu, l1s, o);
+            l1c += __shfl_xor_sync(0xffffffffu, l1c, o);
+        }
+        if (lane == 0) {
+            s_l1s[threadIdx.x >> 5] = l1s;
+            s_l1c[threadIdx.x >> 5] = l1c;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float ts = 0.f;
+            unsigned tc = 0;
+            for (int w = 0; w < NT / 32; ++w) {
+                ts += s_l1s[w];
+                tc += s_l1c[w];
+            }
+            A.l1_sum[g] = ts;
+            A.l1_cnt[g] = tc;
+        }
     }
-    // recompute the winner's barycentrics (same arithmetic as the hit test)
-    const TriS Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
-    const TriView wv = tri_view[(long long)view * A.F + best_f];
-    int dq;
-    float a = 0.f, bb = 0.f;
-    raster_hit(ro_s, dir, Tw, wv.num, dq, a, bb);
-    A.face[pix] = best_f;
-    A.bary[2 * pix + 0] = a;
-    A.bary[2 * pix + 1] = bb;
-    const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
-    A.render[3 * pix + 0] = col.x;
-    A.render[3 * pix + 1] = col.y;
-    A.render[3 * pix + 2] = col.z;
-    if (A.depth_q) A.depth_q[pix] = (int)best_d;
-    if (A.tie_count) A.tie_count[pix] = ties;
+}
+
+// the fused L1's tile partials summed into the L1 state (zeroed before)
+__global__ void k_l1_tiles(long long n, const float* __restrict__ sums, const unsigned* __restrict__ cnts,
+                           L1State* __restrict__ state) {
+    double s = 0.0;
+    unsigned long long c = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        s += sums[i];
+        c += cnts[i];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (s != 0.0 || c != 0)) {
+        atomicAdd(&state->sum, s);
+        atomicAdd(&state->count, c);
+    }
+}
+
+__global__ void k_l1_loss(const L1State* __restrict__ state, float* __restrict__ loss) {
+    const unsigned long long c = state->count;
+    *loss = c ? (float)(state->sum / (double)c) : 0.f;
 }
 
 // ---------------------------------------------------------------------------
@@ -820,7 +883,7 @@ hc_status raster_reserve(RasterWorkspace& ws, int views, int F) {
 hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t s, int B, int C, int albedo,
                          int shading, const float* verts, const float* colors, const float* texture, int tex_h,
                          int tex_w, const float* sh, const float* extr, const float* intr, float* bary, int* face,
-                         float* render, float* vnormal, int* depth_q, int* tie_count) {
+                         float* render, float* vnormal, int* depth_q, int* tie_count, const L1Fuse* l1) {
     const int V = B * C;
     const int N = topo.N, F = topo.F;
     HC_TRY(raster_reserve(ws, V, F));
@@ -889,6 +952,18 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.render = render;
     A.depth_q = depth_q;
     A.tie_count = tie_count;
+    A.l1_target = nullptr;
+    A.l1_mask = nullptr;
+    A.l1_sum = nullptr;
+    A.l1_cnt = nullptr;
+    if (l1) {
+        HC_TRY(ws.l1_part.ensure(8 * (size_t)tiles));
+        HC_CUDA(cudaMemsetAsync(l1->state, 0, sizeof(L1State), s));
+        A.l1_target = l1->target;
+        A.l1_mask = l1->mask;
+        A.l1_sum = ws.l1_part.as<float>();
+        A.l1_cnt = reinterpret_cast<unsigned*>(A.l1_sum + tiles);
+    }
     const int* tcam = ws.tile_cam.as<int>();
     HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
     const unsigned grid = (unsigned)tiles;
@@ -914,6 +989,14 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     }
     HC_CHECK_LAUNCH();
     ws.clock.end(kKResolve, s);
+    if (l1) {
+        k_l1_tiles<<<148 * 2, 256, 0, s>>>(tiles, A.l1_sum, A.l1_cnt, l1->state);
+        HC_CHECK_LAUNCH();
+        if (l1->loss) {
+            k_l1_loss<<<1, 1, 0, s>>>(l1->state, l1->loss);
+            HC_CHECK_LAUNCH();
+        }
+    }
     if (tie_count && depth_q) {
         k_spill<<<148 * 4, 128, 0, s>>>(C, F, TS, ws.T_frame, ws.tile_cam.as<int>(), cams, tf, tv, tstate,
                                     ws.spill.as<int2>(), ws.spill_cap,

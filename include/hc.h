@@ -157,6 +157,36 @@ hc_status hc_renderer_backward(hc_renderer h, void* stream, int32_t batch,
                                float* sh_coeff_grad);
 
 /*
+ * The renderer with the training step's masked image L1 fused in (no
+ * reference counterpart: the reference runs the L1 as separate TF ops,
+ * HPCMeshDL.py:642-688, here hc_image_l1_loss).  hc_renderer_forward_l1
+ * writes what hc_renderer_forward writes (compute_normal_map must be none)
+ * and, from the pixels it shades, the L1 state (16 bytes, the layout of
+ * hc_image_l1_loss's workspace: double sum of |255 R - 255 T|, uint64 count
+ * of non-zero terms, over pixels with a face and a non-zero foreground_mask
+ * [B,C,H,W] uint8, which may be NULL) and loss = sum / count (device float,
+ * may be NULL).  hc_renderer_backward_l1 is hc_renderer_backward with the
+ * image gradient 255 sign(255 R - 255 T) / count formed per pixel from
+ * render_buffer, target_image and that state instead of read from a
+ * gradient image.  Results equal hc_renderer_forward + hc_image_l1_loss +
+ * hc_renderer_backward up to the summation order of the loss.
+ */
+hc_status hc_renderer_forward_l1(hc_renderer h, void* stream, int32_t batch, const float* vertex_pos,
+                                 const float* vertex_color, const float* texture, int32_t texture_height,
+                                 int32_t texture_width, const float* sh_coeff, const float* extrinsics,
+                                 const float* intrinsics, float* barycentric_buffer, int32_t* face_buffer,
+                                 float* render_buffer, float* vertex_normal, const float* target_image,
+                                 const uint8_t* foreground_mask, void* l1_state, float* loss);
+hc_status hc_renderer_backward_l1(hc_renderer h, void* stream, int32_t batch, const void* l1_state,
+                                  const float* render_buffer, const uint8_t* foreground_mask,
+                                  const float* vertex_pos, const float* vertex_color, const float* texture,
+                                  int32_t texture_height, int32_t texture_width, const float* sh_coeff,
+                                  const float* target_image, const float* vertex_normal,
+                                  const float* barycentric_buffer, const int32_t* face_buffer,
+                                  const float* extrinsics, const float* intrinsics, float* vertex_pos_grad,
+                                  float* vertex_color_grad, float* texture_grad, float* sh_coeff_grad);
+
+/*
  * Barycentric Jacobian of the adjoint.  0 (default): the exact derivative of
  * the ray-hit barycentrics in closed form (rank 1 per vertex); 1: the
  * reference's 3x9 formula (dJBCDVerpos, RendererUtil.h:670-861) evaluated as

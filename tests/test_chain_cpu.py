@@ -30,10 +30,10 @@ def test_chain_step_calls(recorder):
     recorder.clear()
     ch.step()
     names = [n for n, _ in recorder]
-    assert names == ["hc_pose2eg_forward", "hc_eg_forward", "hc_renderer_forward", "hc_image_l1_loss",
+    assert names == ["hc_pose2eg_forward", "hc_eg_forward", "hc_renderer_forward_l1",
                      "hc_camera_projection_forward", "hc_camera_projection_forward", "hc_mesh_boundary_forward_hinted",
                      "hc_silhouette_forward", "hc_sum_squares_loss", "hc_sum_squares_loss", "hc_silhouette_backward",
-                     "hc_camera_projection_backward", "hc_renderer_backward", "hc_add_inplace", "hc_eg_backward",
+                     "hc_camera_projection_backward", "hc_renderer_backward_l1", "hc_add_inplace", "hc_eg_backward",
                      "hc_pose2eg_backward"]
     args = dict(recorder)
     # the EG consumes the node transforms that the node skinning wrote
@@ -41,10 +41,13 @@ def test_chain_step_calls(recorder):
     assert args["hc_eg_forward"][6] == args["hc_pose2eg_forward"][8]
     # the raster and the silhouette see the EG vertices; the summed gradient feeds the EG adjoint
     v = args["hc_eg_forward"][8]
-    assert args["hc_renderer_forward"][3] == v and args["hc_camera_projection_forward"][4] == v
-    assert args["hc_eg_backward"][3] == args["hc_renderer_backward"][16] == args["hc_add_inplace"][2]
+    assert args["hc_renderer_forward_l1"][3] == v and args["hc_camera_projection_forward"][4] == v
+    assert args["hc_eg_backward"][3] == args["hc_renderer_backward_l1"][18] == args["hc_add_inplace"][2]
+    # the fused L1: the adjoint reads the state and the render buffer the forward wrote
+    assert args["hc_renderer_backward_l1"][3] == args["hc_renderer_forward_l1"][17]
+    assert args["hc_renderer_backward_l1"][4] == args["hc_renderer_forward_l1"][13]
     # the mesh boundary takes the renderer's face buffer as its coverage hint
-    assert args["hc_mesh_boundary_forward_hinted"][10] == args["hc_renderer_forward"][12]
+    assert args["hc_mesh_boundary_forward_hinted"][10] == args["hc_renderer_forward_l1"][12]
     assert args["hc_add_inplace"][3] == args["hc_camera_projection_backward"][9]
     # joint angles: the EG's skinned-transform gradients feed the node-skinning adjoint
     assert args["hc_pose2eg_backward"][7] == args["hc_eg_backward"][9]
