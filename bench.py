@@ -183,25 +183,28 @@ def stage_bytes(sc):
     K = 4
     eg = B * (12 * N * 2 + 8 * K * N + 24 * M) + 12 * N  # read base / write verts + normals, CSR, node params
     return {
-        # EG + raster: verts read, bary 8 + face 4 + render 12 written per pixel; L1 reads render + target,
-        # writes the image gradient
-        "deform_render_forward": eg + B * C * (24 * P + 12 * N) + B * C * (12 + 12 + 4 + 12) * P,
+        # EG + raster: verts read, bary 8 + face 4 + render 12 written per pixel; the fused L1 reads the
+        # target (counted for every pixel here)
+        "deform_render_forward": eg + B * C * (24 * P + 12 * N) + B * C * 12 * P,
         # projection, coverage + boundary, per-pixel silhouette residual (dt 1, res1 8, closest 4), squared loss
         "silhouette_forward": B * C * (16 * N + 1 * P + 1 * P + 12 * P + 8 * P + 8 * 3 * N),
         "silhouette_backward": B * C * (8 * P + 4 * P + 24 * N) + B * 24 * N,
-        # bwd raster reads grad image 12 + bary 8 + face 4 per pixel, writes vertex grads; EG adjoint
-        "render_eg_backward": B * C * 24 * P + B * (36 * N + 24 * N) + eg,
+        # bwd raster reads render 12 (the fused L1 gradient) + bary 8 + face 4 + target 12 per pixel,
+        # writes vertex grads; EG adjoint
+        "render_eg_backward": B * C * 36 * P + B * (36 * N + 24 * N) + eg,
     }
 
 
-def kernel_bytes(sc):
-    """Algorithmic bytes per launch of the two raster kernels over FRAMES x VIEWS views:
-    k_resolve writes face 4 + barycentrics 8 + colour 12 B per pixel and reads each
-    frame's positions, colours and faces once; k_render_grad reads the image
-    gradient 12, barycentrics 8, face 4 and target 12 B per pixel and each frame's
+def kernel_bytes(sc, covered):
+    """Algorithmic bytes per launch of the two raster kernels over FRAMES x VIEWS views
+    with the image L1 fused in (``covered`` = pixels with a face, all views):
+    k_resolve writes face 4 + barycentrics 8 + colour 12 B per pixel, reads the
+    target (12 B) of the covered pixels and each frame's positions, colours and
+    faces once; k_render_grad reads the render 12 (the image gradient is formed
+    from it), barycentrics 8, face 4 and target 12 B per pixel and each frame's
     positions, colours and faces, and writes the position and colour gradients."""
     V, P, N, F = FRAMES * VIEWS, RES * RES, sc["N"], sc["F"]
-    return {"resolve": V * 24 * P + FRAMES * (24 * N + 12 * F),
+    return {"resolve": V * 24 * P + 12 * covered + FRAMES * (24 * N + 12 * F),
             "render_grad": V * 36 * P + FRAMES * (24 * N + 12 * F + 24 * N)}
 
 
@@ -272,7 +275,7 @@ def run_ours(args, world, rank, local):
             kern_ms.setdefault(k, []).append(kt[k])
     ch.rend.set_kernel_timing(False)
     kern_ms = {k: sum(v) / len(v) for k, v in kern_ms.items()}
-    kbytes = kernel_bytes(sc)
+    kbytes = kernel_bytes(sc, int((ch.buf["face"] >= 0).sum()))
     dom = max(kern_ms, key=kern_ms.get)
     peaks = {}
     try:
