@@ -14,6 +14,7 @@
 // 3x3 cells around it; the candidate with the smallest distance and, among
 // equal distances, the smallest vertex id is the reference's first-strictly-
 // smaller winner.
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -395,28 +396,34 @@ __global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, co
     }
 }
 
-// one CTA per (tile, view): a pixel stops at the first binned triangle that
-// covers it, the tile at the chunk after which all its pixels are covered
-__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, CovBins cb) {
+// Persistent CTAs over the (view, tile) pairs, one thread per pixel of the
+// current tile: a pixel stops at the first binned triangle that covers it,
+// the tile at the chunk after which all its pixels are covered.  Tiles
+// without entries (most of them when a coverage hint was given) cost one
+// count load instead of a CTA launch each.
+__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long long n_keys, CovBins cb) {
     __shared__ CovTileTri s_t[kCovTile * kCovTile];
-    const int tile = blockIdx.x, view = blockIdx.y;
-    const long long key = (long long)view * cb.T + tile;
-    const int n = min(cb.count[key], kCovCap);
-    if (n == 0) return;  // CTA-uniform
-    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
-    const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
-    const bool valid = px < cb.W && py < cb.H;
-    unsigned char* pix = cb.cover + ((long long)view * cb.H + py) * cb.W + px;
-    bool covered = !valid || *pix;
-    const CovTileTri* R = cb.rec + (long long)view * F;
-    for (int base = 0; base < n; base += kCovTile * kCovTile) {
-        const int m = min(kCovTile * kCovTile, n - base);
-        if (__syncthreads_and(covered)) break;  // every pixel of the tile is covered: stop staging
-        if ((int)threadIdx.x < m) s_t[threadIdx.x] = R[cb.bins[key * kCovCap + base + threadIdx.x]];
-        __syncthreads();
-        for (int j = 0; j < m && !covered; ++j) covered = cover_record_test(s_t[j], px, py);
+    for (long long key = blockIdx.x; key < n_keys; key += gridDim.x) {
+        const int n = min(cb.count[key], kCovCap);
+        if (n == 0) continue;  // CTA-uniform
+        const int view = (int)(key / cb.T), tile = (int)(key - (long long)view * cb.T);
+        const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+        const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
+        const bool valid = px < cb.W && py < cb.H;
+        unsigned char* pix = cb.cover + ((long long)view * cb.H + py) * cb.W + px;
+        bool covered = !valid || *pix;
+        const CovTileTri* R = cb.rec + (long long)view * F;
+        // every chunk starts with a barrier (so does the next tile: the staged
+        // records of this one are no longer read there)
+        for (int base = 0; base < n; base += kCovTile * kCovTile) {
+            const int m = min(kCovTile * kCovTile, n - base);
+            if (__syncthreads_and(covered)) break;  // every pixel of the tile is covered: stop staging
+            if ((int)threadIdx.x < m) s_t[threadIdx.x] = R[cb.bins[key * kCovCap + base + threadIdx.x]];
+            __syncthreads();
+            for (int j = 0; j < m && !covered; ++j) covered = cover_record_test(s_t[j], px, py);
+        }
+        if (valid && covered && !*pix) *pix = 1;
     }
-    if (valid && covered && !*pix) *pix = 1;
 }
 
 // boundary test of k_boundary against the coverage image instead of a face buffer
@@ -558,62 +565,88 @@ __global__ void k_grid_fill(int B, int C, int N, int U, int V, SilGrid g, const 
 }
 
 // data -> model term per distance-image pixel (MultiViewSilhouetteLossGPUOp.cu:142-240)
-__global__ void k_sil_pixels(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
-                             const unsigned char* __restrict__ dt, const float* __restrict__ crops,
-                             float* __restrict__ residual1, float* __restrict__ closest) {
-    // grid (pixel blocks of one view, views): 32-bit index arithmetic per pixel
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= U * V) return;
-    const long long view = blockIdx.y;
-    const long long i = view * U * V + p;
+// Data -> model term of one pixel (MultiViewSilhouetteLossGPUOp.cu:98-138):
+// a boundary pixel (DT value 127 with at least 4 boundary pixels in its 5x5
+// window) takes the nearest boundary vertex within 30 * scale px (the
+// minimum (distance, id): the reference's first strictly smaller one).
+__device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N, int U, int V, const SilGrid& g,
+                                          const float* __restrict__ p2d, const unsigned char* __restrict__ D,
+                                          const float* __restrict__ crops, float& r0, float& r1, float& cl) {
+    r0 = 0.f;
+    r1 = 0.f;
+    cl = -1.f;
+    if (dval != 127) return;
     const int vid = p / U, uid = p - vid * U;
-    const unsigned char* D = dt + view * (long long)U * V;
-    int best = -1;
-    float2 imgpos = make_float2(0.f, 0.f);
-    float scale = 1.f;
-    if ((int)D[(long long)vid * U + uid] == 127) {
-        int nb = 0;
-        for (int j = -2; j <= 2; ++j)
-            for (int k = -2; k <= 2; ++k) {
-                const int yy = vid + j, xx = uid + k;
-                if (yy >= 0 && yy < V && xx >= 0 && xx < U && (int)D[(long long)yy * U + xx] == 127) ++nb;
-            }
-        if (nb >= 4) {
-            const float* cr = crops + view * 7;
-            scale = cr[2];
-            imgpos = make_float2(((float)uid - cr[0]) * scale + cr[3], ((float)vid - cr[1]) * scale + cr[4]);
-            float bestd = 30.f * scale;
-            int cx, cy;
-            const int cells = g.gx * g.gy;
-            if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
-                for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.gy - 1); ++yy)
-                    for (int xx = max(cx - 1, 0); xx <= min(cx + 1, g.gx - 1); ++xx) {
-                        const int cell = yy * g.gx + xx;
-                        const int s0 = g.start[view * cells + cell];
-                        const int n = g.count[view * cells + cell];
-                        for (int q = 0; q < n; ++q) {
-                            const int v = g.items[view * (long long)N + s0 + q];
-                            const float* pp = p2d + (view * (long long)N + v) * 2;
-                            const float2 dlt = make_float2(pp[0] - imgpos.x, pp[1] - imgpos.y);
-                            const float dist = sqrtf(dlt.x * dlt.x + dlt.y * dlt.y);
-                            if (dist < bestd || (dist == bestd && best >= 0 && v < best)) {
-                                bestd = dist;
-                                best = v;
-                            }
-                        }
-                    }
-            }
+    int nb = 0;
+    for (int j = -2; j <= 2; ++j)
+        for (int k = -2; k <= 2; ++k) {
+            const int yy = vid + j, xx = uid + k;
+            if (yy >= 0 && yy < V && xx >= 0 && xx < U && (int)D[(long long)yy * U + xx] == 127) ++nb;
         }
+    if (nb < 4) return;
+    const float* cr = crops + view * 7;
+    const float scale = cr[2];
+    const float2 imgpos = make_float2(((float)uid - cr[0]) * scale + cr[3], ((float)vid - cr[1]) * scale + cr[4]);
+    float bestd = 30.f * scale;
+    int best = -1;
+    int cx, cy;
+    const int cells = g.gx * g.gy;
+    if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
+        for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.gy - 1); ++yy)
+            for (int xx = max(cx - 1, 0); xx <= min(cx + 1, g.gx - 1); ++xx) {
+                const int cell = yy * g.gx + xx;
+                const int s0 = g.start[view * cells + cell];
+                const int n = g.count[view * cells + cell];
+                for (int q = 0; q < n; ++q) {
+                    const int v = g.items[view * (long long)N + s0 + q];
+                    const float* pp = p2d + (view * (long long)N + v) * 2;
+                    const float2 dlt = make_float2(pp[0] - imgpos.x, pp[1] - imgpos.y);
+                    const float dist = sqrtf(dlt.x * dlt.x + dlt.y * dlt.y);
+                    if (dist < bestd || (dist == bestd && best >= 0 && v < best)) {
+                        bestd = dist;
+                        best = v;
+                    }
+                }
+            }
     }
     if (best >= 0) {
         const float* pp = p2d + (view * (long long)N + best) * 2;
-        residual1[2 * i] = (pp[0] - imgpos.x) / (30.f * scale);
-        residual1[2 * i + 1] = (pp[1] - imgpos.y) / (30.f * scale);
-        closest[i] = (float)best;
-    } else {
-        residual1[2 * i] = 0.f;
-        residual1[2 * i + 1] = 0.f;
-        closest[i] = -1.f;
+        r0 = (pp[0] - imgpos.x) / (30.f * scale);
+        r1 = (pp[1] - imgpos.y) / (30.f * scale);
+        cl = (float)best;
+    }
+}
+
+// Four consecutive pixels per thread, grid (pixel blocks of one view, views):
+// one 4-byte DT load and 16-byte stores when the buffers allow (vec), and
+// 32-bit index arithmetic.  Most pixels are not on the boundary and only
+// write their zero outputs.
+__global__ void k_sil_pixels(int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
+                             const unsigned char* __restrict__ dt, const float* __restrict__ crops,
+                             float* __restrict__ residual1, float* __restrict__ closest, int vec) {
+    const int P = U * V;
+    const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (p0 >= P) return;
+    const long long view = blockIdx.y;
+    const unsigned char* D = dt + view * (long long)P;
+    const long long i0 = view * (long long)P + p0;
+    if (vec) {  // P % 4 == 0 and aligned buffers: all four pixels exist
+        const uchar4 d4 = *reinterpret_cast<const uchar4*>(D + p0);
+        float r[8], c[4];
+        const int dv[4] = {d4.x, d4.y, d4.z, d4.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) sil_pixel(view, p0 + k, dv[k], N, U, V, g, p2d, D, crops, r[2 * k], r[2 * k + 1], c[k]);
+        reinterpret_cast<float4*>(residual1 + 2 * i0)[0] = make_float4(r[0], r[1], r[2], r[3]);
+        reinterpret_cast<float4*>(residual1 + 2 * i0)[1] = make_float4(r[4], r[5], r[6], r[7]);
+        *reinterpret_cast<float4*>(closest + i0) = make_float4(c[0], c[1], c[2], c[3]);
+        return;
+    }
+    for (int k = 0; k < 4 && p0 + k < P; ++k) {
+        float r0, r1, cl;
+        sil_pixel(view, p0 + k, D[p0 + k], N, U, V, g, p2d, D, crops, r0, r1, cl);
+        residual1[2 * (i0 + k)] = r0;
+        residual1[2 * (i0 + k) + 1] = r1;
+        closest[i0 + k] = cl;
     }
 }
 
@@ -789,7 +822,8 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
                                                                        reinterpret_cast<const float2*>(p2d), cb);
     HC_CHECK_LAUNCH();
-    k_cov_tile<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(h->F, cb);
+    const long long n_keys = views * cb.T;
+    k_cov_tile<<<(unsigned)std::min<long long>(n_keys, 148 * 24), kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb);
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
                                                      h->cover.as<unsigned char>(), is_boundary);
@@ -893,10 +927,13 @@ extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_
     k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
-    k_sil_pixels<<<dim3(div_up((long long)U * V, 256), (unsigned)views), 256, 0, s>>>(batch, n_cameras, N, U, V, g,
-                                                                                      points_image_space,
-                                                  distance_transform_image, multi_view_crops, mv_dt_residual_1,
-                                                  closest_vertex_id);
+    {
+        const int vec = ((long long)U * V) % 4 == 0 && ((uintptr_t)distance_transform_image & 3) == 0 &&
+                        ((uintptr_t)mv_dt_residual_1 & 15) == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
+        k_sil_pixels<<<dim3(div_up((long long)U * V, 4 * 256), (unsigned)views), 256, 0, s>>>(
+            N, U, V, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
+            closest_vertex_id, vec);
+    }
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
@@ -1005,10 +1042,13 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
     k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
-    k_sil_pixels<<<dim3(div_up((long long)U * V, 256), (unsigned)views), 256, 0, s>>>(batch, n_cameras, N, U, V, g,
-                                                                                      points_image_space,
-                                                  distance_transform_image, multi_view_crops, mv_dt_residual_1,
-                                                  closest_vertex_id);
+    {
+        const int vec = ((long long)U * V) % 4 == 0 && ((uintptr_t)distance_transform_image & 3) == 0 &&
+                        ((uintptr_t)mv_dt_residual_1 & 15) == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
+        k_sil_pixels<<<dim3(div_up((long long)U * V, 4 * 256), (unsigned)views), 256, 0, s>>>(
+            N, U, V, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
+            closest_vertex_id, vec);
+    }
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
