@@ -419,8 +419,8 @@ struct ShadeArgs {
     // fused image L1 (NULL sums: not fused)
     const float* l1_target;
     const unsigned char* l1_mask;
-    float* l1_sum;     // [tiles]
-    unsigned* l1_cnt;  // [tiles]
+    float* l1_sum;     // [tiles * warps per tile]
+    unsigned* l1_cnt;  // [tiles * warps per tile]
 };
 
 // colour of a pixel hit by face f at barycentrics (a, bb)
@@ -741,56 +741,47 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_r
             if (A.depth_q) A.depth_q[pix] = 0x7fffffff;
             if (A.tie_count) A.tie_count[pix] = 0;
         } else {
+            // the fused L1's target, loaded before this pixel's stores (which
+            // the compiler may not move it past)
+            const bool l1m = A.l1_sum && (!A.l1_mask || A.l1_mask[pix]);
+            const float3 tg = l1m ? ld3(A.l1_target + 3 * pix) : make_float3(0.f, 0.f, 0.f);
             // recompute the winner's barycentrics (same arithmetic as the hit test)
             const TriS Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
             const TriView wv = tri_view[(long long)view * A.F + best_f];
             int dq;
             float a = 0.f, bb = 0.f;
             raster_hit(ro_s, dir, Tw, wv.num, dq, a, bb);
+            // every load of the shading before the first store of the pixel
+            const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
             A.face[pix] = best_f;
             A.bary[2 * pix + 0] = a;
             A.bary[2 * pix + 1] = bb;
-            const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
             A.render[3 * pix + 0] = col.x;
             A.render[3 * pix + 1] = col.y;
             A.render[3 * pix + 2] = col.z;
             if (A.depth_q) A.depth_q[pix] = (int)best_d;
             if (A.tie_count) A.tie_count[pix] = ties;
-            if (A.l1_sum && (!A.l1_mask || A.l1_mask[pix])) {
-                const float* t = A.l1_target + 3 * pix;
-                const float d0 = l1_diff(col.x, t[0]), d1 = l1_diff(col.y, t[1]), d2 = l1_diff(col.z, t[2]);
+            if (l1m) {
+                const float d0 = l1_diff(col.x, tg.x), d1 = l1_diff(col.y, tg.y), d2 = l1_diff(col.z, tg.z);
                 l1s = fabsf(d0) + fabsf(d1) + fabsf(d2);
                 l1c = (d0 != 0.f) + (d1 != 0.f) + (d2 != 0.f);
             }
         }
     }
-    if (A.l1_sum) {  // launch-uniform: the tile's partial L1 sum and count
-        __shared__ float s_l1s[NT / 32];
-        __shared__ unsigned s_l1c[NT / 32];
+    if (A.l1_sum) {  // launch-uniform: each warp's partial L1 sum and count
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             l1s += __shfl_xor_sync(0xffffffffu, l1s, o);
             l1c += __shfl_xor_sync(0xffffffffu, l1c, o);
         }
         if (lane == 0) {
-            s_l1s[threadIdx.x >> 5] = l1s;
-            s_l1c[threadIdx.x >> 5] = l1c;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float ts = 0.f;
-            unsigned tc = 0;
-            for (int w = 0; w < NT / 32; ++w) {
-                ts += s_l1s[w];
-                tc += s_l1c[w];
-            }
-            A.l1_sum[g] = ts;
-            A.l1_cnt[g] = tc;
+            A.l1_sum[g * (NT / 32) + (threadIdx.x >> 5)] = l1s;
+            A.l1_cnt[g * (NT / 32) + (threadIdx.x >> 5)] = l1c;
         }
     }
 }
 
-// the fused L1's tile partials summed into the L1 state (zeroed before)
+// the fused L1's warp partials summed into the L1 state (zeroed before)
 __global__ void k_l1_tiles(long long n, const float* __restrict__ sums, const unsigned* __restrict__ cnts,
                            L1State* __restrict__ state) {
     double s = 0.0;
@@ -956,13 +947,14 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     A.l1_mask = nullptr;
     A.l1_sum = nullptr;
     A.l1_cnt = nullptr;
+    const long long l1_n = tiles * (TS * TS / 32);  // warp partials of the fused L1
     if (l1) {
-        HC_TRY(ws.l1_part.ensure(8 * (size_t)tiles));
+        HC_TRY(ws.l1_part.ensure(8 * (size_t)l1_n));
         HC_CUDA(cudaMemsetAsync(l1->state, 0, sizeof(L1State), s));
         A.l1_target = l1->target;
         A.l1_mask = l1->mask;
         A.l1_sum = ws.l1_part.as<float>();
-        A.l1_cnt = reinterpret_cast<unsigned*>(A.l1_sum + tiles);
+        A.l1_cnt = reinterpret_cast<unsigned*>(A.l1_sum + l1_n);
     }
     const int* tcam = ws.tile_cam.as<int>();
     HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
@@ -990,7 +982,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     HC_CHECK_LAUNCH();
     ws.clock.end(kKResolve, s);
     if (l1) {
-        k_l1_tiles<<<148 * 2, 256, 0, s>>>(tiles, A.l1_sum, A.l1_cnt, l1->state);
+        k_l1_tiles<<<148 * 2, 256, 0, s>>>(l1_n, A.l1_sum, A.l1_cnt, l1->state);
         HC_CHECK_LAUNCH();
         if (l1->loss) {
             k_l1_loss<<<1, 1, 0, s>>>(l1->state, l1->loss);
