@@ -176,7 +176,8 @@ static void release_all(hc_renderer_s* r) {
     DevBuf* bufs[] = {&r->topo.faces, &r->topo.vf, &r->topo.vf_id, &r->topo.texcoords,
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
                       &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
-                      &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b, &r->ws.proj};
+                      &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b, &r->ws.proj,
+                      &r->ws.l1_part};
     for (DevBuf* b : bufs) b->release();
 }
 
