@@ -274,28 +274,34 @@ __device__ void cov_sweep(const CovBins& cb, int view, int tile, const CovTileTr
 // face, which is checked here exactly; every other pixel stays open for the
 // binned passes, and a tile is marked as needing them when it has an open
 // pixel.  Any hint gives the same coverage; a good one only saves work.
-__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_hint(int N, int F, const int* __restrict__ faces,
-                                                                 const float2* __restrict__ p2d,
-                                                                 const int* __restrict__ hint, CovBins cb,
-                                                                 unsigned char* __restrict__ need) {
-    const int tile = blockIdx.x, view = blockIdx.y;
+// one warp per (view, 8x8 tile), two pixels per lane
+__global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys, const int* __restrict__ faces,
+                                                  const float2* __restrict__ p2d, const int* __restrict__ hint,
+                                                  CovBins cb, unsigned char* __restrict__ need) {
+    const long long key = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (key >= n_keys) return;  // warp-uniform
+    const int view = (int)(key / cb.T), tile = (int)(key - (long long)view * cb.T);
     const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
-    const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
-    const bool valid = px < cb.W && py < cb.H;
     bool covered = true;
-    if (valid) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int q = lane + 32 * h;
+        const int px = tx * kCovTile + q % kCovTile, py = ty * kCovTile + q / kCovTile;
+        if (px >= cb.W || py >= cb.H) continue;
         const long long pix = ((long long)view * cb.H + py) * cb.W + px;
         const int f = hint[pix];
-        covered = false;
+        bool c = false;
         if (f >= 0 && f < F) {
             CoverTri t;
             cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
-            covered = px >= t.x0 && px <= t.x1 && py >= t.y0 && py <= t.y1 && cover_test(t, px + 0.5f, py + 0.5f);
+            c = px >= t.x0 && px <= t.x1 && py >= t.y0 && py <= t.y1 && cover_test(t, px + 0.5f, py + 0.5f);
         }
-        cb.cover[pix] = covered ? 1 : 0;
+        cb.cover[pix] = c ? 1 : 0;
+        covered = covered && c;
     }
-    const bool all = __syncthreads_and(covered);
-    if (threadIdx.x == 0) need[(long long)view * cb.T + tile] = all ? 0 : 1;
+    const bool all = __all_sync(0xffffffffu, covered);
+    if (lane == 0) need[key] = all ? 0 : 1;
 }
 
 // One thread per (view, triangle): its record, then its tiles.  Boxes of up
@@ -658,18 +664,36 @@ __global__ void k_sil_grad_points(long long n, const float* __restrict__ dtgrad,
     out[2 * i + 1] = dtgrad[2 * i + 1] * g[i];
 }
 
-__global__ void k_sil_grad_pixels(int B, int C, int N, int U, int V, const float* __restrict__ g1,
+// four pixels per thread on a (pixel block, view) grid: one 16-byte load of
+// closest_vertex_id when the buffer allows (vec); the rare boundary pixels
+// scatter their residual gradient to the closest vertex
+__global__ void k_sil_grad_pixels(int N, int U, int V, const float* __restrict__ g1,
                                   const float* __restrict__ closest, const float* __restrict__ crops,
-                                  float* __restrict__ out) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * C * U * V) return;
-    const int cv = (int)closest[i];
-    if (cv < 0) return;
-    const long long view = i / ((long long)U * V);
-    const float scale = crops[view * 7 + 2];
-    float* o = out + (view * N + cv) * 2;
-    atomicAdd(o, g1[2 * i] / (30.f * scale));
-    atomicAdd(o + 1, g1[2 * i + 1] / (30.f * scale));
+                                  float* __restrict__ out, int vec) {
+    const int P = U * V;
+    const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (p0 >= P) return;
+    const long long view = blockIdx.y;
+    const long long i0 = view * (long long)P + p0;
+    float cl[4];
+    if (vec) {
+        const float4 c4 = *reinterpret_cast<const float4*>(closest + i0);
+        cl[0] = c4.x;
+        cl[1] = c4.y;
+        cl[2] = c4.z;
+        cl[3] = c4.w;
+    } else {
+        for (int k = 0; k < 4; ++k) cl[k] = p0 + k < P ? closest[i0 + k] : -1.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int cv = (int)cl[k];
+        if (cv < 0) continue;
+        const float scale = crops[view * 7 + 2];
+        float* o = out + (view * N + cv) * 2;
+        atomicAdd(o, g1[2 * (i0 + k)] / (30.f * scale));
+        atomicAdd(o + 1, g1[2 * (i0 + k) + 1] / (30.f * scale));
+    }
 }
 
 }  // namespace
@@ -810,9 +834,10 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     cb.W = width;
     cb.H = height;
     if (face_hint) {  // writes every pixel of the coverage image and the per-tile flags
-        k_cov_hint<<<dim3(cb.T, (unsigned)views), kCovTile * kCovTile, 0, s>>>(
-            h->N, h->F, h->faces.as<int>(), reinterpret_cast<const float2*>(p2d), face_hint, cb,
-            h->need.as<unsigned char>());
+        const long long n_keys = views * cb.T;
+        k_cov_hint<<<div_up(n_keys * 32, 256), 256, 0, s>>>(h->N, h->F, n_keys, h->faces.as<int>(),
+                                                             reinterpret_cast<const float2*>(p2d), face_hint, cb,
+                                                             h->need.as<unsigned char>());
         HC_CHECK_LAUNCH();
         cb.need = h->need.as<unsigned char>();
     } else {
@@ -952,10 +977,12 @@ extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t
     const long long np = (long long)batch * n_cameras * n_points;
     k_sil_grad_points<<<div_up(np, 256), 256, 0, s>>>(np, dt_image_grad, mv_dt_grad, points_image_space_grad);
     HC_CHECK_LAUNCH();
-    const long long npx = (long long)batch * n_cameras * resolution_u * resolution_v;
-    k_sil_grad_pixels<<<div_up(npx, 256), 256, 0, s>>>(batch, n_cameras, n_points, resolution_u, resolution_v,
-                                                       mv_dt_grad_1, closest_vertex_id, multi_view_crops,
-                                                       points_image_space_grad);
+    const long long views = (long long)batch * n_cameras, P = (long long)resolution_u * resolution_v;
+    HC_REQUIRE(views <= 65535 && P < (1ll << 31), "too many views or pixels in one call");
+    const int vec = P % 4 == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
+    k_sil_grad_pixels<<<dim3(div_up(P, 4 * 256), (unsigned)views), 256, 0, s>>>(
+        n_points, resolution_u, resolution_v, mv_dt_grad_1, closest_vertex_id, multi_view_crops,
+        points_image_space_grad, vec);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
