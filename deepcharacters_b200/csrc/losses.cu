@@ -75,11 +75,28 @@ __global__ void k_l1_grad(long long n_px, const float* __restrict__ render, cons
     }
 }
 
-// sum of squares: acc += sum x^2 (block partials in double)
-__global__ void k_sumsq_reduce(long long n, const float* __restrict__ x, double* __restrict__ acc) {
+// one pass: grad = 2 w x and the block partials of sum x^2 (vec: 16-byte
+// loads and stores, n a multiple of 4 and both pointers 16-byte aligned)
+__global__ void k_sumsq_fused(long long n, const float* __restrict__ x, float weight, double* __restrict__ acc,
+                              float* __restrict__ grad, int vec) {
+    const float k = 2.f * weight;
     float s = 0.f;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        s += x[i] * x[i];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    if (vec) {
+        const float4* x4 = reinterpret_cast<const float4*>(x);
+        float4* g4 = reinterpret_cast<float4*>(grad);
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n / 4; i += stride) {
+            const float4 v = x4[i];
+            s += v.x * v.x + v.y * v.y + v.z * v.z + v.w * v.w;
+            g4[i] = make_float4(k * v.x, k * v.y, k * v.z, k * v.w);
+        }
+    } else {
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+            const float v = x[i];
+            s += v * v;
+            grad[i] = k * v;
+        }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     __shared__ float ss[32];
@@ -93,12 +110,8 @@ __global__ void k_sumsq_reduce(long long n, const float* __restrict__ x, double*
     }
 }
 
-__global__ void k_sumsq_grad(long long n, const float* __restrict__ x, float weight, const double* __restrict__ acc,
-                             float* __restrict__ grad, float* __restrict__ loss) {
-    if (blockIdx.x == 0 && threadIdx.x == 0 && loss) *loss = (float)(weight * *acc);
-    const float k = 2.f * weight;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        grad[i] = k * x[i];
+__global__ void k_sumsq_loss(float weight, const double* __restrict__ acc, float* __restrict__ loss) {
+    *loss = (float)(weight * *acc);
 }
 
 __global__ void k_add_inplace(long long n, float* __restrict__ dst, const float* __restrict__ src) {
@@ -215,10 +228,13 @@ extern "C" hc_status hc_sum_squares_loss(void* stream, int64_t n, const float* x
     double* acc = (double*)workspace;
     HC_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), s));
     const int blocks = 148 * 8;
-    k_sumsq_reduce<<<blocks, 256, 0, s>>>(n, x, acc);
+    const int vec = n % 4 == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)grad & 15) == 0;
+    k_sumsq_fused<<<blocks, 256, 0, s>>>(n, x, weight, acc, grad, vec);
     HC_CHECK_LAUNCH();
-    k_sumsq_grad<<<blocks, 256, 0, s>>>(n, x, weight, acc, grad, loss);
-    HC_CHECK_LAUNCH();
+    if (loss) {
+        k_sumsq_loss<<<1, 1, 0, s>>>(weight, acc, loss);
+        HC_CHECK_LAUNCH();
+    }
     return HC_OK;
 }
 
