@@ -189,7 +189,7 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
 enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2, kAlbTexBilinear = 3 };
 
 template <bool SHADED, int ALB, bool PARITY>
-__global__ void __launch_bounds__(BNT, SHADED ? 2 : 3) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles) {
+__global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles) {
     constexpr int NVV = SHADED ? 9 : 6;               // values per vertex
     constexpr int NROW = (3 * NVV + 3) / 4 * 4;       // per-lane row, padded for float4 loads
     __shared__ __align__(16) float s_red[BNT / 32][32][NROW];
