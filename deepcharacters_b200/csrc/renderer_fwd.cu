@@ -209,7 +209,7 @@ struct BinSink {
     }
 };
 
-__global__ void k_bin(int V, int C, int F, int N, int TS, int cap,
+__global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int TS, int cap,
                       const int3* __restrict__ faces, const float4* __restrict__ proj,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
@@ -557,7 +557,7 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 16 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, long long T_frame,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, long long T_frame,
                                                    const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,

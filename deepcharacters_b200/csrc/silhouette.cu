@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys
 // to 4 tiles are binned by their own thread, lanes that hit the same tile
 // sharing one counter atomic; larger boxes are taken by the whole warp, a
 // tile per lane, reading the record back from global memory.
-__global__ void k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
+__global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
                           CovBins cb) {
     // grid (triangle blocks, views): no 64-bit division per thread
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -627,7 +627,7 @@ __device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N
 // one 4-byte DT load and 16-byte stores when the buffers allow (vec), and
 // 32-bit index arithmetic.  Most pixels are not on the boundary and only
 // write their zero outputs.
-__global__ void k_sil_pixels(int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
+__global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
                              const unsigned char* __restrict__ dt, const float* __restrict__ crops,
                              float* __restrict__ residual1, float* __restrict__ closest, int vec) {
     const int P = U * V;
