@@ -20,6 +20,8 @@
 //    frame (same sum as the reference's per-pixel loops, reassociated).
 #include <algorithm>
 
+#include <cuda.h>  // CUtensorMap and its enums (the encoder is fetched through the runtime)
+
 #include "renderer.cuh"
 
 namespace hc {
@@ -61,6 +63,7 @@ struct BwdArgs {
     // target instead of read from grad (NULL state: not fused)
     const L1State* l1_state;
     const float* l1_render;          // [V,H,W,3]
+    int* err;                        // bit 2: a target copy did not complete (RasterStats::overflow)
     const unsigned char* l1_mask;    // [V,H,W] or NULL
 };
 
@@ -163,6 +166,37 @@ constexpr int MAXFS = 4;                 // image filter sizes staged in shared 
 constexpr int TILE_S = BT + 2 * MAXFS;   // staged target tile edge
 
 constexpr int MAXTAPS = (2 * MAXFS + 1) * (2 * MAXFS + 1);
+// TMA staging: one box of rows x kRawX floats of the target viewed as
+// [views][H][3W], its x start rounded down to 16 bytes
+constexpr int kRawX = (3 * TILE_S + 3 + 3) / 4 * 4;
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned mbar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(mbar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// a bounded wait: false when the phase did not complete within the limit
+__device__ __forceinline__ bool mbar_wait(unsigned mbar, unsigned parity) {
+    for (int k = 0; k < (1 << 20); ++k)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+
+// one thread: expect the box's bytes on the barrier and start the tensor copy
+__device__ __forceinline__ void tma_box(const CUtensorMap* map, unsigned dst, unsigned mbar, int x, int y, int z,
+                                        unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(dst), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(mbar)
+        : "memory");
+}
 
 // G . dTarget/d(u, v) over the staged (2 FS + 1)^2 window for a compile-time
 // filter size: the weights (i, j) / (i^2 + j^2) fold to the same correctly
@@ -189,14 +223,17 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
 enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2, kAlbTexBilinear = 3 };
 
 template <bool SHADED, int ALB, bool PARITY>
-__global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles) {
+__global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles,
+                                                                     const __grid_constant__ CUtensorMap tmap,
+                                                                     int use_tma) {
     constexpr int NVV = SHADED ? 9 : 6;               // values per vertex
     constexpr int NROW = (3 * NVV + 3) / 4 * 4;       // per-lane row, padded for float4 loads
     __shared__ __align__(16) float s_red[BNT / 32][32][NROW];
     __shared__ float s_sh[SHADED ? BNT / 32 : 1][27];
-    __shared__ float4 s_tgt2[2][TILE_S * TILE_S];      // target tile + halo, double-buffered
+    __shared__ __align__(128) float4 s_tgt2[2][TILE_S * TILE_S];  // target tile + halo, double-buffered
     __shared__ float2 s_tap[MAXTAPS];  // image-gradient tap weights (i, j) / (i^2 + j^2)
     __shared__ float s_norm;
+    __shared__ __align__(8) unsigned long long s_mbar;
     constexpr bool shaded = SHADED;
     constexpr bool vcol = ALB == kAlbVcol;
     constexpr bool textured = ALB == kAlbTex;
@@ -251,13 +288,64 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
             }
         }
     };
-    if (staged && (long long)blockIdx.x < n_tiles) stage(blockIdx.x, 0);
+    // TMA mode (all cameras of one size, rows of 16-byte multiples): one
+    // tensor copy per tile of the target box [rows][kRawX] into s_raw,
+    // completing on s_mbar, issued while the previous tile is processed and
+    // spread into the tap layout when its tile starts.
+    const bool tma = use_tma && staged;
+    // TMA mode: the tap layout lives in s_tgt2[0] and the box of the next
+    // tile in s_tgt2[1] (TILE_S x kRawX floats fit in TILE_S^2 float4)
+    static_assert(TILE_S * kRawX <= 4 * TILE_S * TILE_S, "the TMA box fits the second buffer");
+    float* const s_raw = reinterpret_cast<float*>(s_tgt2[1]);
+    const int e_st = BT + 2 * A.ifs;
+    const unsigned raw_bytes = (unsigned)(e_st * kRawX * sizeof(float));
+    auto tma_issue = [&](long long gt) {  // thread 0
+        const int sb = (int)(gt / A.Tb_frame);
+        const int sv = sb * A.C + A.tile_cam_b[gt % A.Tb_frame];
+        const ViewCam& sc = cams[sv];
+        const int st = (int)(gt - sc.tile_base_b);
+        const int x = (3 * ((st % sc.tiles_x_b) * BT - A.ifs)) & ~3;  // floats, rounded down to 16 bytes
+        const int y = (st / sc.tiles_x_b) * BT - A.ifs;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tma_box(&tmap, smem_u32(s_raw), smem_u32(&s_mbar), x, y, sv, raw_bytes);
+    };
+    if (tma) {
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && (long long)blockIdx.x < n_tiles) tma_issue(blockIdx.x);
+    } else if (staged && (long long)blockIdx.x < n_tiles) {
+        stage(blockIdx.x, 0);
+    }
     asm volatile("cp.async.commit_group;\n" ::);
     int it = 0;
     for (long long g = blockIdx.x; g < n_tiles; g += gridDim.x, ++it) {
-    const int buf = it & 1;
+    const int buf = tma ? 0 : it & 1;
     const float4* s_tgt = s_tgt2[buf];
-    if (staged && g + gridDim.x < n_tiles) stage(g + gridDim.x, buf ^ 1);
+    if (tma) {
+        // this tile's box: wait (bounded), spread it into the tap layout, then
+        // start the next tile's copy into the freed box
+        const bool ok = __syncthreads_and(mbar_wait(smem_u32(&s_mbar), (unsigned)(it & 1)));
+        if (!ok) {  // the copy did not land: flag it, give it one more bounded wait, stop
+            if (threadIdx.x == 0) atomicOr(A.err, 4);
+            mbar_wait(smem_u32(&s_mbar), (unsigned)(it & 1));
+            return;
+        }
+        const ViewCam& gc = cams[(int)(g / A.Tb_frame) * A.C + A.tile_cam_b[g % A.Tb_frame]];
+        const int cx0 = ((int)(g - gc.tile_base_b) % gc.tiles_x_b) * BT - A.ifs;
+        const int off = 3 * cx0 - ((3 * cx0) & ~3);  // floats before the first halo column in a box row
+        for (int i = threadIdx.x; i < e_st * e_st; i += BNT) {
+            const int r = i / e_st, c = i - r * e_st;
+            const float* q = s_raw + r * kRawX + off + 3 * c;
+            s_tgt2[buf][i] = make_float4(q[0], q[1], q[2], 0.f);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && g + gridDim.x < n_tiles) tma_issue(g + gridDim.x);
+    } else if (staged && g + gridDim.x < n_tiles) {
+        stage(g + gridDim.x, buf ^ 1);
+    }
     asm volatile("cp.async.commit_group;\n" ::);
     const int b = (int)(g / A.Tb_frame);
     const int view = b * A.C + A.tile_cam_b[g % A.Tb_frame];
@@ -627,6 +715,40 @@ static unsigned persistent_grid(K kernel, long long tiles) {
 
 hc_status raster_layout(RasterWorkspace& ws);
 
+// The target image [V][H][W][3] as a 3-D tensor map {3W, H, V} (floats) with a
+// box of kRawX x (16 + 2 ifs) x 1 for the adjoint's TMA staging.  False when
+// the layout does not allow it (cameras of different sizes, rows that are not
+// 16-byte multiples, an unaligned base, a filter wider than the staged tile,
+// no driver entry point): the adjoint then stages with cp.async.
+static bool target_tensor_map(const RasterWorkspace& ws, const float* target, int V, int ifs, CUtensorMap* map) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<Encode>(fn);
+        cudaGetLastError();
+    }
+    if (!encode || ifs > MAXFS || ((uintptr_t)target & 15) != 0 || ws.cam_w.empty()) return false;
+    const int W = ws.cam_w[0], H = ws.cam_h[0];
+    for (size_t c = 1; c < ws.cam_w.size(); ++c)
+        if (ws.cam_w[c] != W || ws.cam_h[c] != H) return false;
+    if (W % 4 != 0) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)3 * W, (cuuint64_t)H, (cuuint64_t)V};
+    const cuuint64_t strides[2] = {(cuuint64_t)12 * W, (cuuint64_t)12 * W * H};
+    const cuuint32_t box[3] = {(cuuint32_t)kRawX, (cuuint32_t)(BT + 2 * ifs), 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(target), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm_ws, cudaStream_t s, int B, int C,
                           int albedo, int shading, int ifs, int tfs, const float* grad,
                           const float* verts, const float* colors, const float* texture, int tex_h, int tex_w,
@@ -677,10 +799,16 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.tex_grad = tex_grad;
     A.sh_grad = sh_grad;
     A.nrm_grad = shaded ? nrm_ws.as<float>() : nullptr;
+    HC_TRY(ws.stats.ensure(sizeof(RasterStats)));
+    A.err = &ws.stats.as<RasterStats>()->overflow;
     A.l1_state = l1 ? l1->state : nullptr;
     A.l1_render = l1 ? l1->render : nullptr;
     A.l1_mask = l1 ? l1->mask : nullptr;
     const long long tiles = (long long)B * ws.Tb_frame;
+    // the target's tensor map for the TMA staging, where its layout allows it
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    const int use_tma = target_tensor_map(ws, target, V, ifs, &tmap) ? 1 : 0;
     ws.clock.begin(kKRenderGrad, s);
     const int alb = albedo == kVertexColor ? kAlbVcol
                     : albedo == kTextured ? kAlbTex
@@ -690,7 +818,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
 #define HC_GRAD_CASE(SH, AL, PA) \
     case (SH ? 8 : 0) + AL * 2 + PA:                                                                    \
         k_render_grad<SH, AL, PA><<<persistent_grid(k_render_grad<SH, AL, PA>, tiles), BNT, 0, s>>>(A, cams, \
-                                                                                              tiles);     \
+                                                                                              tiles, tmap, use_tma); \
         break;
         HC_GRAD_CASE(false, kAlbVcol, false)
         HC_GRAD_CASE(false, kAlbVcol, true)

@@ -557,7 +557,7 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 4 : 1)) k_resolve(ShadeArgs A, long long T_frame,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, long long T_frame,
                                                    const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
