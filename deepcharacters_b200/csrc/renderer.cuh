@@ -72,7 +72,8 @@ struct RasterStats {
     unsigned long long binned;
     unsigned long long spilled;
     int spill_tiles;
-    int overflow;      // bit 0: spill list full, bit 1: spill tile slots exhausted
+    int overflow;      // bit 0: spill list full, bit 1: spill tile slots exhausted,
+                       // bit 2: an adjoint target copy (TMA) did not complete
 };
 
 // Pixel-centre camera ray (reference getRayCuda2 / backprojectPixelCuda,

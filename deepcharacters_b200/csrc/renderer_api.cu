@@ -265,6 +265,8 @@ extern "C" hc_status hc_renderer_stats(hc_renderer h, void* stream, int64_t* bin
     }
     if (binned) *binned = (int64_t)st.binned;
     if (spilled) *spilled = (int64_t)st.spilled;
+    if (st.overflow & 4) HC_FAIL(HC_ERR_CUDA, "a target copy of the raster adjoint did not complete (flags %d)",
+                                 st.overflow);
     if (st.overflow) HC_FAIL(HC_ERR_OVERFLOW, "raster spill capacity exceeded (flags %d)", st.overflow);
     return HC_OK;
 }
