@@ -113,9 +113,14 @@ __device__ __forceinline__ TriS tri_from(const TriFrame& f) {
 // rounding of either side cannot break it.
 __device__ __forceinline__ int depth_lower_bound(float num, float3 n, const TriS& T, float3 o) {
     const float pd = fabsf(num) / sqrtf(dot(n, n));
-    const float d0 = length3(T.s0 - o), d1 = length3(T.s1 - o), d2 = length3(T.s2 - o);
-    const float e = fmaxf(length3(T.s1 - T.s0), fmaxf(length3(T.s2 - T.s1), length3(T.s0 - T.s2)));
-    const float vd = fminf(d0, fminf(d1, d2)) - e;
+    // the minimum / maximum taken on the squared lengths and rooted once: the
+    // correctly rounded square root is monotone, so the values are those of
+    // the per-vertex and per-edge lengths
+    const float3 a0 = T.s0 - o, a1 = T.s1 - o, a2 = T.s2 - o;
+    const float dmin = sqrtf(fminf(dot(a0, a0), fminf(dot(a1, a1), dot(a2, a2))));
+    const float3 e0 = T.s1 - T.s0, e1 = T.s2 - T.s1, e2 = T.s0 - T.s2;
+    const float e = sqrtf(fmaxf(dot(e0, e0), fmaxf(dot(e1, e1), dot(e2, e2))));
+    const float vd = dmin - e;
     const float z = fmaxf(pd, vd) * 10000.f * (1.f - 1e-4f);
     if (!(z < 2.0e9f)) return 0x7fffffff;
     return max((int)z - 2, 0);
@@ -368,6 +373,7 @@ struct RasterWorkspace {
     DevBuf cams, tri_frame, tri_view, tile_state, bins, spill, spill_keys, stats;
     DevBuf proj;  // float4 [V,N]: projected vertices of the current call
     DevBuf l1_part;  // per raster tile: float L1 sum, unsigned count (fused L1 only)
+    DevBuf claim;    // the tile resolve's tile counter
     KernelClock clock;
 };
 

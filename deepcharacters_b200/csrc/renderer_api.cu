@@ -177,7 +177,7 @@ static void release_all(hc_renderer_s* r) {
                       &r->ws.cams, &r->ws.tri_frame, &r->ws.tri_view, &r->ws.tile_state,
                       &r->ws.bins, &r->ws.spill, &r->ws.spill_keys, &r->ws.stats, &r->nrm_grad,
                       &r->uv.faces, &r->uv.table, &r->ws.layout, &r->ws.tile_cam, &r->ws.tile_cam_b, &r->ws.proj,
-                      &r->ws.l1_part};
+                      &r->ws.l1_part, &r->ws.claim};
     for (DevBuf* b : bufs) b->release();
 }
 

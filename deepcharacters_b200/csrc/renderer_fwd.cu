@@ -565,7 +565,8 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                                                    const int2* __restrict__ tile_state,
                                                    const int* __restrict__ bins,
                                                    const unsigned long long* __restrict__ spill_keys,
-                                                   int spill_tile_cap) {
+                                                   int spill_tile_cap, long long n_tiles,
+                                                   unsigned long long* __restrict__ claim) {
     constexpr int NT = TS * TS;
     constexpr int CHUNK = NT > 256 ? 256 : NT;  // triangles staged per round
     constexpr int SB = CHUNK == 64 ? 6 : 8;     // slot bits of a sort key
@@ -573,8 +574,17 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     __shared__ TileTri s_tri[CHUNK];             // staged triangles in key order
     __shared__ unsigned s_key[CHUNK];            // per warp: its keys, sorted
     __shared__ unsigned char s_rank[CHUNK];       // position of each slot in key order
-    // one CTA per tile of the call; the frame's cameras are concatenated
-    const long long g = blockIdx.x;
+    // Resident CTAs claim the tiles of the call from a counter (the frame's
+    // cameras concatenated): no launch cost per tile, and tiles of very
+    // different cost still balance.  Thread 0 claims into the slot of this
+    // round's parity; the slot is rewritten two rounds later, after every
+    // thread has passed the next round's barrier.
+    __shared__ long long s_g[2];
+    for (int it = 0;; ++it) {
+    if (threadIdx.x == 0) s_g[it & 1] = (long long)atomicAdd(claim, 1ull);
+    __syncthreads();
+    const long long g = s_g[it & 1];
+    if (g >= n_tiles) break;
     const int b = (int)(g / T_frame);
     const int view = b * A.C + tile_cam[g % T_frame];
     const ViewCam& cam = cams[view];
@@ -779,6 +789,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
             A.l1_cnt[g * (NT / 32) + (threadIdx.x >> 5)] = l1c;
         }
     }
+    }
 }
 
 // the fused L1's warp partials summed into the L1 state (zeroed before)
@@ -809,6 +820,17 @@ __global__ void k_l1_loss(const L1State* __restrict__ state, float* __restrict__
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// grid of a persistent kernel: as many CTAs as are resident at once (SMs x
+// CTAs per SM), never more than the work items
+template <typename K>
+static unsigned resident_grid(K kernel, int threads, long long items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    return (unsigned)std::max<long long>(1, std::min((long long)sms * per_sm, items));
+}
 // Per-camera layout of a frame for the current tile size: each camera's
 // resolution, tile grids and offsets, and the camera of every tile (the tile
 // resolve and the adjoint launch one CTA per tile of the whole call).
@@ -958,27 +980,25 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     }
     const int* tcam = ws.tile_cam.as<int>();
     HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
-    const unsigned grid = (unsigned)tiles;
+    HC_TRY(ws.claim.ensure(sizeof(unsigned long long)));
+    unsigned long long* claim = ws.claim.as<unsigned long long>();
+    HC_CUDA(cudaMemsetAsync(claim, 0, sizeof(unsigned long long), s));
+    const int* kbins = ws.bins.as<int>();
+    const unsigned long long* kspill = ws.spill_keys.as<unsigned long long>();
     ws.clock.begin(kKResolve, s);
+#define HC_RESOLVE_CASE(TSV)                                                                                   \
+    case TSV:                                                                                                  \
+        k_resolve<TSV><<<resident_grid(k_resolve<TSV>, TSV * TSV, tiles), TSV * TSV, 0, s>>>(                  \
+            A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill, ws.spill_tile_cap, tiles, claim); \
+        break;
     switch (TS) {
-        case 8:
-            k_resolve<8><<<grid, 64, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
-                                             ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
-                                             ws.spill_tile_cap);
-            break;
-        case 16:
-            k_resolve<16><<<grid, 256, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
-                                               ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
-                                               ws.spill_tile_cap);
-            break;
-        case 32:
-            k_resolve<32><<<grid, 1024, 0, s>>>(A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate,
-                                                ws.bins.as<int>(), ws.spill_keys.as<unsigned long long>(),
-                                                ws.spill_tile_cap);
-            break;
+        HC_RESOLVE_CASE(8)
+        HC_RESOLVE_CASE(16)
+        HC_RESOLVE_CASE(32)
         default:
             HC_FAIL(HC_ERR_INVALID, "unsupported tile size %d", TS);
     }
+#undef HC_RESOLVE_CASE
     HC_CHECK_LAUNCH();
     ws.clock.end(kKResolve, s);
     if (l1) {
