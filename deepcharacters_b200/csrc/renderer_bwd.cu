@@ -201,7 +201,8 @@ __device__ __forceinline__ void tma_box(const CUtensorMap* map, unsigned dst, un
 // G . dTarget/d(u, v) over the staged (2 FS + 1)^2 window for a compile-time
 // filter size: the weights (i, j) / (i^2 + j^2) fold to the same correctly
 // rounded constants the per-CTA table holds, and the taps are summed in the
-// same (row, column) order, so both paths give identical results.
+// same (row, column) order, leaving out only terms that are exact zeros, so
+// both paths give identical results for finite targets.
 template <int FS>
 __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, float& gu, float& gv) {
     constexpr int e = BT + 2 * FS;
@@ -209,12 +210,15 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
     for (int j = -FS; j <= FS; ++j)
 #pragma unroll
         for (int i = -FS; i <= FS; ++i) {
+            // the centre has no weight and the zero weights add exact zeros
+            // (the sums start at +0 and stay finite), so they are skipped
+            if (i == 0 && j == 0) continue;
             const float den = (float)(i * i + j * j);
-            const float wi = den == 0.f ? 0.f : (float)i / den, wj = den == 0.f ? 0.f : (float)j / den;
+            const float wi = (float)i / den, wj = (float)j / den;
             const float4 I = s_tgt[s0 + (j + FS) * e + (i + FS)];
             const float gi = G.x * I.x + G.y * I.y + G.z * I.z;
-            gu += gi * wi;
-            gv += gi * wj;
+            if (i != 0) gu += gi * wi;
+            if (j != 0) gv += gi * wj;
         }
 }
 
@@ -500,8 +504,10 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
             gbc += make_float3(dot(gnu, n0), dot(gnu, n1), dot(gnu, n2));
         }
     }
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile's copies (the next tile's stay in flight)
-    __syncthreads();
+    if (!tma) {  // (TMA mode: the tile's target was spread before its pixel work)
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile's copies (the next tile's stay in flight)
+        __syncthreads();
+    }
     if (f >= 0) {
         // model -> data: -G^T dTarget/d(u,v) d(u,v)/d(frag) d(frag)/d(v)
         float3 m = make_float3(0.f, 0.f, 0.f);
