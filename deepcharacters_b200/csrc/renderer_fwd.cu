@@ -169,7 +169,7 @@ __global__ void k_project_vertices(int V, int C, int N, const float* __restrict_
 // counter (match + ballot + popc); entries beyond the tile's capacity go to
 // the spill list.
 // ---------------------------------------------------------------------------
-constexpr int kBinSmall = 4;  // tiles a thread bins on its own
+constexpr int kBinSmall = 9;  // tiles a thread bins on its own (a 3x3 box of tiles)
 
 // Where a (tile, triangle) pair goes once it has a slot in the tile's bin:
 // the bin itself, or beyond the bin's capacity the spill list (the first

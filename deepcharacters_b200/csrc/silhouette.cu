@@ -173,6 +173,7 @@ __device__ __forceinline__ Footprint cover_footprint(const CoverTri& t, int W, i
 // OR of triangles, so any order of writes gives the same image).
 constexpr int kCovTile = 8;
 constexpr int kCovCap = 256;
+constexpr int kCovSmall = 9;  // tiles a thread bins on its own (a 3x3 box of tiles)
 
 __device__ __forceinline__ void cover_tri(int view, int f, int N, int W, int H, const int* __restrict__ faces,
                                           const float2* __restrict__ p2d, CoverTri& t) {
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys
 }
 
 // One thread per (view, triangle): its record, then its tiles.  Boxes of up
-// to 4 tiles are binned by their own thread, lanes that hit the same tile
+// to kCovSmall tiles are binned by their own thread, lanes that hit the same tile
 // sharing one counter atomic; larger boxes are taken by the whole warp, a
 // tile per lane, reading the record back from global memory.
 __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
     const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
     const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
     int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
-    if (cb.need && nt > 0 && nt <= 4) {  // a small box whose tiles are all covered already needs nothing
+    if (cb.need && nt > 0 && nt <= kCovSmall) {  // a small box whose tiles are all covered already needs nothing
         bool any = false;
         for (int k = 0; k < nt; ++k)
             any = any || cb.need[(long long)view * cb.T + (ty0 + k / ntx) * cb.tiles_x + tx0 + k % ntx];
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
         fp = cover_footprint(t, cb.W, cb.H);
         cb.rec[i] = cover_record(t, fp);
     }
-    const bool big = nt > 4;
+    const bool big = nt > kCovSmall;
     const int my_nt = big ? 0 : nt;
     int maxnt = my_nt;
 #pragma unroll
