@@ -605,8 +605,8 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     int best_f = 0x7fffffff;
     int ties = 0;
     // Each staged chunk is sorted by (back-facing, depth lower bound rounded
-    // down to a multiple of 2^SB).  All front faces are tested first, nearest
-    // bound first, then the back faces.  A triangle whose rounded bound
+    // down to a multiple of 2^SB) and staged once: its front faces are tested
+    // first, nearest bound first, then its back faces.  A triangle whose rounded bound
     // exceeds the pixel's current best depth can neither win nor tie, and
     // neither can any triangle after it in the same run (their bounds are at
     // least as large), so a pixel stops scanning a run there.  The result is
@@ -621,10 +621,10 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     // sorted keys (5-step binary searches).
     int n_front = 0;
     const int lane = threadIdx.x & 31;
-    for (int pass = 0; pass < 2; ++pass) {
-        for (int base = 0; base < n; base += CHUNK) {
+    for (int base = 0; base < n; base += CHUNK) {
+        for (int pass = 0; pass < 2; ++pass) {
             const int m = min(CHUNK, n - base);
-            if (pass == 0 || n > CHUNK) {
+            if (pass == 0) {
                 __syncthreads();  // the previous chunk's readers are done
                 bool front = false;
                 unsigned key = kNoKey;
