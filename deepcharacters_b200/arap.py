@@ -39,6 +39,12 @@ class ArapEngine:
         self._h = h
 
     @classmethod
+    def from_graph_file(cls, graph) -> "ArapEngine":
+        """From a ``loaders.GraphFile`` (graph-mesh neighbours, segmentation rigidity)."""
+        return cls(graph.eg.base_vertices, graph.eg.node_vertex, graph.n2n_offsets, graph.n2n_sizes,
+                   graph.n2n_indices, graph.rigidity, graph.max_connections)
+
+    @classmethod
     def from_graph(cls, base_vertices, node_vertex, g):
         """From a ``synthetic.NodeGraph`` (or any object with its fields)."""
         return cls(base_vertices, node_vertex, g.n2n_offsets, g.n2n_sizes, g.n2n_indices, g.rigidity,

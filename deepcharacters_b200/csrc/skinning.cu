@@ -777,12 +777,14 @@ extern "C" hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_
     std::vector<float> js(n_joints, 1.f), ss(n_skin, 1.f);
     if (joint_scale) js.assign(joint_scale, joint_scale + n_joints);
     if (skin_scale) ss.assign(skin_scale, skin_scale + n_skin);
-    // inverse rest-pose transforms of the skinning joints (zero dofs), the
-    // character's initial transformations (skinnedcharacter.cpp:130-138)
+    // inverse bind transforms of the skinning joints, the character's initial
+    // transformations (skinnedcharacter.cpp:130-138, 178-183): the bind pose has
+    // zero dofs and every joint scale set to 1 (skeleton.cpp:2840-2853); the
+    // joint scales come back afterwards (skeleton.cpp:2857-2862)
     std::vector<double> TR(9 * (size_t)n_joints), TT(3 * (size_t)n_joints);
     for (int j = 0; j < n_joints; ++j) {
         double lt[3];
-        for (int c = 0; c < 3; ++c) lt[c] = (double)offset[3 * j + c] * js[j];
+        for (int c = 0; c < 3; ++c) lt[c] = (double)offset[3 * j + c];
         const int p = parent[j];
         for (int r = 0; r < 3; ++r) {
             for (int c = 0; c < 3; ++c) TR[9 * j + 3 * r + c] = p >= 0 ? TR[9 * p + 3 * r + c] : (r == c);

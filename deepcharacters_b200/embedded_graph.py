@@ -144,18 +144,23 @@ class _EGFn(torch.autograd.Function):
 class EmbeddedGraphGpu:
     """Reference-shaped wrapper (Projects/CustomTFOperators/EmbeddedGraphGpu.py:21-76).
 
-    ``characterFilePath`` / ``graphFilePath`` are kept for signature
-    compatibility; the arrays come from ``graph_data`` (file parsing is out of
-    this package's scope)."""
+    Without ``graph_data`` or ``engine`` the graph is built from
+    ``characterFilePath`` and ``graphFilePath`` as the reference op does
+    (EmbeddedGraphGPUOp.cpp:22-60), with ``loaders.load_character`` and
+    ``loaders.load_graph``."""
 
     def __init__(self, characterFilePath="", graphFilePath="", numberOfBatches=0, deltaT=None, deltaR=None,
                  skinnedT=None, skinnedR=None, displacements=None, refinement=None, nodeName="",
                  graph_data: EGData | None = None, engine: EmbeddedGraphEngine | None = None,
                  full_skinned_gradient: bool = False):
         if engine is None:
+            if graph_data is None and characterFilePath and graphFilePath:
+                from . import loaders
+                graph_data = loaders.load_graph(loaders.load_character(characterFilePath), graphFilePath,
+                                                bool(refinement)).eg
             if graph_data is None:
                 raise ValueError("Invalid argument during the construction of the embedded graph operator! "
-                                 "(pass graph_data= the character's graph arrays)")
+                                 "(pass characterFilePath and graphFilePath, or graph_data=)")
             engine = EmbeddedGraphEngine(graph_data, full_skinned_gradient)
         if any(t is None for t in (deltaT, deltaR, skinnedT, skinnedR, displacements)):
             raise ValueError("Invalid argument during the construction of the embedded graph operator!")

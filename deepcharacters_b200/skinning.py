@@ -90,6 +90,12 @@ class SkinningEngine:
         self._h = h
         self.set_parity(parity)
 
+    @classmethod
+    def from_file(cls, character_file_path: str, parity: bool = True) -> "SkinningEngine":
+        """The op's construction from ``character_file_path_skinning`` (DQSkinningGPUOp.cpp:22-44)."""
+        from . import loaders
+        return cls(loaders.load_character(character_file_path).character(), parity)
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and _lib._lib is not None:

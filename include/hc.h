@@ -329,7 +329,8 @@ typedef struct hc_skin_s* hc_skin;
  *   dofs: CSR dof_offsets [D+1] over (dof_joint, dof_weight) entries; a dof
  *   adds weight * value to each joint's parameter (dof.cpp:9-17);
  *   skinning joints: skin_joint [S] and skin_scale [S] (NULL = 1), whose
- *   transform is joint * scale * inverse(rest joint);
+ *   transform is joint * scale * inverse(bind joint), the bind joint taken at
+ *   zero dofs with every joint scale 1 (skeleton.cpp:2840-2853);
  *   mesh: base_vertices / base_normals [N,3], skin_index [N,K] (skinning joint
  *   per weight slot).
  */

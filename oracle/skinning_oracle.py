@@ -28,12 +28,15 @@ def axis_angle(a, th):
                      [z * x * C - y * s, z * y * C + x * s, c + z * z * C]])
 
 
-def fk(ch, dofs):
-    """Joint transforms (R [B,J,3,3], t [B,J,3]), global positions and axes [B,J,3]."""
+def fk(ch, dofs, unit_scale=False):
+    """Joint transforms (R [B,J,3,3], t [B,J,3]), global positions and axes [B,J,3].
+
+    ``unit_scale``: every joint scale taken as 1, as in the bind pose
+    (Skeletool/Character/skeleton.cpp:2840-2853)."""
     dofs = np.asarray(dofs, np.float64)
     B = dofs.shape[0]
     J = ch.n_joints
-    js = np.ones(J) if ch.joint_scale is None else np.asarray(ch.joint_scale, np.float64)
+    js = np.ones(J) if ch.joint_scale is None or unit_scale else np.asarray(ch.joint_scale, np.float64)
     R = np.zeros((B, J, 3, 3))
     t = np.zeros((B, J, 3))
     gaxis = np.zeros((B, J, 3))
@@ -62,9 +65,12 @@ def fk(ch, dofs):
 
 
 def skin_transforms(ch, dofs):
-    """Per skinning joint: joint * scale * inverse(rest joint) as (R [B,S,3,3], t [B,S,3])."""
+    """Per skinning joint: joint * scale * inverse(bind joint) as (R [B,S,3,3], t [B,S,3]).
+
+    The bind transforms are taken at zero dofs with unit joint scales
+    (skinnedcharacter.cpp:178-183 after skeleton.cpp:2840-2853)."""
     R, t, _, _ = fk(ch, dofs)
-    R0, t0, _, _ = fk(ch, np.zeros((1, ch.n_dofs)))
+    R0, t0, _, _ = fk(ch, np.zeros((1, ch.n_dofs)), unit_scale=True)
     S = ch.n_skin
     ss = np.ones(S) if ch.skin_scale is None else np.asarray(ch.skin_scale, np.float64)
     B = R.shape[0]
