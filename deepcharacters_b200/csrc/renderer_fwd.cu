@@ -575,15 +575,19 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     __shared__ unsigned s_key[CHUNK];            // per warp: its keys, sorted
     __shared__ unsigned char s_rank[CHUNK];       // position of each slot in key order
     // Resident CTAs claim the tiles of the call from a counter (the frame's
-    // cameras concatenated): no launch cost per tile, and tiles of very
-    // different cost still balance.  Thread 0 claims into the slot of this
-    // round's parity; the slot is rewritten two rounds later, after every
-    // thread has passed the next round's barrier.
+    // cameras concatenated), kClaim consecutive tiles per atomic: no launch
+    // cost per tile, tiles of very different cost still balance, and the one
+    // counter sees a quarter of the atomics.  Thread 0 claims into the slot of
+    // this claim's parity; the slot is rewritten two claims later, after every
+    // thread has passed the next claim's barrier.
+    constexpr int kClaim = 4;
     __shared__ long long s_g[2];
     for (int it = 0;; ++it) {
-    if (threadIdx.x == 0) s_g[it & 1] = (long long)atomicAdd(claim, 1ull);
-    __syncthreads();
-    const long long g = s_g[it & 1];
+    if (it % kClaim == 0) {
+        if (threadIdx.x == 0) s_g[(it / kClaim) & 1] = (long long)atomicAdd(claim, (unsigned long long)kClaim);
+        __syncthreads();
+    }
+    const long long g = s_g[(it / kClaim) & 1] + it % kClaim;
     if (g >= n_tiles) break;
     const int b = (int)(g / T_frame);
     const int view = b * A.C + tile_cam[g % T_frame];

@@ -113,15 +113,29 @@ __global__ void k_fk(Skel sk, int B, const float* __restrict__ dofs, Xf* __restr
                      float* __restrict__ gaxis, Xf* __restrict__ skin_xf, float* __restrict__ params) {
     extern __shared__ float fk_sm[];
     const int b = blockIdx.x;
+    const int J4 = (sk.J + 3) & ~3, E = sk.dof_off[sk.D], E4 = (E + 3) & ~3;
     float* P = fk_sm;                                        // [J]
-    Xf* Lx = reinterpret_cast<Xf*>(fk_sm + ((sk.J + 3) & ~3));  // [J] local transforms
+    Xf* Lx = reinterpret_cast<Xf*>(fk_sm + J4);              // [J] local transforms
     Xf* T = Lx + sk.J;                                       // [J] global transforms
-    if (threadIdx.x == 0) {  // DOF -> joint parameters (dof.cpp:9-17), in dof order
-        for (int j = 0; j < sk.J; ++j) P[j] = 0.f;
-        for (int d = 0; d < sk.D; ++d) {
-            const float v = dofs[(long long)b * sk.D + d];
-            for (int e = sk.dof_off[d]; e < sk.dof_off[d + 1]; ++e) P[sk.dof_joint[e]] += sk.dof_w[e] * v;
+    int* par = reinterpret_cast<int*>(T + sk.J);             // [J] parents
+    float* prod = reinterpret_cast<float*>(par + J4);        // [E] dof weight * dof value
+    int* ent_joint = reinterpret_cast<int*>(prod + E4);      // [E] joint of each dof entry
+    // DOF -> joint parameters (dof.cpp:9-17): the products in parallel, then
+    // every joint sums its entries in dof order, the reference's order
+    for (int d = threadIdx.x; d < sk.D; d += blockDim.x) {
+        const float v = dofs[(long long)b * sk.D + d];
+        for (int e = sk.dof_off[d]; e < sk.dof_off[d + 1]; ++e) {
+            prod[e] = sk.dof_w[e] * v;
+            ent_joint[e] = sk.dof_joint[e];
         }
+    }
+    for (int j = threadIdx.x; j < sk.J; j += blockDim.x) par[j] = sk.parent[j];
+    __syncthreads();
+    for (int j = threadIdx.x; j < sk.J; j += blockDim.x) {
+        float acc = 0.f;
+        for (int e = 0; e < E; ++e)
+            if (ent_joint[e] == j) acc += prod[e];
+        P[j] = acc;
     }
     __syncthreads();
     for (int j = threadIdx.x; j < sk.J; j += blockDim.x) {
@@ -140,7 +154,7 @@ __global__ void k_fk(Skel sk, int B, const float* __restrict__ dofs, Xf* __restr
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int j = 0; j < sk.J; ++j) {
-            const int p = sk.parent[j];
+            const int p = par[j];
             if (p >= 0) xf_mul(T[p], Lx[j], T[j]);
             else T[j] = Lx[j];
         }
@@ -629,11 +643,15 @@ __device__ void pose2eg_node_grad(float4 br, float4 bt, float3 gT, float3 gE, fl
 __global__ void k_pose2eg_grad_nodes(Skel sk, int M, const int* __restrict__ node_vertex, const float* __restrict__ dq,
                                      const float* __restrict__ w, const float* __restrict__ gT,
                                      const float* __restrict__ gA, float* __restrict__ gdq) {
-    extern __shared__ float s_g[];  // [S][8]
-    const int b = blockIdx.x;
-    for (int i = threadIdx.x; i < sk.S * 8; i += blockDim.x) s_g[i] = 0.f;
+    // grid (node slices, frames); every warp accumulates into its own [S][8]
+    // copy, and the block adds the copies' sum to the frame's gradient
+    extern __shared__ float s_g[];  // [warps][S][8]
+    const int b = blockIdx.y;
+    const int SS = sk.S * 8;
+    for (int i = threadIdx.x; i < SS * (int)(blockDim.x >> 5); i += blockDim.x) s_g[i] = 0.f;
     __syncthreads();
-    for (int n = threadIdx.x; n < M; n += blockDim.x) {
+    float* s_w = s_g + SS * (threadIdx.x >> 5);
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < M; n += gridDim.x * blockDim.x) {
         const int v = node_vertex[n];
         float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bt = br, first = br;
         float sgn[16];
@@ -655,7 +673,7 @@ __global__ void k_pose2eg_grad_nodes(Skel sk, int M, const int* __restrict__ nod
         for (int k = 0; k < sk.K && k < 16; ++k) {
             const int s = sk.skin_idx[(long long)v * sk.K + k];
             const float c = w[(long long)v * sk.K + k] * sgn[k];
-            float* g = s_g + s * 8;
+            float* g = s_w + s * 8;
             atomicAdd(g + 0, c * gbr.x);
             atomicAdd(g + 1, c * gbr.y);
             atomicAdd(g + 2, c * gbr.z);
@@ -667,7 +685,11 @@ __global__ void k_pose2eg_grad_nodes(Skel sk, int M, const int* __restrict__ nod
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < sk.S * 8; i += blockDim.x) gdq[(long long)b * sk.S * 8 + i] = s_g[i];
+    for (int i = threadIdx.x; i < SS; i += blockDim.x) {
+        float acc = 0.f;
+        for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) acc += s_g[wp * SS + i];
+        atomicAdd(gdq + (long long)b * SS + i, acc);
+    }
 }
 
 // per (frame, dof): sum over the dof's joints and the skinning joints below them
@@ -716,7 +738,7 @@ __global__ void k_pose2eg_grad_dofs(Skel sk, int B, const float* __restrict__ dq
 using namespace hc;
 
 struct hc_skin_s {
-    int J = 0, D = 0, S = 0, K = 0, N = 0;
+    int J = 0, D = 0, S = 0, K = 0, N = 0, E = 0;
     int parity = 1;
     DevBuf parent, type, offset, axis, jscale, dof_off, dof_joint, dof_w, skin_joint, skin_scale, t0inv, in_chain,
         skin_idx, base_v, base_n;
@@ -808,6 +830,7 @@ extern "C" hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_
     hc_skin_s* h = new hc_skin_s();
     h->J = n_joints;
     h->D = n_dofs;
+    h->E = E;
     h->S = n_skin;
     h->K = k;
     h->N = n_vertices;
@@ -861,7 +884,8 @@ static hc_status fk(hc_skin h, cudaStream_t s, int B, const float* dofs, float* 
     HC_TRY(h->joints.ensure(sizeof(Xf) * (size_t)B * h->J));
     HC_TRY(h->params.ensure(sizeof(float) * (size_t)B * h->J));
     HC_TRY(h->skin_xf.ensure(sizeof(Xf) * (size_t)B * h->S));
-    const size_t smem = sizeof(float) * ((h->J + 3) & ~3) + 2 * sizeof(Xf) * (size_t)h->J;
+    const size_t smem = sizeof(float) * (2 * (size_t)((h->J + 3) & ~3) + 2 * (size_t)((h->E + 3) & ~3)) +
+                        2 * sizeof(Xf) * (size_t)h->J;
     HC_REQUIRE(smem <= 48 * 1024, "skeleton too large for the kinematics kernel (%d joints)", h->J);
     k_fk<<<B, 128, smem, s>>>(h->skel(), B, dofs, h->joints.as<Xf>(), gpos, gaxis, h->skin_xf.as<Xf>(),
                               h->params.as<float>());
@@ -1022,6 +1046,7 @@ extern "C" hc_status hc_pose2eg_backward(hc_skin h, void* stream, int32_t batch,
                    nodes_skinned_rotation_grad && dofs_grad,
                "NULL pointer");
     HC_REQUIRE(h->K <= 16, "node skinning gradient supports up to 16 skinning joints per vertex");
+    HC_REQUIRE(batch <= 65535, "batch %d above 65535", batch);
     cudaStream_t s = (cudaStream_t)stream;
     HC_TRY(hc_skin_reserve(h, batch));
     HC_TRY(h->dq_ws.ensure(sizeof(float) * 8 * (size_t)batch * h->S));
@@ -1030,9 +1055,11 @@ extern "C" hc_status hc_pose2eg_backward(hc_skin h, void* stream, int32_t batch,
     const int BS = batch * h->S;
     k_dq_from_xf<<<div_up(BS, 128), 128, 0, s>>>(BS, h->skin_xf.as<Xf>(), h->dq_ws.as<float>());
     HC_CHECK_LAUNCH();
-    const size_t smem = sizeof(float) * 8 * (size_t)h->S;
+    const size_t smem = sizeof(float) * 8 * (size_t)h->S * 4;  // 4 warps
     HC_REQUIRE(smem <= 48 * 1024, "too many skinning joints (%d)", h->S);
-    k_pose2eg_grad_nodes<<<batch, 256, smem, s>>>(h->skel(), n_nodes, node_vertex, h->dq_ws.as<float>(),
+    HC_CUDA(cudaMemsetAsync(h->gdq.ptr, 0, sizeof(float) * 8 * (size_t)batch * h->S, s));
+    const dim3 grid((unsigned)std::min(div_up(n_nodes, 128), 64), (unsigned)batch);
+    k_pose2eg_grad_nodes<<<grid, 128, smem, s>>>(h->skel(), n_nodes, node_vertex, h->dq_ws.as<float>(),
                                                   vertex_weights, nodes_skinned_translation_grad,
                                                   nodes_skinned_rotation_grad, h->gdq.as<float>());
     HC_CHECK_LAUNCH();
