@@ -624,30 +624,151 @@ __device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N
     }
 }
 
+// sil_pixel for a boundary pixel p (DT value 127) evaluated by a whole warp
+// (p uniform): lanes 0-24 test the 5x5 neighbourhood, and the lanes share the
+// grid cells' vertices.  Each lane keeps the sequential rule over its
+// vertices (accept dist < 30 * scale, then the smaller id on equal distance),
+// so the lane results merge into the same lexicographic minimum of
+// (distance, vertex) as the one-thread loop.
+__device__ __forceinline__ void sil_pixel_warp(long long view, int p, int N, int U, int V, const SilGrid& g,
+                                               const float* __restrict__ p2d, const unsigned char* __restrict__ D,
+                                               const float* __restrict__ crops, int lane, float& r0, float& r1,
+                                               float& cl) {
+    r0 = 0.f;
+    r1 = 0.f;
+    cl = -1.f;
+    const int vid = p / U, uid = p - vid * U;
+    bool on = false;
+    if (lane < 25) {
+        const int yy = vid + lane / 5 - 2, xx = uid + lane % 5 - 2;
+        on = yy >= 0 && yy < V && xx >= 0 && xx < U && (int)D[(long long)yy * U + xx] == 127;
+    }
+    if (__popc(__ballot_sync(0xffffffffu, on)) < 4) return;
+    const float* cr = crops + view * 7;
+    const float scale = cr[2];
+    const float2 imgpos = make_float2(((float)uid - cr[0]) * scale + cr[3], ((float)vid - cr[1]) * scale + cr[4]);
+    float bestd = 30.f * scale;
+    int best = -1;
+    int cx, cy;
+    const int cells = g.gx * g.gy;
+    if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
+        // lanes 0-8 load the 3x3 cells' ranges at once; the cells' vertices
+        // are then dealt to the lanes through an inclusive prefix of the
+        // counts, so the loads do not chain from cell to cell
+        int cs = 0, cn = 0;
+        if (lane < 9) {
+            const int yy = cy - 1 + lane / 3, xx = cx - 1 + lane % 3;
+            if (yy >= 0 && yy < g.gy && xx >= 0 && xx < g.gx) {
+                const int cell = yy * g.gx + xx;
+                cs = g.start[view * cells + cell];
+                cn = g.count[view * cells + cell];
+            }
+        }
+        int pre = cn;
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, pre, o);
+            if (lane >= o) pre += t;
+        }
+        const int total = __shfl_sync(0xffffffffu, pre, 8);  // the prefix is complete over lanes 0-15
+        for (int base = 0; base < total; base += 32) {
+            const int q = base + lane;
+            int c = 0;  // the cell holding entry q: the cells whose inclusive prefix is <= q
+#pragma unroll
+            for (int cc = 0; cc < 9; ++cc) c += __shfl_sync(0xffffffffu, pre, cc) <= q ? 1 : 0;
+            c = min(c, 8);
+            const int c_pre = __shfl_sync(0xffffffffu, pre, c), c_n = __shfl_sync(0xffffffffu, cn, c);
+            const int c_s = __shfl_sync(0xffffffffu, cs, c);
+            if (q < total) {
+                const int v = g.items[view * (long long)N + c_s + (q - (c_pre - c_n))];
+                const float* pp = p2d + (view * (long long)N + v) * 2;
+                const float2 dlt = make_float2(pp[0] - imgpos.x, pp[1] - imgpos.y);
+                const float dist = sqrtf(dlt.x * dlt.x + dlt.y * dlt.y);
+                if (dist < bestd || (dist == bestd && best >= 0 && v < best)) {
+                    bestd = dist;
+                    best = v;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float od = __shfl_xor_sync(0xffffffffu, bestd, o);
+        const int ob = __shfl_xor_sync(0xffffffffu, best, o);
+        if (ob >= 0 && (best < 0 || od < bestd || (od == bestd && ob < best))) {
+            bestd = od;
+            best = ob;
+        }
+    }
+    if (best >= 0) {
+        const float* pp = p2d + (view * (long long)N + best) * 2;
+        r0 = (pp[0] - imgpos.x) / (30.f * scale);
+        r1 = (pp[1] - imgpos.y) / (30.f * scale);
+        cl = (float)best;
+    }
+}
+
 // Four consecutive pixels per thread, grid (pixel blocks of one view, views):
 // one 4-byte DT load and 16-byte stores when the buffers allow (vec), and
 // 32-bit index arithmetic.  Most pixels are not on the boundary and only
-// write their zero outputs.
+// write their zero outputs; in the vec path the warp takes its boundary
+// pixels one at a time, all lanes together (sil_pixel_warp), instead of
+// leaving one lane to search while the others wait.
 __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
                              const unsigned char* __restrict__ dt, const float* __restrict__ crops,
                              float* __restrict__ residual1, float* __restrict__ closest, int vec) {
     const int P = U * V;
     const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (p0 >= P) return;
     const long long view = blockIdx.y;
     const unsigned char* D = dt + view * (long long)P;
     const long long i0 = view * (long long)P + p0;
-    if (vec) {  // P % 4 == 0 and aligned buffers: all four pixels exist
-        const uchar4 d4 = *reinterpret_cast<const uchar4*>(D + p0);
+    if (vec) {  // P % 4 == 0 and aligned buffers: all four pixels of an active thread exist
+        const bool active = p0 < P;  // no early exit: the warp's lanes all take part below
+        int dv[4] = {0, 0, 0, 0};
+        if (active) {
+            const uchar4 d4 = *reinterpret_cast<const uchar4*>(D + p0);
+            dv[0] = d4.x;
+            dv[1] = d4.y;
+            dv[2] = d4.z;
+            dv[3] = d4.w;
+        }
         float r[8], c[4];
-        const int dv[4] = {d4.x, d4.y, d4.z, d4.w};
+        unsigned mine = 0;  // bit k: pixel k of this lane is a boundary pixel
 #pragma unroll
-        for (int k = 0; k < 4; ++k) sil_pixel(view, p0 + k, dv[k], N, U, V, g, p2d, D, crops, r[2 * k], r[2 * k + 1], c[k]);
-        reinterpret_cast<float4*>(residual1 + 2 * i0)[0] = make_float4(r[0], r[1], r[2], r[3]);
-        reinterpret_cast<float4*>(residual1 + 2 * i0)[1] = make_float4(r[4], r[5], r[6], r[7]);
-        *reinterpret_cast<float4*>(closest + i0) = make_float4(c[0], c[1], c[2], c[3]);
+        for (int k = 0; k < 4; ++k) {
+            r[2 * k] = r[2 * k + 1] = 0.f;
+            c[k] = -1.f;
+            mine |= (dv[k] == 127 ? 1u : 0u) << k;
+        }
+        const int lane = threadIdx.x & 31;
+        unsigned any = __ballot_sync(0xffffffffu, mine != 0);
+        while (any) {
+            const int src = __ffs(any) - 1;
+            const unsigned m = __shfl_sync(0xffffffffu, mine, src);
+            const int k = __ffs(m) - 1;
+            const int p = __shfl_sync(0xffffffffu, p0, src) + k;
+            if (lane == src) mine &= mine - 1;
+            any = __ballot_sync(0xffffffffu, mine != 0);
+            float a0, a1, cl;
+            sil_pixel_warp(view, p, N, U, V, g, p2d, D, crops, lane, a0, a1, cl);
+            if (lane == src) {
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)
+                    if (kk == k) {
+                        r[2 * kk] = a0;
+                        r[2 * kk + 1] = a1;
+                        c[kk] = cl;
+                    }
+            }
+        }
+        if (active) {
+            reinterpret_cast<float4*>(residual1 + 2 * i0)[0] = make_float4(r[0], r[1], r[2], r[3]);
+            reinterpret_cast<float4*>(residual1 + 2 * i0)[1] = make_float4(r[4], r[5], r[6], r[7]);
+            *reinterpret_cast<float4*>(closest + i0) = make_float4(c[0], c[1], c[2], c[3]);
+        }
         return;
     }
+    if (p0 >= P) return;
     for (int k = 0; k < 4 && p0 + k < P; ++k) {
         float r0, r1, cl;
         sil_pixel(view, p0 + k, D[p0 + k], N, U, V, g, p2d, D, crops, r0, r1, cl);
