@@ -608,6 +608,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     unsigned best_d = 0xffffffffu;
     int best_f = 0x7fffffff;
     int ties = 0;
+    int best_e = -1;  // bin entry (base + slot) of the winner, -1 when it came from the spill
     // Each staged chunk is sorted by (back-facing, depth lower bound rounded
     // down to a multiple of 2^SB) and staged once: its front faces are tested
     // first, nearest bound first, then its back faces.  A triangle whose rounded bound
@@ -718,9 +719,13 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                     if ((unsigned)dq < best_d) {
                         best_d = (unsigned)dq;
                         best_f = f;
+                        best_e = base + slot;
                         ties = 1;
                     } else {  // equal depth (deeper hits were rejected)
-                        best_f = min(best_f, f);
+                        if (f < best_f) {
+                            best_f = f;
+                            best_e = base + slot;
+                        }
                         ++ties;
                     }
                 }
@@ -738,9 +743,11 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                 if (kd < best_d) {
                     best_d = kd;
                     best_f = kf;
+                    best_e = -1;
                     ties = 0;  // spilled ties are added by the diagnostics pass
-                } else if (kd == best_d) {
-                    best_f = min(best_f, kf);
+                } else if (kd == best_d && kf < best_f) {
+                    best_f = kf;
+                    best_e = -1;
                 }
             }
         }
@@ -760,11 +767,27 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
             const bool l1m = A.l1_sum && (!A.l1_mask || A.l1_mask[pix]);
             const float3 tg = l1m ? ld3(A.l1_target + 3 * pix) : make_float3(0.f, 0.f, 0.f);
             // recompute the winner's barycentrics (same arithmetic as the hit test)
-            const TriS Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
-            const TriView wv = tri_view[(long long)view * A.F + best_f];
+            // the winner's triangle and plane offset: from the staged chunk when
+            // the winner is in the last one staged (s_tri is rewritten only
+            // after the next tile's first barrier), else from global memory
+            const int last_base = n > 0 ? ((n - 1) / CHUNK) * CHUNK : 0;
+            TriS Tw;
+            float wnum;
+            if (best_e >= last_base) {
+                const TileTri& w = s_tri[best_e - last_base];
+                TriFrame tf;
+                tf.a = w.a;
+                tf.b = w.b;
+                tf.c = w.c;
+                Tw = tri_from(tf);
+                wnum = w.nm.x;
+            } else {
+                Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
+                wnum = tri_view[(long long)view * A.F + best_f].num;
+            }
             int dq;
             float a = 0.f, bb = 0.f;
-            raster_hit(ro_s, dir, Tw, wv.num, dq, a, bb);
+            raster_hit(ro_s, dir, Tw, wnum, dq, a, bb);
             // every load of the shading before the first store of the pixel
             const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
             A.face[pix] = best_f;
