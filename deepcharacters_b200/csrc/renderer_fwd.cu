@@ -358,9 +358,13 @@ __global__ void k_spill(int C, int F, int TS, long long T_frame, const int* __re
                         const int2* __restrict__ spill, long long spill_cap, int spill_tile_cap,
                         unsigned long long* __restrict__ spill_keys, const RasterStats* __restrict__ stats,
                         const int* __restrict__ count_depth, int* __restrict__ tie_out) {
+    // one warp per spilled (tile, triangle) entry, its lanes over the pixels
+    // of the triangle's box in the tile (the per-pixel atomic minimum does
+    // not depend on the order)
     const long long n = min((long long)stats->spilled, spill_cap);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
         const int2 it = spill[i];
         const long long g = it.x;
         const int f = it.y;
@@ -378,8 +382,11 @@ __global__ void k_spill(int C, int F, int TS, long long T_frame, const int* __re
         const int tx = tile % tiles_x, ty = tile / tiles_x;
         const int px0 = max(x0, tx * TS), px1 = min(x1, min(tx * TS + TS - 1, W - 1));
         const int py0 = max(y0, ty * TS), py1 = min(y1, min(ty * TS + TS - 1, H - 1));
-        for (int py = py0; py <= py1; ++py)
-            for (int px = px0; px <= px1; ++px) {
+        const int bw = px1 - px0 + 1, bh = py1 - py0 + 1;
+        if (bw <= 0 || bh <= 0) continue;
+        for (int q = lane; q < bw * bh; q += 32) {
+            {
+                const int px = px0 + q % bw, py = py0 + q / bw;
                 const float3 dir = pixel_ray(cam, px, py);
                 int dq;
                 float a, b;
@@ -393,6 +400,7 @@ __global__ void k_spill(int C, int F, int TS, long long T_frame, const int* __re
                     atomicMin(&spill_keys[(long long)ks * TS * TS + local], key);
                 }
             }
+        }
     }
 }
 
