@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                     t.c = tf.c;
                     key = (front ? 0u : 0x80000000u) | (coarse << SB) | threadIdx.x;
                 }
-                if (threadIdx.x < CHUNK) {  // whole warps
+                if (threadIdx.x < CHUNK && (int)(threadIdx.x & ~31u) < m) {  // whole warps that hold keys
 #pragma unroll
                     for (int size = 2; size <= 32; size <<= 1) {
 #pragma unroll
