@@ -970,7 +970,18 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
                                                                        reinterpret_cast<const float2*>(p2d), cb);
     HC_CHECK_LAUNCH();
     const long long n_keys = views * cb.T;
-    k_cov_tile<<<(unsigned)std::min<long long>(n_keys, 148 * 24), kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb);
+    {
+        // persistent: as many CTAs as are resident at once (a second partial
+        // wave would run its strided keys after everything else)
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cov_tile, kCovTile * kCovTile, 0) != cudaSuccess ||
+            per_sm <= 0)
+            per_sm = 1;
+        const long long grid = std::max<long long>(1, std::min<long long>(n_keys, (long long)sms * per_sm));
+        k_cov_tile<<<(unsigned)grid, kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb);
+    }
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
                                                      h->cover.as<unsigned char>(), is_boundary);
