@@ -4,6 +4,7 @@
 // loss = sum |difference| / count_nonzero(difference)), and its gradient
 // d loss / d R = 255 sign(difference) * mask * model_mask / count
 // (the count is a constant for the gradient, as in TF).
+#include <algorithm>
 #include <math.h>
 
 #include "hc_common.cuh"
@@ -227,7 +228,14 @@ extern "C" hc_status hc_sum_squares_loss(void* stream, int64_t n, const float* x
     cudaStream_t s = (cudaStream_t)stream;
     double* acc = (double*)workspace;
     HC_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), s));
-    const int blocks = 148 * 8;
+    // grid-stride: as many CTAs as are resident at once, so that no partial
+    // second wave runs after the rest
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sumsq_fused, 256, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    const int blocks = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm, n / 1024 + 1));
     const int vec = n % 4 == 0 && ((uintptr_t)x & 15) == 0 && ((uintptr_t)grad & 15) == 0;
     k_sumsq_fused<<<blocks, 256, 0, s>>>(n, x, weight, acc, grad, vec);
     HC_CHECK_LAUNCH();
