@@ -8,27 +8,36 @@ of a 1000-node embedded graph by a 24-joint tree (3 revolute dofs each),
 embedded-graph deformation, vertex-colour rasterization at 1024x1024 from
 cameras on a 3 m ring (fx = fy = 1200), the masked L1 image loss, camera
 projection + projected-mesh boundary + the silhouette distance-transform loss,
-and the adjoints back to node rotations / translations and vertex colours.
-Synthetic data; inputs larger than L2 (1.6 GB of target images per step).
+and the adjoints back to node rotations / translations, joint angles and
+vertex colours.  Synthetic data; inputs larger than L2 (1.6 GB of target
+images per step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--adjoint parity|exact]
 
 ours:       the chain through libhc.so, captured once in a CUDA graph and
             replayed (value: device time, inputs resident in HBM); e2e runs the
             same step through the public Python API with every step's inputs
-            copied from pinned host memory and the loss read back.
+            copied from pinned host memory and the loss read back; `unbatched`
+            runs the same kernels one view per call, eagerly, without a graph.
+            The renderer adjoint is the reference's barycentric-Jacobian
+            formula (`parity`, the mode checked against the reference kernels
+            at this shape) unless `--adjoint exact` selects the closed form.
 reference:  the reference's own CUDA kernels (compiled unmodified for sm_100a
             into oracle/_ref) driven op by op like its TF ops (the renderer
             per frame), node skinning on the host as the reference's CPU op,
             the losses as elementwise torch ops: the plain per-op path.
-Under torchrun every rank runs its own 16 frames (weak scaling); the
-gradient of the shared vertex colours is all-reduced over NCCL each step.
+With N > 1 every rank renders its own 16 frames (weak scaling; frames
+sharded by ``dist.rank_frames``) and the gradient of the shared vertex
+colours is summed over frames and ranks (NCCL all-reduce) every step.  Run
+bare with --gpus N > 1, the script starts the N ranks itself.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -45,6 +54,11 @@ from deepcharacters_b200 import dist as D  # noqa: E402
 
 METRIC = "fwd+bwd views/s at 81,920 tris 1024²: batched/graph vs plain per-view (same B200)"
 FRAMES, VIEWS, RES, SUBDIV = 16, 8, 1024, 6
+SEED = 2
+WORKLOAD = ("deform-and-render chain fwd+bwd: icosphere subdiv-6 (40,962 verts / 81,920 tris), 1000-node embedded "
+            "graph (K=4) skinned by a 24-joint tree (72 revolute dofs, node DQ), 16 frames x 8 views 1024x1024, "
+            "vertexColor raster + masked L1 + silhouette DT loss, gradients to node rotations / translations, joint "
+            "angles and vertex colours")
 
 
 def algorithmic_bytes_per_view(N, F, H, W, V):
@@ -60,53 +74,99 @@ def algorithmic_bytes_per_view(N, F, H, W, V):
 # clocks
 # --------------------------------------------------------------------------
 class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and clock-event reasons of this rank's GPU sampled every
+    20 ms during the timed region (NVML; nvidia-smi at 200 ms if NVML is
+    unavailable)."""
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
 
-    def __init__(self, index: int):
-        self.index = index
-        self.rows = []
-        self.proc = None
+    def __init__(self, cuda_index: int, period_s: float = 0.02):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []  # (sm_mhz, max_mhz, reason names, power W)
+        self.stop_evt = threading.Event()
         self.thread = None
+        self.source = None
+        self.proc = None
+
+    def _nvml_handle(self):
+        import pynvml as N
+        N.nvmlInit()
+        p = torch.cuda.get_device_properties(self.cuda_index)
+        try:
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return N, N.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _nvml_loop(self, N, h):
+        get_reasons = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        masks = [(name, getattr(N, attr, 0)) for name, attr in self.REASONS]
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        while not self.stop_evt.is_set():
+            try:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                r = get_reasons(h)
+                pw = N.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((float(sm), float(mx), [n for n, m in masks if m and (r & m)], pw))
+            except Exception:
+                pass
+            self.stop_evt.wait(self.period)
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.proc = None
+            N, h = self._nvml_handle()
+            self.source = "nvml"
+            self.thread = threading.Thread(target=self._nvml_loop, args=(N, h), daemon=True)
+            self.thread.start()
             return
-        self.thread = threading.Thread(target=self._read, daemon=True)
+        except Exception:
+            pass
+        fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                  "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.cuda_index), f"--query-gpu={fields}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return
+        self.source = "nvidia-smi"
+
+        def read():
+            names = [n for n, _ in self.REASONS[:4]]
+            for line in self.proc.stdout:
+                r = [x.strip() for x in line.split(",")]
+                try:
+                    self.samples.append((float(r[0]), float(r[1]),
+                                         [n for n, x in zip(names, r[3:7]) if x.lower().startswith("active")],
+                                         float(r[2])))
+                except (ValueError, IndexError):
+                    pass
+
+        self.thread = threading.Thread(target=read, daemon=True)
         self.thread.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
-
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
+        self.stop_evt.set()
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
         if self.thread:
             self.thread.join(timeout=2)
-        sm = [float(r[0]) for r in self.rows if len(r) >= 8 and r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for r in self.rows:
-            if len(r) < 8:
-                continue
-            for i, n in enumerate(names):
-                if r[4 + i].lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        reasons = sorted({n for _, _, rs, _ in self.samples for n in rs})
+        return {"sm_mhz": statistics.median(x[0] for x in self.samples),
+                "sm_max_mhz": max(x[1] for x in self.samples), "reasons": reasons, "samples": len(self.samples),
+                "power_w_max": max(x[3] for x in self.samples), "source": self.source}
 
 
 # --------------------------------------------------------------------------
@@ -114,6 +174,8 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 def dist_setup(gpus: int):
     world, rank, local = D.env_rank()
+    if world != gpus:
+        raise SystemExit(f"bench.py: --gpus {gpus} but WORLD_SIZE={world} ranks were launched")
     torch.cuda.set_device(local if world > 1 else 0)
     return D.init("nccl", timeout_s=120, device=torch.device("cuda", local))
 
@@ -133,9 +195,11 @@ N_NODES, N_SKEL, FX = 1000, 24, 1200.0
 W_SIL, W_SIL1 = 1e-3, 1e-3  # weights of the two silhouette residual terms
 
 
-def make_workload(rank: int):
+def make_workload(first: int, count: int):
+    """Frames first .. first+count-1 of the job's seeded sequence (one
+    character, per-frame poses / node deltas / lighting / targets)."""
     from deepcharacters_b200 import synthetic as S
-    return S.chain_scene(SUBDIV, N_NODES, N_SKEL, FRAMES, VIEWS, RES, RES, seed=2 + 100 * rank, fx=FX)
+    return S.chain_scene(SUBDIV, N_NODES, N_SKEL, count, VIEWS, RES, RES, seed=SEED, fx=FX, first_frame=first)
 
 
 def cpu_baseline(sc, frames=1, views=2):
@@ -170,16 +234,17 @@ def cpu_baseline(sc, frames=1, views=2):
     dt = time.perf_counter() - t0
     return {"value": B * C / dt, "unit": "views/s", "cores": cores, "kind": "port",
             "sample": f"{B} frame x {C} views of the same workload: node skinning + EG fwd, raster + L1 + raster "
-                      "adjoint + EG adjoint (float oracle, OpenMP; silhouette terms not in the sample)"}
+                      "adjoint + EG adjoint (float oracle built -O3 -fopenmp, OpenMP over all host threads; "
+                      "silhouette terms not in the sample)"}
 
 
 # --------------------------------------------------------------------------
 # our arm
 # --------------------------------------------------------------------------
-def stage_bytes(sc):
+def stage_bytes(sc, frames):
     """Algorithmic bytes per call of each stage (compulsory traffic of what
     the stage must read and write once)."""
-    B, C, P, N, F, M = FRAMES, VIEWS, RES * RES, sc["N"], sc["F"], sc["M"]
+    B, C, P, N, F, M = frames, VIEWS, RES * RES, sc["N"], sc["F"], sc["M"]
     K = 4
     eg = B * (12 * N * 2 + 8 * K * N + 24 * M) + 12 * N  # read base / write verts + normals, CSR, node params
     return {
@@ -195,26 +260,102 @@ def stage_bytes(sc):
     }
 
 
-def kernel_bytes(sc, covered):
-    """Algorithmic bytes per launch of the two raster kernels over FRAMES x VIEWS views
-    with the image L1 fused in (``covered`` = pixels with a face, all views):
-    k_resolve writes face 4 + barycentrics 8 + colour 12 B per pixel, reads the
-    target (12 B) of the covered pixels and each frame's positions, colours and
-    faces once; k_render_grad reads the render 12 (the image gradient is formed
-    from it), barycentrics 8, face 4 and target 12 B per pixel and each frame's
-    positions, colours and faces, and writes the position and colour gradients."""
-    V, P, N, F = FRAMES * VIEWS, RES * RES, sc["N"], sc["F"]
-    return {"resolve": V * 24 * P + 12 * covered + FRAMES * (24 * N + 12 * F),
-            "render_grad": V * 36 * P + FRAMES * (24 * N + 12 * F + 24 * N)}
+def kernel_bytes(sc, frames, covered):
+    """Algorithmic bytes per launch of the two raster kernels over frames x
+    VIEWS views with the image L1 fused in (``covered`` = pixels with a face,
+    all views).  k_resolve writes face 4 + barycentrics 8 + colour 12 B for
+    every pixel (background included: the buffers are outputs), reads the
+    target (12 B) of the covered pixels and each frame's positions, colours
+    and faces once.  k_render_grad reads the face id (4 B) of every pixel and,
+    of the covered pixels only, the render 12 (the image gradient is formed
+    from it), the barycentrics 8 and the target 12 B, plus each frame's
+    positions, colours and faces, and writes the position and colour
+    gradients."""
+    V, P, N, F = frames * VIEWS, RES * RES, sc["N"], sc["F"]
+    return {"resolve": V * 24 * P + 12 * covered + frames * (24 * N + 12 * F),
+            "render_grad": V * 4 * P + 32 * covered + frames * (24 * N + 12 * F + 24 * N)}
+
+
+def one_view_scene(sc):
+    """The scene arrays of frame 0, camera 0 (shapes of a 1-frame 1-view chain)."""
+    d = dict(sc)
+    for k in ("dofs", "dT", "dA", "disp", "colors", "texture"):
+        d[k] = sc[k][:1]
+    for k in ("sh", "target", "target_u8", "dt", "crops"):
+        d[k] = sc[k][:1, :1]
+    d["extr"], d["intr"] = sc["extr"][:1, :12], sc["intr"][:1, :9]
+    return d
+
+
+def view_inputs(inp, f, c):
+    """Views into a batched chain's input tensors: frame f, camera c."""
+    o = {k: inp[k][f:f + 1] for k in ("dofs", "dT", "dA", "disp", "colors", "texture")}
+    o.update({k: inp[k][f:f + 1, c:c + 1] for k in ("sh", "target", "dt", "crops")})
+    o["extr"], o["intr"] = inp["extr"][f:f + 1, 12 * c:12 * c + 12], inp["intr"][f:f + 1, 9 * c:9 * c + 9]
+    return o
+
+
+def run_unbatched(ch, sc, dev, frames, parity, steps):
+    """The same kernels without batching or graph capture: one chain call
+    per (frame, view), eager (node skinning, EG, raster + L1, silhouette and
+    all adjoints per view), the raster tiling of the batched chain."""
+    from deepcharacters_b200.chain import DeformRenderChain
+    one = DeformRenderChain(one_view_scene(sc), dev, 1, 1, RES, RES, W_SIL, W_SIL1, tile=ch.tuning[0],
+                            bin_capacity=ch.tuning[1], gradient_parity=parity)
+    pairs = [(f, c) for f in range(frames) for c in range(VIEWS)]
+
+    def step():
+        for f, c in pairs:
+            one.inp.update(view_inputs(ch.inp, f, c))
+            one.step()
+
+    step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    return {"value": len(pairs) / (ms / 1e3), "unit": "views/s", "ms_per_step": ms, "steps": steps,
+            "how": "the same libhc kernels issued one view per call (a 1-frame, 1-camera DeformRenderChain stepped "
+                   "eagerly over every (frame, view) of the step: node skinning, EG, raster + L1, silhouette and "
+                   "all adjoints per view), no CUDA graph; device time (CUDA events)"}
+
+
+def parity_record(adjoint):
+    """The committed record of tests/test_chain_c2_gpu.py (the chain at this
+    per-frame shape, 1 frame x 4 views, against the reference kernels and the
+    FP64 oracle), quoted for the adjoint mode this run times."""
+    path = os.path.join(ROOT, "profiles", "parity_c2.json")
+    if not os.path.exists(path):
+        return {"adjoint": adjoint, "record": None}
+    rec = json.load(open(path))
+    out = {"adjoint": adjoint, "record": "profiles/parity_c2.json (tests/test_chain_c2_gpu.py on a B200)"}
+    ref = rec.get("parity_mode_vs_reference_kernels", {})
+    f64 = rec.get("adjoints_vs_fp64", {})
+    if adjoint == "parity":
+        out["vs_reference_kernels"] = {k: ref[k] for k in ("loss", "gv", "gcol", "gT", "gA", "gv_sil",
+                                                           "face_mismatch_outside_ties", "tie_pixels") if k in ref}
+    mode = f64.get(adjoint, {})
+    out["vs_fp64"] = {px: {k: v for k, v in mode.get(px, {}).items()}
+                      for px in ("all_pixels", "well_conditioned_pixels") if px in mode}
+    if "joint_angles_vs_fp64_central_differences" in f64:
+        out["vs_fp64"]["joint_angles_central_differences"] = f64["joint_angles_vs_fp64_central_differences"]
+    return out
 
 
 def run_ours(args, world, rank, local):
     from deepcharacters_b200 import _lib
     dev = torch.device("cuda", local)
     from deepcharacters_b200.chain import DeformRenderChain
-    sc = make_workload(rank)
-    ch = DeformRenderChain(sc, dev, FRAMES, VIEWS, RES, RES, W_SIL, W_SIL1)
-    views_per_step = FRAMES * VIEWS
+    first, frames = D.rank_frames(FRAMES, world, rank)
+    sc = make_workload(first, frames)
+    parity = args.adjoint == "parity"
+    ch = DeformRenderChain(sc, dev, frames, VIEWS, RES, RES, W_SIL, W_SIL1, gradient_parity=parity)
+    views_per_step = frames * VIEWS
+    gcol_shared = torch.zeros((sc["N"], 3), device=dev)
     # autotuner: raster tile size and bin capacity (untimed)
     tune = ch.autotune() if not args.no_autotune else {}
     binned, spilled = ch.check()  # raises if the raster's spill capacity overflowed
@@ -227,12 +368,12 @@ def run_ours(args, world, rank, local):
     launches_per_step = _lib.lib().hc_kernel_launches() - l0
     torch.cuda.synchronize()
 
-    def allreduce():  # the shared vertex-colour gradient; frames are sharded
-        D.allreduce_shared([ch.buf["gcol"]], world)
+    def reduce_shared():  # the vertex colours are one parameter of every frame and rank
+        D.shared_gradient(ch.buf["gcol"], gcol_shared, world)
 
     for _ in range(args.warmup):
         g.replay()
-        allreduce()
+        reduce_shared()
     torch.cuda.synchronize()
     barrier(world)
     clk = ClockSampler(local)
@@ -242,7 +383,7 @@ def run_ours(args, world, rank, local):
     st.record()
     for _ in range(args.steps):
         g.replay()
-        allreduce()
+        reduce_shared()
     en.record()
     torch.cuda.synchronize()
     clocks = clk.stop()
@@ -262,7 +403,7 @@ def run_ours(args, world, rank, local):
         b.record()
         torch.cuda.synchronize()
         stage_ms[name] = a.elapsed_time(b) / 3
-    sbytes = stage_bytes(sc)
+    sbytes = stage_bytes(sc, frames)
     N, F = sc["N"], sc["F"]
     # per-kernel device time of the two raster kernels (events around each launch, eager)
     ch.rend.set_kernel_timing(True)
@@ -275,7 +416,8 @@ def run_ours(args, world, rank, local):
             kern_ms.setdefault(k, []).append(kt[k])
     ch.rend.set_kernel_timing(False)
     kern_ms = {k: sum(v) / len(v) for k, v in kern_ms.items()}
-    kbytes = kernel_bytes(sc, int((ch.buf["face"] >= 0).sum()))
+    covered = int((ch.buf["face"] >= 0).sum())
+    kbytes = kernel_bytes(sc, frames, covered)
     dom = max(kern_ms, key=kern_ms.get)
     peaks = {}
     try:
@@ -289,10 +431,16 @@ def run_ours(args, world, rank, local):
     if os.path.exists(traffic_path):
         tj = json.load(open(traffic_path)).get("k_" + dom)
         if tj:  # ncu DRAM bytes per view of a smaller capture, scaled to this launch's views
-            traffic = tj["dram_bytes_per_view"] * FRAMES * VIEWS
+            traffic = tj["dram_bytes_per_view"] * frames * VIEWS
+    # issue-rate view of the tile resolve: pixels resolved and bin entries
+    # scanned per second (its ceiling is the SMs' instruction issue, not HBM)
+    issue = {"resolve_pixels_per_s": frames * VIEWS * RES * RES / (kern_ms["resolve"] / 1e3),
+             "resolve_bin_entries_per_s": binned / (kern_ms["resolve"] / 1e3),
+             "bin_entries_per_covered_pixel": binned / max(covered, 1)}
 
+    unbatched = None if args.no_unbatched or world > 1 else run_unbatched(ch, sc, dev, frames, parity, 2)
     # e2e: public API, pinned host inputs copied every step, losses read back
-    e2e = None if args.no_e2e else run_e2e(ch, sc, dev, args, world)
+    e2e = None if args.no_e2e else run_e2e(ch, sc, dev, args, world, reduce_shared)
 
     line = {
         "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
@@ -300,23 +448,24 @@ def run_ours(args, world, rank, local):
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded icosphere character, random pose / node deltas, ring cameras, random targets, "
                 "ellipse silhouettes)",
-        "config": {"workload": "deform-and-render chain fwd+bwd: icosphere subdiv-6 (40,962 verts / 81,920 tris), "
-                               "1000-node embedded graph (K=4) skinned by a 24-joint tree (node DQ), 16 frames x 8 "
-                               "views 1024x1024, vertexColor raster + masked L1 + silhouette DT loss, gradients to "
-                               "node rotations / translations and vertex colours, one CUDA graph per step",
+        "config": {"workload": WORKLOAD + ", one CUDA graph per step",
                    "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES], "triangles": F, "vertices": N,
-                   "nodes": N_NODES, "joints": 3 * N_SKEL,
-                   "parallelism": f"frames sharded, {world} rank(s)",
+                   "nodes": N_NODES, "joints": 3 * N_SKEL, "adjoint": args.adjoint,
+                   "parallelism": f"frames sharded (dist.rank_frames), {world} rank(s), {FRAMES} frames per rank",
                    "l2": "inputs larger than L2 (1.6 GB of target images per step)",
                    "raster_tile": ch.tuning[0], "bin_capacity": ch.tuning[1],
                    "autotune_ms": {f"{t}x{c}": round(v, 3) for (t, c), v in tune.items()},
                    "bin_pairs": binned, "spilled_pairs": spilled},
         "e2e": e2e,
+        "unbatched": unbatched,
+        "parity": parity_record(args.adjoint),
         "gpu_launches": int(launches_per_step * args.steps),
         "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "traffic": traffic,
-                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6650",
-                     "kernel_ms": kern_ms, "kernel_bytes": kbytes,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                     else "fallback 6650",
+                     "kernel_ms": kern_ms, "kernel_bytes": kbytes, "covered_pixels": covered,
+                     "issue": issue,
                      "stage_ms": stage_ms, "stage_bytes": sbytes,
                      "chain_bytes_per_view": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS),
                      "chain_frac": algorithmic_bytes_per_view(N, F, RES, RES, VIEWS) * value / world / 1e9 / peak},
@@ -331,7 +480,7 @@ def run_ours(args, world, rank, local):
 E2E_KEYS = ("dofs", "dT", "dA", "colors", "sh", "extr", "intr", "target_u8", "dt")
 
 
-def run_e2e(ch, sc, dev, args, world):
+def run_e2e(ch, sc, dev, args, world, reduce_shared):
     """Same step through the C ABI with host inputs: per step H2D of the pose,
     node deltas, vertex colours, cameras, SH, the 8-bit target images
     (widened to float32 on the device by ``hc_image_u8_to_f32``, the same
@@ -377,7 +526,7 @@ def run_e2e(ch, sc, dev, args, world):
             if i + 1 < n:
                 upload((i + 1) % 2)
             graphs[slot].replay()
-            D.allreduce_shared([ch.buf["gcol"]], world)
+            reduce_shared()
             done[slot].record()
             loss_host.copy_(ch.loss, non_blocking=True)
         torch.cuda.synchronize()
@@ -389,7 +538,7 @@ def run_e2e(ch, sc, dev, args, world):
     run(args.steps)
     dt = max_over_ranks(time.perf_counter() - t0, world)
     ch.inp.update(saved)
-    return {"value": FRAMES * VIEWS * world * args.steps / dt, "unit": "views/s", "h2d_bytes_per_step": h2d,
+    return {"value": ch.B * VIEWS * world * args.steps / dt, "unit": "views/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": 12, "ms_per_step": dt / args.steps * 1e3,
             "path": "DeformRenderChain.capture_step graphs (one per input slot) replayed per step, inputs copied "
                     "from pinned host memory on a copy stream (double buffer), target images as 8-bit RGB widened "
@@ -408,7 +557,7 @@ def run_reference(args, world, rank, local):
         return
     from oracle.chain_ref import RefChain
     dev = torch.device("cuda", local)
-    sc = make_workload(0)
+    sc = make_workload(0, FRAMES)
     ref = RefChain(sc, dev, FRAMES, VIEWS, RES, RES, W_SIL, W_SIL1)
 
     def step():
@@ -430,11 +579,7 @@ def run_reference(args, world, rank, local):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "views/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "deform-and-render chain fwd+bwd: icosphere subdiv-6 (40,962 verts / 81,920 tris), "
-                               "1000-node embedded graph (K=4) skinned by a 24-joint tree (node DQ), 16 frames x 8 "
-                               "views 1024x1024, vertexColor raster + masked L1 + silhouette DT loss, gradients to "
-                               "node rotations / translations and vertex colours",
-                   "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES]},
+        "config": {"workload": WORKLOAD, "frames": FRAMES, "views": VIEWS, "resolution": [RES, RES]},
         "cpu_baseline": {"value": value, "unit": "views/s", "kind": "reference", "cores": 1,
                          "sample": "full step; the reference's own CUDA kernels (renderer, EG, camera projection, "
                                    "mesh boundary, silhouette loss; unmodified, sm_100a) launched per op like its TF "
@@ -446,19 +591,29 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def main():
+def parse_args(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 150 for ours, about 3 s; 10 for the reference arm)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--adjoint", choices=("parity", "exact"), default="parity",
+                    help="renderer adjoint: the reference's barycentric-Jacobian formula (parity) or the closed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-unbatched", action="store_true", help="skip the un-batched, no-graph leg")
     ap.add_argument("--frames", type=int, default=FRAMES, help="frames per rank (default 16; smaller for profiling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default raster tiling (8 px, 256)")
-    args = ap.parse_args()
-    globals()["FRAMES"] = args.frames
+    args = ap.parse_args(argv)
+    if args.steps is None:
+        args.steps = 150 if args.impl == "ours" else 10
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else max(args.warmup, 1)
+    return args
+
+
+def run(args):
+    globals()["FRAMES"] = args.frames
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
@@ -467,6 +622,32 @@ def main():
             run_ours(args, world, rank, local)
     finally:
         D.finalize(world)
+
+
+def _spawned_rank(rank, world, port, argv):
+    os.environ.update(RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE=str(world), LOCAL_WORLD_SIZE=str(world),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    run(parse_args(argv))
+
+
+def main():
+    args = parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # started bare: one process per GPU, rendezvous on 127.0.0.1
+        import torch.multiprocessing as mp
+        if torch.cuda.device_count() < args.gpus:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but {torch.cuda.device_count()} GPUs are visible")
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        ctx = mp.get_context("spawn")
+        procs = [ctx.Process(target=_spawned_rank, args=(r, args.gpus, port, sys.argv[1:])) for r in range(args.gpus)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join()
+        sys.exit(max(abs(p.exitcode or 0) for p in procs))
+    run(args)
 
 
 if __name__ == "__main__":

@@ -1043,30 +1043,41 @@ extern "C" hc_status hc_silhouette_reserve(hc_silhouette h, int32_t batch, int32
     return HC_OK;
 }
 
-extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
-                                           int32_t n_points, int32_t resolution_u, int32_t resolution_v,
-                                           const float* points_image_space, const float* normals_image_space,
-                                           const uint8_t* is_boundary, const uint8_t* distance_transform_image,
-                                           const float* multi_view_crops, float* mv_dt_residual,
-                                           float* mv_dt_residual_1, float* dt_image_gradient,
-                                           float* closest_vertex_id) {
-    clear_error();
-    HC_REQUIRE(h, "invalid handle");
+namespace {
+
+// Argument checks shared by both silhouette forward entry points; sets the
+// boundary-vertex grid's cells per view and the scratch bytes the call needs.
+hc_status sil_forward_plan(int32_t batch, int32_t n_cameras, int32_t n_points, int32_t resolution_u,
+                           int32_t resolution_v, const float* points_image_space, const float* normals_image_space,
+                           const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                           const float* multi_view_crops, const float* mv_dt_residual, const float* mv_dt_residual_1,
+                           const float* dt_image_gradient, const float* closest_vertex_id, SilGrid& g,
+                           size_t& need) {
     HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 2 && resolution_v > 2, "bad sizes");
     HC_REQUIRE(points_image_space && normals_image_space && is_boundary && distance_transform_image &&
                    multi_view_crops && mv_dt_residual && mv_dt_residual_1 && dt_image_gradient && closest_vertex_id,
                "NULL pointer");
-    cudaStream_t s = (cudaStream_t)stream;
+    const long long views = (long long)batch * n_cameras;
+    HC_REQUIRE(views <= 65535 && (long long)resolution_u * resolution_v < (1ll << 31),
+               "too many views or pixels in one call");
+    g.gx = div_up(resolution_u, 30) + 3;
+    g.gy = div_up(resolution_v, 30) + 3;
+    need = grid_bytes(views, g.gx, g.gy, n_points);
+    return HC_OK;
+}
+
+// The launches of one silhouette forward, the grid laid out in the scratch at
+// `base` (at least the planned bytes).  The cell counts are cleared first:
+// the scratch may hold a previous call's grid.
+hc_status sil_forward_run(cudaStream_t s, int* base, SilGrid g, int32_t batch, int32_t n_cameras, int32_t n_points,
+                          int32_t resolution_u, int32_t resolution_v, const float* points_image_space,
+                          const float* normals_image_space, const uint8_t* is_boundary,
+                          const uint8_t* distance_transform_image, const float* multi_view_crops,
+                          float* mv_dt_residual, float* mv_dt_residual_1, float* dt_image_gradient,
+                          float* closest_vertex_id) {
     const int U = resolution_u, V = resolution_v, N = n_points;
     const long long views = (long long)batch * n_cameras;
-    HC_REQUIRE(views <= 65535 && (long long)U * V < (1ll << 31), "too many views or pixels in one call");
-    SilGrid g;
-    g.gx = div_up(U, 30) + 3;
-    g.gy = div_up(V, 30) + 3;
-    HC_REQUIRE(g.gx * g.gy <= 1024 * 64, "distance image too large for the boundary grid");
-    HC_TRY(h->grid.ensure(grid_bytes(views, g.gx, g.gy, N)));
     const long long cells = views * g.gx * g.gy;
-    int* base = h->grid.as<int>();
     g.count = base;
     g.start = base + cells;
     g.cursor = base + 2 * cells + 1;
@@ -1094,6 +1105,29 @@ extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_
     }
     HC_CHECK_LAUNCH();
     return HC_OK;
+}
+
+}  // namespace
+
+extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
+                                           int32_t n_points, int32_t resolution_u, int32_t resolution_v,
+                                           const float* points_image_space, const float* normals_image_space,
+                                           const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                           const float* multi_view_crops, float* mv_dt_residual,
+                                           float* mv_dt_residual_1, float* dt_image_gradient,
+                                           float* closest_vertex_id) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    SilGrid g;
+    size_t need = 0;
+    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, resolution_u, resolution_v, points_image_space,
+                            normals_image_space, is_boundary, distance_transform_image, multi_view_crops,
+                            mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id, g, need));
+    HC_TRY(h->grid.ensure(need));
+    return sil_forward_run((cudaStream_t)stream, h->grid.as<int>(), g, batch, n_cameras, n_points, resolution_u,
+                           resolution_v, points_image_space, normals_image_space, is_boundary,
+                           distance_transform_image, multi_view_crops, mv_dt_residual, mv_dt_residual_1,
+                           dt_image_gradient, closest_vertex_id);
 }
 
 extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
@@ -1164,51 +1198,21 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
                                                   float* mv_dt_residual_1, float* dt_image_gradient,
                                                   float* closest_vertex_id) {
     clear_error();
-    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 2 && resolution_v > 2, "bad sizes");
-    HC_REQUIRE(points_image_space && normals_image_space && is_boundary && distance_transform_image &&
-                   multi_view_crops && mv_dt_residual && mv_dt_residual_1 && dt_image_gradient && closest_vertex_id,
-               "NULL pointer");
-    const int U = resolution_u, V = resolution_v, N = n_points;
-    const long long views = (long long)batch * n_cameras;
-    HC_REQUIRE(views <= 65535 && (long long)U * V < (1ll << 31), "too many views or pixels in one call");
     SilGrid g;
-    g.gx = div_up(U, 30) + 3;
-    g.gy = div_up(V, 30) + 3;
-    const size_t need = grid_bytes(views, g.gx, g.gy, N);
+    size_t need = 0;
+    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, resolution_u, resolution_v, points_image_space,
+                            normals_image_space, is_boundary, distance_transform_image, multi_view_crops,
+                            mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id, g, need));
     HC_REQUIRE(need <= kSilStaticBytes,
                "hc_silhouette_forward_static: %lld views x %d points at %dx%d need %zu bytes of grid scratch; the "
                "static scratch holds %zu bytes (use hc_silhouette_forward)",
-               views, N, U, V, need, kSilStaticBytes);
+               (long long)batch * n_cameras, n_points, resolution_u, resolution_v, need, kSilStaticBytes);
     int* base = nullptr;
     HC_TRY(sil_static_base(&base));
-    cudaStream_t s = (cudaStream_t)stream;
-    const long long cells = views * g.gx * g.gy;
-    g.count = base;
-    g.start = base + cells;
-    g.cursor = base + 2 * cells + 1;
-    g.items = base + 3 * cells + 1;
-    // the array keeps the previous call's contents; the cell counts must start at zero
-    HC_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)cells, s));
-    const long long np = views * N;
-    k_sil_points<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, points_image_space, normals_image_space,
-                                                 is_boundary, distance_transform_image, multi_view_crops,
-                                                 mv_dt_residual, dt_image_gradient);
-    HC_CHECK_LAUNCH();
-    k_grid_count<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
-                                                 multi_view_crops);
-    HC_CHECK_LAUNCH();
-    k_grid_scan<<<(unsigned)views, 1024, 0, s>>>(g);
-    HC_CHECK_LAUNCH();
-    k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
-                                                multi_view_crops);
-    HC_CHECK_LAUNCH();
-    {
-        const int vec = ((long long)U * V) % 4 == 0 && ((uintptr_t)distance_transform_image & 3) == 0 &&
-                        ((uintptr_t)mv_dt_residual_1 & 15) == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
-        k_sil_pixels<<<dim3(div_up((long long)U * V, 4 * 256), (unsigned)views), 256, 0, s>>>(
-            N, U, V, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
-            closest_vertex_id, vec);
-    }
-    HC_CHECK_LAUNCH();
-    return HC_OK;
+    // the array keeps the previous call's contents: sil_forward_run clears the
+    // cell counts before the grid is built
+    return sil_forward_run((cudaStream_t)stream, base, g, batch, n_cameras, n_points, resolution_u, resolution_v,
+                           points_image_space, normals_image_space, is_boundary, distance_transform_image,
+                           multi_view_crops, mv_dt_residual, mv_dt_residual_1, dt_image_gradient,
+                           closest_vertex_id);
 }

@@ -49,6 +49,22 @@ def allreduce_shared(tensors, world: int) -> None:
             dist.all_reduce(t, op=dist.ReduceOp.SUM)
 
 
+def shared_gradient(per_frame: torch.Tensor, out: torch.Tensor, world: int) -> torch.Tensor:
+    """Gradient of a parameter that every frame shares (the vertex colours
+    [N,3] of the character): the chain writes one gradient per frame slot
+    [B,...]; the parameter's gradient is their sum over this rank's frames,
+    then over the ranks (one all-reduce).  ``out`` [...] receives it."""
+    torch.sum(per_frame, dim=0, out=out)
+    allreduce_shared([out], world)
+    return out
+
+
+def rank_frames(total_per_rank: int, world: int, rank: int) -> tuple[int, int]:
+    """Weak scaling: the job has ``total_per_rank * world`` frames, rank r
+    renders the contiguous block ``shard_frames`` gives it."""
+    return shard_frames(total_per_rank * world, world, rank)
+
+
 def max_over_ranks(x: float, world: int, device: torch.device | str = "cpu") -> float:
     """The largest value of x over the ranks (step times are reported this way)."""
     if world == 1:

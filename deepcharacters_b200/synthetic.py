@@ -34,6 +34,13 @@ def rng_for(seed: int, sub: int | None = None) -> np.random.Generator:
     return np.random.Generator(np.random.PCG64(s))
 
 
+def frame_rng(seed: int, frame: int) -> np.random.Generator:
+    """Stream of one frame's per-frame inputs (node deltas, colours, lighting,
+    targets): a frame's data depends only on (seed, frame), so the frames a
+    data-parallel rank generates for itself equal its slice of the whole job."""
+    return np.random.Generator(np.random.PCG64(np.random.SeedSequence([int(seed), 1 + int(frame)])))
+
+
 # ----------------------------------------------------------------------------
 # meshes
 # ----------------------------------------------------------------------------
@@ -529,16 +536,23 @@ def identity_crops(batch: int, views: int, width: int, height: int) -> np.ndarra
 
 def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int, width: int, height: int, seed: int,
                 fx: float | None = None, ring_radius: float = 3.0 * MM, k: int = 4, pose_amplitude: float = 0.5,
-                delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, n_masks: int | None = None) -> dict:
+                delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, n_masks: int | None = None,
+                first_frame: int = 0) -> dict:
     """Inputs of the whole deform-and-render chain on one character: a
     jittered icosphere with an embedded graph (``n_nodes`` farthest-point
     nodes, K nearest nodes per vertex) and a random ``n_skel``-joint tree with
     K-nearest-joint skinning weights; per frame an independent pose (joint
     angles U(-a, a)) and node deltas (Euler N(0, 0.05) rad, translation
-    N(0, 10) mm); 8 markers on random nodes; cameras on a ring; vertex colours U[0,1]; 8-bit target
+    N(0, 10) mm); 8 markers on random nodes; cameras on a ring; vertex colours U[0,1] (one set for
+    all frames: the character's appearance); 8-bit target
     images (``target_u8`` uniform bytes, ``target`` = byte / 255 in float32, the value
     ``hc_image_u8_to_f32`` computes on the device); silhouette distance-transform images of
-    seeded random ellipses (``n_masks`` distinct ones, default one per view, reused across frames)."""
+    seeded random ellipses (``n_masks`` distinct ones, default one per view, reused across frames).
+
+    ``frames`` frames starting at frame ``first_frame`` of the seed's
+    sequence: the character, cameras and masks depend on the seed alone and
+    every per-frame input on (seed, frame), so ``chain_scene(..., frames=n,
+    first_frame=f)`` equals frames f .. f+n-1 of a longer scene."""
     rng = rng_for(seed)
     verts, faces = sphere_mesh(subdiv, rng)
     N = verts.shape[0]
@@ -547,24 +561,36 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
     markers = (verts[graph.node_vertex[mk_nodes]] + rng.normal(0, 5.0, (8, 3))).astype(np.float32)
     sk = random_skeleton(n_skel, rng)
     skin_idx, skin_w = skinning_weights(verts, sk, k, rng)
-    dofs = np.stack([random_pose(sk, rng_for(seed, b), pose_amplitude) for b in range(frames)])
-    f = lambda std, shape: rng.normal(0.0, std, size=shape).astype(np.float32)  # noqa: E731
+    fr = range(first_frame, first_frame + frames)
+    dofs = np.stack([random_pose(sk, rng_for(seed, b), pose_amplitude) for b in fr])
     if fx is None:
         fx = 600.0 * min(width, height) / 512.0
     ex, it = camera_ring(views, ring_radius, fx, width, height)
     nm = views if n_masks is None else n_masks
     masks = silhouette_masks(1, nm, width, height, seed=seed, scale=min(width, height) / 512.0)[0]
     dt = np.stack([masks[np.arange(views) % nm]] * frames)
-    target_u8 = rng.integers(0, 256, size=(frames, views, height, width, 3), dtype=np.uint8)
+    # the appearance is shared by all frames (one parameter, its gradient
+    # summed over frames and ranks); pose, node deltas, lighting and targets
+    # are per frame
+    colors = rng.uniform(0.0, 1.0, size=(N, 3)).astype(np.float32)
+    texture = rng.uniform(0.0, 1.0, size=(16, 16, 3)).astype(np.float32)
+    per = {key: [] for key in ("dT", "dA", "sh", "target_u8")}
+    for b in fr:
+        r = frame_rng(seed, b)
+        per["dT"].append(r.normal(0.0, delta_t_std, size=(n_nodes, 3)).astype(np.float32))
+        per["dA"].append(r.normal(0.0, delta_rot_std, size=(n_nodes, 3)).astype(np.float32))
+        per["sh"].append(sh_coefficients(views, r))
+        per["target_u8"].append(r.integers(0, 256, size=(views, height, width, 3), dtype=np.uint8))
+    per = {key: np.stack(v) for key, v in per.items()}
+    target_u8 = per["target_u8"]
     return dict(verts=verts, faces=faces, graph=graph, markers=markers, marker_node=mk_nodes, skeleton=sk,
                 skin_index=skin_idx, skin_weights=skin_w,
-                dofs=dofs, dT=f(delta_t_std, (frames, n_nodes, 3)), dA=f(delta_rot_std, (frames, n_nodes, 3)),
+                dofs=dofs, dT=per["dT"], dA=per["dA"],
                 disp=np.zeros((frames, N, 3), np.float32),
-                colors=rng.uniform(0.0, 1.0, size=(frames, N, 3)).astype(np.float32),
-                texture=rng.uniform(0.0, 1.0, size=(frames, 16, 16, 3)).astype(np.float32),
-                sh=sh_coefficients(frames * views, rng).reshape(frames, views, 27),
+                colors=np.tile(colors[None], (frames, 1, 1)), texture=np.tile(texture[None], (frames, 1, 1, 1)),
+                sh=per["sh"],
                 extr=np.tile(ex[None], (frames, 1)), intr=np.tile(it[None], (frames, 1)),
                 texcoords=spherical_uvs(verts, faces),
                 target=target_u8.astype(np.float32) / np.float32(255.0), target_u8=target_u8,
                 dt=dt, crops=identity_crops(frames, views, width, height),
-                N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=width, H=height)
+                N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=width, H=height, first_frame=first_frame)

@@ -14,6 +14,8 @@ from deepcharacters_b200 import synthetic as S
 from deepcharacters_b200.renderer import RendererEngine, renderer_backward
 from oracle import oracle as O
 
+from _conditioning import well_conditioned_mask
+
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not O.ref_available(), reason="reference kernels (oracle/_ref) not built")]
 
@@ -72,48 +74,6 @@ def test_backward_matches_reference_kernels(albedo, shading, ifs, tfs):
     print(msg)
 
 
-def well_conditioned_mask(sc, face, bary, albedo, min_cos=0.1, margin=2e-3):
-    """Pixels whose gradient is well conditioned in FP32: the ray is not
-    grazing the triangle (|cos| >= min_cos; the derivative scales with
-    1/cos and so does its FP32 rounding) and, for textures, the discrete
-    texel / tap choices are not within `margin` of flipping."""
-    B, C, H, W = face.shape
-    faces = sc["faces"]
-    tc = sc["texcoords"].reshape(-1, 3, 2)
-    TH = TW = sc["texture"].shape[1]
-    m = np.zeros(face.shape, bool)
-    yy, xx = np.mgrid[0:H, 0:W].astype(np.float64)
-    for b in range(B):
-        V = sc["verts"][b].astype(np.float64)
-        for c in range(C):
-            E = np.eye(4)
-            E[:3] = sc["extr"][b, 12 * c:12 * c + 12].reshape(3, 4)
-            K = np.eye(4)
-            K[:3, :3] = sc["intr"][b, 9 * c:9 * c + 9].reshape(3, 3)
-            inv = np.linalg.inv(K @ E)
-            o = np.linalg.inv(E)[:3, 3]
-            pts = np.stack([(xx + 0.5) * 1000, (yy + 0.5) * 1000, np.full_like(xx, 1000.0), np.ones_like(xx)], -1)
-            q = pts @ inv.T
-            d = q[..., :3] - o
-            d /= np.linalg.norm(d, axis=-1, keepdims=True)
-            f = face[b, c]
-            ok = f >= 0
-            fi = np.where(ok, f, 0)
-            v0, v1, v2 = V[faces[fi, 0]], V[faces[fi, 1]], V[faces[fi, 2]]
-            n = np.cross(v1 - v0, v2 - v0)
-            n /= np.linalg.norm(n, axis=-1, keepdims=True)
-            good = ok & (np.abs((d * n).sum(-1)) >= min_cos)
-            if albedo == "textured":
-                a, bb = bary[b, c, ..., 0].astype(np.float64), bary[b, c, ..., 1].astype(np.float64)
-                t = tc[fi]
-                u = (t[..., 0, 0] * a + t[..., 1, 0] * bb + t[..., 2, 0] * (1 - a - bb)) * TW
-                v = ((1 - t[..., 0, 1]) * a + (1 - t[..., 1, 1]) * bb + (1 - t[..., 2, 1]) * (1 - a - bb)) * TH
-                fr = lambda x: np.minimum(np.mod(x, 1.0), 1 - np.mod(x, 1.0))  # noqa: E731
-                good &= (fr(u - 0.5) > margin) & (fr(v - 0.5) > margin) & (fr(v * TW + u) > margin * TW)
-            m[b, c] = good
-    return m
-
-
 @pytest.mark.parametrize("albedo,shading,ifs,tfs", CASES)
 def test_exact_backward_matches_fp64_oracle(albedo, shading, ifs, tfs):
     """Default (closed-form) adjoint against the FP64 restatement of the
@@ -129,7 +89,8 @@ def test_exact_backward_matches_fp64_oracle(albedo, shading, ifs, tfs):
     extr, intr, target = _t(sc["extr"]), _t(sc["intr"]), _t(sc["target"])
     bary, face, render, vn, _ = eng.forward(verts, colors, tex, sh, extr, intr)
     g_all = torch.randn((B, C, H, W, 3), device=DEV, generator=torch.Generator(DEV).manual_seed(4))
-    mask = well_conditioned_mask(sc, face.cpu().numpy(), bary.cpu().numpy(), albedo)
+    mask = well_conditioned_mask(sc["verts"], sc["faces"], sc["texcoords"], sc["texture"].shape[1], sc["extr"],
+                                 sc["intr"], face.cpu().numpy(), bary.cpu().numpy(), albedo)
     t = lambda a: torch.from_numpy(a)  # noqa: E731
     keys = {"pos": "vertex_pos_grad", "col": "vertex_color_grad", "tex": "texture_grad", "sh": "sh_coeff_grad"}
     use = ["pos", "col" if albedo == "vertexColor" else "tex"] + (["sh"] if shading == "shaded" else [])

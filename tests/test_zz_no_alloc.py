@@ -63,3 +63,53 @@ def test_static_scratch_matches_allocating_entry_point_twice():
         assert int((ref[3] >= 0).sum()) > 0
         for a, b in zip(out, ref):
             assert torch.equal(a, b), f"call {call}"
+
+
+def _need_bytes(views, N, U, V):
+    """Grid scratch of one call, as documented in hc.h."""
+    cells = (-(-U // 30) + 3) * (-(-V // 30) + 3)
+    return 4 * (views * (3 * cells + N) + 1)
+
+
+@pytest.mark.gpu
+def test_static_scratch_at_its_limit():
+    """8 views of 1024x1024: with 40,962 points (the documented example) and
+    with the largest point count whose grid still fits the 8 MiB array (its
+    last words in use), the static call equals the handle-based forward on
+    synthetic points; one point more is refused with HC_ERR_INVALID."""
+    import torch
+
+    from deepcharacters_b200 import synthetic as S
+    from deepcharacters_b200.silhouette import SilhouetteEngine
+
+    dev = "cuda:0"
+    B, Cn, U, V = 1, 8, 1024, 1024
+    cap = 8 << 20
+    n_max = (cap // 4 - 1 - B * Cn * 3 * ((-(-U // 30) + 3) * (-(-V // 30) + 3))) // (B * Cn)
+    assert _need_bytes(B * Cn, n_max, U, V) <= cap < _need_bytes(B * Cn, n_max + 1, U, V)
+    P = _lib.ptr
+    eng = SilhouetteEngine()
+    dt = torch.from_numpy(S.silhouette_masks(B, Cn, U, V, seed=5, scale=2.0)).to(dev)
+    crops = torch.from_numpy(S.identity_crops(B, Cn, U, V)).to(dev)
+    gen = torch.Generator(dev).manual_seed(9)
+    for N in (40962, n_max):
+        p2d = torch.rand((B, Cn, N, 2), device=dev, generator=gen) * torch.tensor([U, V], device=dev)
+        n2d = torch.nn.functional.normalize(torch.randn((B, Cn, N, 2), device=dev, generator=gen), dim=-1)
+        isb = (torch.rand((B, Cn, N), device=dev, generator=gen) < 0.05).to(torch.uint8)
+        ref = eng.forward(p2d, n2d, isb, dt, crops)
+        for call in range(2):
+            out = [torch.full_like(x, 7.0) for x in ref]
+            st = _static_call(B, Cn, N, U, V, [P(p2d), P(n2d), P(isb), P(dt), P(crops)] + [P(x) for x in out],
+                              torch.cuda.current_stream().cuda_stream)
+            assert st == 0, _lib.lib().hc_last_error()
+            torch.cuda.synchronize()
+            assert int((ref[3] >= 0).sum()) > 0
+            for a, b in zip(out, ref):
+                assert torch.equal(a, b), (N, call)
+    N = n_max + 1
+    big = [torch.zeros((B, Cn, N, 2), device=dev)] * 2 + [torch.zeros((B, Cn, N), device=dev, dtype=torch.uint8)]
+    outs = [torch.zeros((B, Cn, N), device=dev), torch.zeros((B, Cn, V, U, 2), device=dev),
+            torch.zeros((B, Cn, N, 2), device=dev), torch.zeros((B, Cn, V, U), device=dev)]
+    st = _static_call(B, Cn, N, U, V, [P(big[0]), P(big[1]), P(big[2]), P(dt), P(crops)] + [P(x) for x in outs],
+                      torch.cuda.current_stream().cuda_stream)
+    assert st == 1 and b"static scratch holds 8388608 bytes" in _lib.lib().hc_last_error()
