@@ -30,6 +30,33 @@ HC_HD float3 cross(float3 a, float3 b) {
 HC_HD float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 HC_HD float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 
+
+// Quotient and remainder of 32-bit unsigned integers by a divisor that is
+// fixed for a launch, as a multiply-high and two shifts instead of the
+// emulated integer division.  Method: Granlund and Montgomery, "Division by
+// invariant integers using multiplication" (PLDI 1994), figure 4.1: for
+// 1 <= d < 2^32 with l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+// sh1 = min(l, 1), sh2 = max(l - 1, 0), every n < 2^32 has
+// n / d = (t + ((n - t) >> sh1)) >> sh2 with t = mulhi(m, n).
+struct FastDiv {
+    unsigned d = 1, m = 1, sh1 = 0, sh2 = 0;
+    FastDiv() = default;
+    explicit FastDiv(unsigned divisor) : d(divisor ? divisor : 1u) {
+        unsigned l = 0;
+        while (l < 32 && (1ull << l) < d) ++l;
+        m = (unsigned)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+        sh1 = l < 1 ? l : 1u;
+        sh2 = l > 1 ? l - 1 : 0u;
+    }
+#ifdef __CUDACC__
+    __device__ __forceinline__ unsigned div(unsigned n) const {
+        const unsigned t = __umulhi(m, n);
+        return (t + ((n - t) >> sh1)) >> sh2;
+    }
+    __device__ __forceinline__ unsigned mod(unsigned n, unsigned q) const { return n - q * d; }
+#endif
+};
+
 #ifdef __CUDACC__
 __device__ __forceinline__ float length3(float3 v) { return sqrtf(dot(v, v)); }
 __device__ __forceinline__ float3 normalize3(float3 v) {

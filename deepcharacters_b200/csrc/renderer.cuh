@@ -39,6 +39,7 @@ struct ViewCam {
     // start in the call's buffers (cameras of a frame may differ in size)
     int W, H, tiles_x, tiles_x_b;
     long long pix_base, tile_base, tile_base_b;
+    FastDiv fd_tiles_x, fd_tiles_x_b;  // division by tiles_x / tiles_x_b
 };
 
 constexpr int kAdjointTile = 16;  // tile edge of the renderer adjoint
@@ -49,6 +50,7 @@ struct CamLayout {
     int W, H;
     int tiles_x, tiles_x_b;        // raster tiles (ws.tile px) / adjoint tiles (16 px) per row
     long long pix, tile, tile_b;   // first pixel / raster tile / adjoint tile in the frame
+    FastDiv fd_tiles_x, fd_tiles_x_b;
 };
 
 struct TriFrame {    // 48 bytes: s0.xyz n.x | s1.xyz n.y | s2.xyz n.z

@@ -39,6 +39,7 @@ static_assert(BT == kAdjointTile, "the adjoint tile grid of the layout");
 struct BwdArgs {
     int B, C, N, F;
     long long Tb_frame;      // adjoint tiles per frame (all cameras)
+    FastDiv fd_frame;        // division by Tb_frame (the call has < 2^31 adjoint tiles)
     const int* tile_cam_b;   // camera of each adjoint tile of a frame
     int albedo, shading;
     int ifs, tfs;
@@ -73,16 +74,20 @@ __device__ __forceinline__ float3 unit3(int k) {
 
 // d(a, b)/d(v0, v1, v2): the barycentric Jacobian of the reference's
 // dJBCDVerpos (RendererUtil.h:670-861) for a = dot(N, C1)/|N|^2 (weight of
-// v0) and b = dot(N, C2)/|N|^2 (weight of v1), in unscaled (mm) coordinates.
-// Returns false (all zero) for grazing rays or degenerate triangles.
-__device__ bool bary_jacobian(float3 o, float3 d, float3 v0, float3 v1, float3 v2, float ja[9], float jb[9]) {
+// v0) and b = dot(N, C2)/|N|^2 (weight of v1), in unscaled (mm) coordinates,
+// contracted with the gradient w.r.t. the three barycentrics as it is formed:
+// gp[var] = g.x * ja[var] + g.y * jb[var] + g.z * (-ja[var] - jb[var]), the
+// reference's 3x9 product, one column at a time (no 2 x 9 row arrays live).
+// Leaves gp at zero for grazing rays or degenerate triangles.
+__device__ __forceinline__ void bary_jacobian_apply(float3 o, float3 d, float3 v0, float3 v1, float3 v2, float3 g,
+                                                    float gp[9]) {
     const float3 e01 = v1 - v0, e02 = v2 - v0;
     const float3 N = cross(e01, e02);
     const float denom = dot(N, N);
     const float ndr = dot(d, N);
 #pragma unroll
-    for (int i = 0; i < 9; ++i) ja[i] = jb[i] = 0.f;
-    if (fabsf(dot(normalize3(d), normalize3(N))) < 0.001f || fabsf(denom * denom) < 0.001f) return false;
+    for (int i = 0; i < 9; ++i) gp[i] = 0.f;
+    if (fabsf(dot(normalize3(d), normalize3(N))) < 0.001f || fabsf(denom * denom) < 0.001f) return;
     const float t = (dot(v0, N) - dot(o, N)) / ndr;
     const float3 P = o + t * d;
     const float3 E0 = v2 - v1, E1 = v0 - v2;
@@ -112,10 +117,10 @@ __device__ bool bary_jacobian(float3 o, float3 d, float3 v0, float3 v1, float3 v
         const float nd = 2.f * dot(N, dN);
         const float dtmp0 = dot(dN, C0) + dot(N, cross(dE0, vp0) + cross(E0, dt * d - dv1));
         const float dtmp1 = dot(dN, C1) + dot(N, cross(dE1, vp1) + cross(E1, dt * d - dv2));
-        ja[var] = dtmp0 * inv_den + tmp0 * inv_den2 * nd;
-        jb[var] = dtmp1 * inv_den + tmp1 * inv_den2 * nd;
+        const float ja = dtmp0 * inv_den + tmp0 * inv_den2 * nd;
+        const float jb = dtmp1 * inv_den + tmp1 * inv_den2 * nd;
+        gp[var] = g.x * ja + g.y * jb + g.z * (-ja - jb);
     }
-    return true;
 }
 
 // Sobel-like image gradient of the reference (imageGradient, RendererUtil.h:566-620):
@@ -273,10 +278,11 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
     // copied into the other shared buffer with cp.async while this tile's
     // pixels are processed, so the copy latency is hidden.
     auto stage = [&](long long gt, int buf) {
-        const int sb = (int)(gt / A.Tb_frame);
-        const ViewCam& sc = cams[sb * A.C + A.tile_cam_b[gt % A.Tb_frame]];
+        const unsigned sb = A.fd_frame.div((unsigned)gt);
+        const ViewCam& sc = cams[(int)sb * A.C + A.tile_cam_b[A.fd_frame.mod((unsigned)gt, sb)]];
         const int st = (int)(gt - sc.tile_base_b);
-        const int sx0 = (st % sc.tiles_x_b) * BT, sy0 = (st / sc.tiles_x_b) * BT;
+        const int sty = (int)sc.fd_tiles_x_b.div((unsigned)st);
+        const int sx0 = (int)sc.fd_tiles_x_b.mod((unsigned)st, sty) * BT, sy0 = sty * BT;
         const float* stg = A.target + sc.pix_base * 3;
         const int e = BT + 2 * A.ifs;
         for (int i = threadIdx.x; i < e * e; i += BNT) {
@@ -304,12 +310,13 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
     const int e_st = BT + 2 * A.ifs;
     const unsigned raw_bytes = (unsigned)(e_st * kRawX * sizeof(float));
     auto tma_issue = [&](long long gt) {  // thread 0
-        const int sb = (int)(gt / A.Tb_frame);
-        const int sv = sb * A.C + A.tile_cam_b[gt % A.Tb_frame];
+        const unsigned sb = A.fd_frame.div((unsigned)gt);
+        const int sv = (int)sb * A.C + A.tile_cam_b[A.fd_frame.mod((unsigned)gt, sb)];
         const ViewCam& sc = cams[sv];
         const int st = (int)(gt - sc.tile_base_b);
-        const int x = (3 * ((st % sc.tiles_x_b) * BT - A.ifs)) & ~3;  // floats, rounded down to 16 bytes
-        const int y = (st / sc.tiles_x_b) * BT - A.ifs;
+        const int sty = (int)sc.fd_tiles_x_b.div((unsigned)st);
+        const int x = (3 * ((int)sc.fd_tiles_x_b.mod((unsigned)st, sty) * BT - A.ifs)) & ~3;  // floats, rounded down to 16 bytes
+        const int y = sty * BT - A.ifs;
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tma_box(&tmap, smem_u32(s_raw), smem_u32(&s_mbar), x, y, sv, raw_bytes);
     };
@@ -337,8 +344,10 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
             mbar_wait(smem_u32(&s_mbar), (unsigned)(it & 1));
             return;
         }
-        const ViewCam& gc = cams[(int)(g / A.Tb_frame) * A.C + A.tile_cam_b[g % A.Tb_frame]];
-        const int cx0 = ((int)(g - gc.tile_base_b) % gc.tiles_x_b) * BT - A.ifs;
+        const unsigned gb = A.fd_frame.div((unsigned)g);
+        const ViewCam& gc = cams[(int)gb * A.C + A.tile_cam_b[A.fd_frame.mod((unsigned)g, gb)]];
+        const unsigned gtile = (unsigned)(g - gc.tile_base_b);
+        const int cx0 = (int)gc.fd_tiles_x_b.mod(gtile, gc.fd_tiles_x_b.div(gtile)) * BT - A.ifs;
         const int off = 3 * cx0 - ((3 * cx0) & ~3);  // floats before the first halo column in a box row
         for (int i = threadIdx.x; i < e_st * e_st; i += BNT) {
             const int r = i / e_st, c = i - r * e_st;
@@ -351,12 +360,14 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         stage(g + gridDim.x, buf ^ 1);
     }
     asm volatile("cp.async.commit_group;\n" ::);
-    const int b = (int)(g / A.Tb_frame);
-    const int view = b * A.C + A.tile_cam_b[g % A.Tb_frame];
+    const unsigned fb = A.fd_frame.div((unsigned)g);
+    const int b = (int)fb;
+    const int view = b * A.C + A.tile_cam_b[A.fd_frame.mod((unsigned)g, fb)];
     const ViewCam& cam = cams[view];
     const int tile = (int)(g - cam.tile_base_b);
-    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x_b;
-    const int tx0 = (tile % tiles_x) * BT, ty0 = (tile / tiles_x) * BT;
+    const int W = cam.W, H = cam.H;
+    const int tyi = (int)cam.fd_tiles_x_b.div((unsigned)tile);
+    const int tx0 = (int)cam.fd_tiles_x_b.mod((unsigned)tile, tyi) * BT, ty0 = tyi * BT;
     const int px = tx0 + threadIdx.x % BT;
     const int py = ty0 + threadIdx.x / BT;
     const float* tgt = A.target + cam.pix_base * 3;
@@ -571,10 +582,7 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         // data -> model through the barycentric Jacobian
         if constexpr (PARITY) {
             const float3 o = make_float3(cam.ro[0], cam.ro[1], cam.ro[2]);
-            float ja[9], jb[9];
-            bary_jacobian(o, d, v0, v1, v2, ja, jb);
-#pragma unroll
-            for (int k = 0; k < 9; ++k) gp[k] = gbc.x * ja[k] + gbc.y * jb[k] + gbc.z * (-ja[k] - jb[k]);
+            bary_jacobian_apply(o, d, v0, v1, v2, gbc, gp);
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 gp[3 * i + 0] += m.x * bw[i];
@@ -782,6 +790,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.N = N;
     A.F = topo.F;
     A.Tb_frame = ws.Tb_frame;
+    A.fd_frame = FastDiv((unsigned)ws.Tb_frame);
     A.tile_cam_b = ws.tile_cam_b.as<int>();
     A.albedo = albedo;
     A.shading = shading;
@@ -811,6 +820,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.l1_render = l1 ? l1->render : nullptr;
     A.l1_mask = l1 ? l1->mask : nullptr;
     const long long tiles = (long long)B * ws.Tb_frame;
+    HC_REQUIRE(tiles < (1ll << 31), "too many adjoint tiles in one call (%lld)", tiles);
     // the target's tensor map for the TMA staging, where its layout allows it
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));

@@ -35,6 +35,8 @@ __global__ void k_view_setup(int V, int C, const float* __restrict__ extr, const
         c.H = L.H;
         c.tiles_x = L.tiles_x;
         c.tiles_x_b = L.tiles_x_b;
+        c.fd_tiles_x = L.fd_tiles_x;
+        c.fd_tiles_x_b = L.fd_tiles_x_b;
         c.pix_base = b * P_frame + L.pix;
         c.tile_base = b * T_frame + L.tile;
         c.tile_base_b = b * Tb_frame + L.tile_b;
@@ -565,7 +567,7 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, long long T_frame,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, FastDiv fd_frame,
                                                    const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
@@ -597,12 +599,13 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     }
     const long long g = s_g[(it / kClaim) & 1] + it % kClaim;
     if (g >= n_tiles) break;
-    const int b = (int)(g / T_frame);
-    const int view = b * A.C + tile_cam[g % T_frame];
+    // tile -> (frame, camera, tile of the camera): the call has < 2^31 tiles
+    const int b = (int)fd_frame.div((unsigned)g);
+    const int view = b * A.C + tile_cam[fd_frame.mod((unsigned)g, (unsigned)b)];
     const ViewCam& cam = cams[view];
     const int tile = (int)(g - cam.tile_base);
-    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x;
-    const int tx = tile % tiles_x, ty = tile / tiles_x;
+    const int W = cam.W, H = cam.H;
+    const int ty = (int)cam.fd_tiles_x.div((unsigned)tile), tx = (int)cam.fd_tiles_x.mod((unsigned)tile, ty);
     const int lx = threadIdx.x % TS, ly = threadIdx.x / TS;
     const int px = tx * TS + lx, py = ty * TS + ly;
     const unsigned col_bit = 1u << lx, row_bit = 1u << ly;
@@ -881,6 +884,8 @@ hc_status raster_layout(RasterWorkspace& ws) {
         l.H = ws.cam_h[c];
         l.tiles_x = div_up(l.W, TS);
         l.tiles_x_b = div_up(l.W, kAdjointTile);
+        l.fd_tiles_x = FastDiv((unsigned)l.tiles_x);
+        l.fd_tiles_x_b = FastDiv((unsigned)l.tiles_x_b);
         l.pix = pix;
         l.tile = tile;
         l.tile_b = tile_b;
@@ -1024,7 +1029,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
 #define HC_RESOLVE_CASE(TSV)                                                                                   \
     case TSV:                                                                                                  \
         k_resolve<TSV><<<resident_grid(k_resolve<TSV>, TSV * TSV, tiles), TSV * TSV, 0, s>>>(                  \
-            A, ws.T_frame, tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill, ws.spill_tile_cap, tiles, claim); \
+            A, FastDiv((unsigned)ws.T_frame), tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill, ws.spill_tile_cap, tiles, claim); \
         break;
     switch (TS) {
         HC_RESOLVE_CASE(8)
