@@ -387,6 +387,7 @@ def run_ours(args, world, rank, local):
     en.record()
     torch.cuda.synchronize()
     clocks = clk.stop()
+    ch.rend.stats()  # raises if a raster capacity overflowed or an adjoint copy failed
     ms = max_over_ranks(st.elapsed_time(en) / args.steps, world)
     barrier(world)
     value = views_per_step * world / (ms / 1e3)
@@ -473,6 +474,114 @@ def run_ours(args, world, rank, local):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+C3_METRIC = ("fwd+bwd views/s at 20,480 tris, 16 frames x 8 views of mixed resolution "
+             "{512², 768x1024, 1024², 1536x1024}: one call per stage, one CUDA graph per step")
+C3_SUBDIV = 5
+
+
+def run_ours_c3(args, world, rank, local):
+    """The batched mixed-resolution configuration: the subdivision-5 character
+    (10,242 vertices / 20,480 triangles) skinned per vertex by dual
+    quaternions of a 24-joint tree (U(-0.5, 0.5) joint angles), 16 frames x 8
+    cameras whose sizes are drawn uniformly from {512x512, 768x1024,
+    1024x1024, 1536x1024} (fx = fy = 600 min(W, H) / 512), vertex-colour
+    raster + masked L1 + silhouette DT loss, adjoints to the joint angles and
+    vertex colours; every stage one call over all views of the step, the step
+    one CUDA graph, the raster tiling autotuned."""
+    from deepcharacters_b200 import _lib
+    from deepcharacters_b200 import synthetic as S
+    from deepcharacters_b200.chain import DeformRenderChain
+    dev = torch.device("cuda", local)
+    first, frames = D.rank_frames(FRAMES, world, rank)
+    ws, hs = S.mixed_camera_sizes(VIEWS, SEED)
+    sc = S.chain_scene(C3_SUBDIV, 200, N_SKEL, frames, VIEWS, ws, hs, seed=SEED, first_frame=first)
+    parity = args.adjoint == "parity"
+    ch = DeformRenderChain(sc, dev, frames, VIEWS, ws, hs, W_SIL, W_SIL1, gradient_parity=parity, deformation="dq")
+    gcol_shared = torch.zeros((sc["N"], 3), device=dev)
+    cands = ((8, 128), (8, 256), (16, 256), (16, 512), (32, 512), (32, 1024))
+    tune = ch.autotune(cands) if not args.no_autotune else {}
+    binned, spilled = ch.check()
+    for _ in range(2):
+        ch.step()
+    torch.cuda.synchronize()
+    l0 = _lib.lib().hc_kernel_launches()
+    g = ch.capture_step()
+    launches_per_step = _lib.lib().hc_kernel_launches() - l0
+
+    def reduce_shared():
+        D.shared_gradient(ch.buf["gcol"], gcol_shared, world)
+
+    for _ in range(args.warmup):
+        g.replay()
+        reduce_shared()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = ClockSampler(local)
+    clk.start()
+    st, en = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st.record()
+    for _ in range(args.steps):
+        g.replay()
+        reduce_shared()
+    en.record()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    ch.rend.stats()  # raises if a raster capacity overflowed or an adjoint copy failed
+    ms = max_over_ranks(st.elapsed_time(en) / args.steps, world)
+    barrier(world)
+    value = frames * VIEWS * world / (ms / 1e3)
+    ch.rend.set_kernel_timing(True)
+    kern = {}
+    for _ in range(3):
+        ch.forward()
+        ch.backward()
+        for k, v in ch.rend.kernel_times().items():
+            kern.setdefault(k, []).append(v)
+    ch.rend.set_kernel_timing(False)
+    kern = {k: sum(v) / len(v) for k, v in kern.items()}
+    covered = int((ch.buf["face"] >= 0).sum())
+    N, F, P = sc["N"], sc["F"], sc["P_frame"]
+    kbytes = {"resolve": frames * 24 * P + 12 * covered + frames * (24 * N + 12 * F),
+              "render_grad": frames * 4 * P + 32 * covered + frames * (24 * N + 12 * F + 24 * N)}
+    dom = max(("resolve", "render_grad"), key=lambda k: kern[k])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    ach = kbytes[dom] / (kern[dom] / 1e3) / 1e9
+    e2e = None if args.no_e2e else run_e2e(ch, sc, dev, args, world, reduce_shared)
+    line = {
+        "metric": C3_METRIC, "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded icosphere character, random poses, ring cameras of mixed sizes, "
+                                "random targets, ellipse silhouettes)",
+        "config": {"workload": "batched mixed-resolution chain fwd+bwd: icosphere subdiv-5 (10,242 verts / 20,480 "
+                               "tris), vertex DQ skinning by a 24-joint tree (72 revolute dofs), 16 frames x 8 views "
+                               "at per-camera sizes drawn from {512x512, 768x1024, 1024x1024, 1536x1024}, "
+                               "vertexColor raster + masked L1 + silhouette DT loss, gradients to joint angles and "
+                               "vertex colours, one CUDA graph per step",
+                   "frames": FRAMES, "views": VIEWS, "camera_sizes": [[w, h] for w, h in zip(ws, hs)],
+                   "pixels_per_frame": P, "triangles": F, "vertices": N, "joints": 3 * N_SKEL,
+                   "adjoint": args.adjoint, "parallelism": f"frames sharded, {world} rank(s)",
+                   "l2": "inputs larger than L2 (%.0f MB of target images per step)" % (frames * P * 12 / 1e6),
+                   "raster_tile": ch.tuning[0], "bin_capacity": ch.tuning[1],
+                   "autotune_ms": {f"{t}x{c}": round(v, 3) for (t, c), v in tune.items()},
+                   "bin_pairs": binned, "spilled_pairs": spilled},
+        "e2e": e2e,
+        "gpu_launches": int(launches_per_step * args.steps),
+        "roofline": {"bound": "hbm", "kernel": "k_" + dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks
+                     else "fallback 6650",
+                     "kernel_ms": kern, "kernel_bytes": kbytes, "covered_pixels": covered},
+        "clocks": clocks,
+    }
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -605,6 +714,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-unbatched", action="store_true", help="skip the un-batched, no-graph leg")
     ap.add_argument("--frames", type=int, default=FRAMES, help="frames per rank (default 16; smaller for profiling)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default raster tiling (8 px, 256)")
+    ap.add_argument("--config", choices=("c2", "c3"), default="c2",
+                    help="c2: the headline chain (default); c3: the batched mixed-resolution chain (own line)")
     args = ap.parse_args(argv)
     if args.steps is None:
         args.steps = 150 if args.impl == "ours" else 10
@@ -617,7 +728,14 @@ def run(args):
     world, rank, local = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
-            run_reference(args, world, rank, local)
+            if args.config != "c2":
+                if rank == 0:
+                    print(json.dumps({"impl": "reference", "config": args.config,
+                                      "unavailable": "the reference arm is run for the headline configuration only"}))
+            else:
+                run_reference(args, world, rank, local)
+        elif args.config == "c3":
+            run_ours_c3(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

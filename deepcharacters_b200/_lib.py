@@ -70,6 +70,11 @@ _SIGS: dict[str, list] = {
     "hc_mesh_boundary_forward": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp],
     "hc_mesh_boundary_forward_hinted": [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, vp,
                                         vp],
+    "hc_mesh_boundary_reserve_sized": [vp, C.c_int32, C.c_int32, vp, vp],
+    "hc_mesh_boundary_forward_sized": [vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp],
+    "hc_silhouette_reserve_sized": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp],
+    "hc_silhouette_forward_sized": [vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp] + [vp] * 9,
+    "hc_silhouette_backward_sized": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp] + [vp] * 6,
     "hc_sum_squares_loss": [vp, C.c_int64, vp, C.c_float, vp, vp, vp],
     "hc_add_inplace": [vp, C.c_int64, vp, vp],
     "hc_image_u8_to_f32": [vp, C.c_int64, vp, vp],

@@ -41,6 +41,14 @@ class DeformRenderChain:
       EG vertices -> camera projection -> mesh boundary -> silhouette DT loss
       adjoints back to node rotations / translations and vertex colours.
 
+    ``deformation="dq"`` replaces node skinning + EG by per-vertex dual-
+    quaternion skinning of the character (DqSkinningGpu), the composition of
+    a skinned character without an embedded graph; its adjoint carries the
+    vertex gradient to the joint angles.  ``width`` / ``height`` may be
+    per-camera sequences: cameras of different sizes share every call, and
+    the per-pixel buffers are [B, pixels of a frame, ...] with the frame's
+    cameras concatenated in order (the reference needs one op per size).
+
     ``loss`` holds (L1, silhouette model->data, silhouette data->model);
     ``buf`` holds every intermediate and gradient (``gT`` / ``gA`` are the
     node translation / rotation gradients, ``gcol`` the vertex colours',
@@ -49,12 +57,24 @@ class DeformRenderChain:
     carries them to the dofs; the reference chain has no such gradient, its
     Pose2EmbeddedGraphCpu op being non-differentiable)."""
 
-    def __init__(self, sc, dev, frames: int, views: int, width: int, height: int, w_sil: float = 1e-3,
+    def __init__(self, sc, dev, frames: int, views: int, width, height, w_sil: float = 1e-3,
                  w_sil1: float = 1e-3, tile: int = 8, bin_capacity: int = 256, gradient_parity: bool = False,
-                 joint_gradients: bool = True, fused_l1: bool = True):
-        B, C, H, W, N = frames, views, height, width, int(sc["verts"].shape[0])
-        M = int(sc["graph"].n_nodes)
-        Mk = int(len(sc["markers"]))
+                 joint_gradients: bool = True, fused_l1: bool = True, deformation: str = "eg"):
+        B, C, N = frames, views, int(sc["verts"].shape[0])
+        # one image size for all cameras, or one per camera (`width` / `height`
+        # sequences): then every per-pixel buffer is [B, pixels of a frame, ...]
+        # with the frame's cameras concatenated, and one call still covers all views
+        ws = np.ascontiguousarray(np.broadcast_to(np.asarray(width, np.int32), (C,)))
+        hs = np.ascontiguousarray(np.broadcast_to(np.asarray(height, np.int32), (C,)))
+        self.widths, self.heights = ws, hs
+        self.multires = not (np.all(ws == ws[0]) and np.all(hs == hs[0]))
+        W, H = int(ws[0]), int(hs[0])
+        self.P_frame = int((ws.astype(np.int64) * hs).sum())
+        if deformation not in ("eg", "dq"):
+            raise ValueError("deformation must be 'eg' (node skinning + embedded graph) or 'dq' (vertex DQ skinning)")
+        self.deformation = deformation
+        M = int(sc["graph"].n_nodes) if deformation == "eg" else 0
+        Mk = int(len(sc["markers"])) if deformation == "eg" else 0
         self.B, self.C, self.H, self.W, self.N, self.M, self.Mk = B, C, H, W, N, M, Mk
         self.w_sil, self.w_sil1 = float(w_sil), float(w_sil1)
         self.skin = SkinningEngine(character(sc))
@@ -64,48 +84,66 @@ class DeformRenderChain:
         # (hc_renderer_forward_l1 / _backward_l1) or as its own op
         # (hc_image_l1_loss + hc_renderer_backward on the gradient image)
         self.fused_l1 = bool(fused_l1)
-        self.eg = EmbeddedGraphEngine(eg_data(sc), full_skinned_gradient=self.joint_gradients)
-        self.eg.reserve(B)
-        self.rend = RendererEngine(sc["faces"], sc["texcoords"], N, C, W, H, "vertexColor", "shadeless", 2, 2)
+        if deformation == "eg":
+            self.eg = EmbeddedGraphEngine(eg_data(sc), full_skinned_gradient=self.joint_gradients)
+            self.eg.reserve(B)
+        self.rend = RendererEngine(sc["faces"], sc["texcoords"], N, C, ws if self.multires else W,
+                                   hs if self.multires else H, "vertexColor", "shadeless", 2, 2)
         self.rend.set_tuning(tile, bin_capacity)
         self.tuning = (tile, bin_capacity)
         if gradient_parity:
             _lib.call("hc_renderer_set_gradient_parity", self.rend.handle, 1)
         self.rend.reserve(B)
         self.mb = MeshBoundaryEngine(sc["faces"], N)
-        self.mb.reserve(B, C, W, H)
         self.sil = SilhouetteEngine()
-        self.sil.reserve(B, C, N, W, H)
+        if self.multires:
+            self.mb.reserve_sized(B, C, ws, hs)
+            self.sil.reserve_sized(B, C, N, ws, hs)
+        else:
+            self.mb.reserve(B, C, W, H)
+            self.sil.reserve(B, C, N, W, H)
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
-        self.inp = {k: t(sc[k]) for k in ("dofs", "dT", "dA", "disp", "colors", "texture", "sh", "extr", "intr",
-                                          "target", "dt", "crops")}
+        keys = ("dofs", "dT", "dA", "disp", "colors", "texture", "sh", "extr", "intr", "target", "dt", "crops")
+        self.inp = {k: t(sc[k]) for k in keys if k in sc}
         self.tex_hw = (int(sc["texture"].shape[1]), int(sc["texture"].shape[2]))
-        self.node_vertex = t(sc["graph"].node_vertex.astype(np.int32))
         self.skin_w = t(np.asarray(sc["skin_weights"], np.float32))
         e = lambda *shape, dt=torch.float32: torch.empty(shape, device=dev, dtype=dt)  # noqa: E731
+        img = (B, self.P_frame) if self.multires else (B, C, H, W)
         self.buf = dict(
-            sT=e(B, M, 3), sA=e(B, M, 3), dq=e(B, self.skin.S, 8),
-            v=e(B, N, 3), n=e(B, N, 3), mk=e(B, Mk, 3), graph=e(B, M, 3), da=e(B, M, 3), sa=e(B, M, 3),
-            bary=e(B, C, H, W, 2), face=e(B, C, H, W, dt=torch.int32), render=e(B, C, H, W, 3),
-            vnormal=e(B, C, N, 3), grad_img=None if fused_l1 else e(B, C, H, W, 3),
+            v=e(B, N, 3), n=e(B, N, 3),
+            bary=e(*img, 2), face=e(*img, dt=torch.int32), render=e(*img, 3),
+            vnormal=e(B, C, N, 3), grad_img=None if fused_l1 else e(*img, 3),
             p2d=e(B, C, N, 2), n2d=e(B, C, N, 2), isb=e(B, C, N, dt=torch.uint8),
-            res=e(B, C, N), res1=e(B, C, H, W, 2), dtg=e(B, C, N, 2), cid=e(B, C, H, W),
-            g_res=e(B, C, N), g_res1=e(B, C, H, W, 2), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
-            gv=e(B, N, 3), gcol=e(B, N, 3), gsh=e(B, C, 27), gm=torch.zeros((B, Mk, 3), device=dev),
-            gT=e(B, M, 3), gA=e(B, M, 3), gsT=e(B, M, 3), gsA=e(B, M, 3), gdisp=e(B, N, 3),
+            res=e(B, C, N), res1=e(*img, 2), dtg=e(B, C, N, 2), cid=e(*img),
+            g_res=e(B, C, N), g_res1=e(*img, 2), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
+            gv=e(B, N, 3), gcol=e(B, N, 3), gsh=e(B, C, 27),
             gdofs=torch.zeros((B, self.skin.D), device=dev))
+        if deformation == "eg":
+            self.node_vertex = t(sc["graph"].node_vertex.astype(np.int32))
+            self.buf.update(sT=e(B, M, 3), sA=e(B, M, 3), dq=e(B, self.skin.S, 8), mk=e(B, Mk, 3),
+                            graph=e(B, M, 3), da=e(B, M, 3), sa=e(B, M, 3), gm=torch.zeros((B, Mk, 3), device=dev),
+                            gT=e(B, M, 3), gA=e(B, M, 3), gsT=e(B, M, 3), gsA=e(B, M, 3), gdisp=e(B, N, 3))
+        else:  # per-vertex DQ skinning: the frame's skin weights, joints and dual quaternions
+            K = self.skin.K
+            self.buf.update(weights=self.skin_w.unsqueeze(0).expand(B, N, K).contiguous(), gjp=e(B, self.skin.J, 3),
+                            gja=e(B, self.skin.J, 3), dq=e(B, self.skin.S, 8), outw=e(B, N, K), gw=e(B, N, K))
         self.loss = torch.zeros((3,), device=dev)
         self.ws = torch.zeros((8,), device=dev, dtype=torch.float64)
 
     def forward(self):
-        """Node skinning, EG deformation, raster and the L1 image loss + its gradient."""
+        """Deformation (node skinning + EG, or vertex DQ skinning), raster and the
+        L1 image loss + its gradient."""
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
-        B, C, H, W, M = self.B, self.C, self.H, self.W, self.M
-        L("hc_pose2eg_forward", self.skin.handle, s, B, P(i["dofs"]), M, P(self.node_vertex), P(self.skin_w),
-          P(o["sT"]), P(o["sA"]), P(o["dq"]))
-        L("hc_eg_forward", self.eg.handle, s, B, P(i["dT"]), P(i["dA"]), P(o["sT"]), P(o["sA"]), P(i["disp"]),
-          P(o["v"]), P(o["n"]), P(o["mk"]), P(o["graph"]), P(o["da"]), P(o["sa"]))
+        B, C, M = self.B, self.C, self.M
+        if self.deformation == "eg":
+            L("hc_pose2eg_forward", self.skin.handle, s, B, P(i["dofs"]), M, P(self.node_vertex), P(self.skin_w),
+              P(o["sT"]), P(o["sA"]), P(o["dq"]))
+            L("hc_eg_forward", self.eg.handle, s, B, P(i["dT"]), P(i["dA"]), P(o["sT"]), P(o["sA"]), P(i["disp"]),
+              P(o["v"]), P(o["n"]), P(o["mk"]), P(o["graph"]), P(o["da"]), P(o["sa"]))
+        else:
+            L("hc_dq_skinning_forward", self.skin.handle, s, B, P(i["dofs"]), P(o["weights"]), P(o["v"]), P(o["n"]),
+              P(o["gjp"]), P(o["gja"]), P(o["dq"]), P(o["outw"]))
         if self.fused_l1:
             L("hc_renderer_forward_l1", self.rend.handle, s, B, P(o["v"]), P(i["colors"]), P(i["texture"]),
               *self.tex_hw, P(i["sh"]), P(i["extr"]), P(i["intr"]), P(o["bary"]), P(o["face"]), P(o["render"]),
@@ -113,7 +151,7 @@ class DeformRenderChain:
             return
         L("hc_renderer_forward", self.rend.handle, s, B, P(o["v"]), P(i["colors"]), P(i["texture"]), *self.tex_hw,
           P(i["sh"]), P(i["extr"]), P(i["intr"]), P(o["bary"]), P(o["face"]), P(o["render"]), P(o["vnormal"]), None)
-        L("hc_image_l1_loss", s, B * C * H * W, P(o["render"]), P(i["target"]), P(o["face"]), None, P(self.ws),
+        L("hc_image_l1_loss", s, B * self.P_frame, P(o["render"]), P(i["target"]), P(o["face"]), None, P(self.ws),
           P(self.loss), P(o["grad_img"]))
 
     def silhouette_forward(self):
@@ -125,13 +163,20 @@ class DeformRenderChain:
         L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), P(o["n"]), P(i["extr"]), P(i["intr"]), 0,
           P(o["n2d"]))
         # the renderer's face buffer of the same views is the coverage hint
-        L("hc_mesh_boundary_forward_hinted", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]), P(i["intr"]),
-          P(o["p2d"]), P(o["face"]), P(o["isb"]))
-        L("hc_silhouette_forward", self.sil.handle, s, B, C, N, W, H, P(o["p2d"]), P(o["n2d"]), P(o["isb"]),
-          P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
+        if self.multires:
+            ws, hs = self.widths.ctypes.data, self.heights.ctypes.data
+            L("hc_mesh_boundary_forward_sized", self.mb.handle, s, B, C, ws, hs, P(o["v"]), P(i["extr"]),
+              P(i["intr"]), P(o["p2d"]), P(o["face"]), P(o["isb"]))
+            L("hc_silhouette_forward_sized", self.sil.handle, s, B, C, N, ws, hs, P(o["p2d"]), P(o["n2d"]),
+              P(o["isb"]), P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
+        else:
+            L("hc_mesh_boundary_forward_hinted", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]),
+              P(i["intr"]), P(o["p2d"]), P(o["face"]), P(o["isb"]))
+            L("hc_silhouette_forward", self.sil.handle, s, B, C, N, W, H, P(o["p2d"]), P(o["n2d"]), P(o["isb"]),
+              P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
         L("hc_sum_squares_loss", s, B * C * N, P(o["res"]), self.w_sil, self.ws.data_ptr() + 16,
           self.loss.data_ptr() + 4, P(o["g_res"]))
-        L("hc_sum_squares_loss", s, B * C * H * W * 2, P(o["res1"]), self.w_sil1, self.ws.data_ptr() + 24,
+        L("hc_sum_squares_loss", s, B * self.P_frame * 2, P(o["res1"]), self.w_sil1, self.ws.data_ptr() + 24,
           self.loss.data_ptr() + 8, P(o["g_res1"]))
 
     def silhouette_backward(self):
@@ -139,14 +184,19 @@ class DeformRenderChain:
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
         B, C, H, W, N = self.B, self.C, self.H, self.W, self.N
-        L("hc_silhouette_backward", s, B, C, N, W, H, P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]),
-          P(i["crops"]), P(o["gp2d"]))
+        if self.multires:
+            L("hc_silhouette_backward_sized", s, B, C, N, self.widths.ctypes.data, self.heights.ctypes.data,
+              P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]), P(i["crops"]), P(o["gp2d"]))
+        else:
+            L("hc_silhouette_backward", s, B, C, N, W, H, P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]),
+              P(i["crops"]), P(o["gp2d"]))
         L("hc_camera_projection_backward", s, B, C, N, P(o["gp2d"]), P(o["v"]), P(i["extr"]), P(i["intr"]), 1,
           P(o["gv_sil"]))
 
     def backward(self):
-        """Raster adjoint, the sum of the two vertex-position gradients, EG adjoint
-        (and the node-skinning adjoint to the joint angles)."""
+        """Raster adjoint, the sum of the two vertex-position gradients, then the
+        deformation's adjoint: EG (and the node-skinning adjoint to the joint
+        angles), or the vertex DQ skinning's to the joint angles."""
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
         B, N = self.B, self.N
@@ -159,6 +209,10 @@ class DeformRenderChain:
               P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]), P(o["bary"]),
               P(o["face"]), P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
         L("hc_add_inplace", s, B * N * 3, P(o["gv"]), P(o["gv_sil"]))
+        if self.deformation == "dq":  # joint angles (and skin weights) through the vertex DQ skinning
+            L("hc_dq_skinning_backward", self.skin.handle, s, B, P(o["gv"]), P(o["v"]), P(o["gjp"]), P(o["gja"]),
+              P(o["dq"]), P(o["weights"]), P(o["gdofs"]), P(o["gw"]))
+            return
         full = self.joint_gradients
         L("hc_eg_backward", self.eg.handle, s, B, P(o["gv"]), P(o["gm"]), P(o["da"]), P(o["sa"]), P(o["gT"]),
           P(o["gA"]), P(o["gsT"]), P(o["gsA"]), P(o["gdisp"]), P(i["dT"]) if full else None,

@@ -175,6 +175,58 @@ constexpr int kCovTile = 8;
 constexpr int kCovCap = 256;
 constexpr int kCovSmall = 9;  // tiles a thread bins on its own (a 3x3 box of tiles)
 
+// Image layout of the views of one call.  Views are frame-major (view =
+// frame * n_cam + camera) and every camera has its own image size: a view's
+// pixels (coverage image, distance image, per-pixel outputs), 8x8 coverage
+// tiles and boundary-grid cells start at frame * (P, T, G) + the camera's
+// offset in the frame.  When every camera has the same size the layout has
+// n_cam = 1 (each view is a "frame" of one camera), so any number of cameras
+// works; mixed sizes take up to kMaxLayoutCams cameras.  Passed by value.
+constexpr int kMaxLayoutCams = 32;
+struct CamImg {
+    int W, H;          // image size (the distance image's U, V)
+    int tiles_x;       // 8x8 coverage tiles per row
+    int gx, gy;        // boundary-grid cells (edge: the search radius)
+    long long pix;     // first pixel in the frame
+    long long tile;    // first coverage tile in the frame
+    long long cell;    // first grid cell in the frame
+};
+struct ImgLayout {
+    int n_cam;
+    long long P, T, G;  // pixels, coverage tiles, grid cells of a frame
+    FastDiv fd_T;       // division by T
+    CamImg cam[kMaxLayoutCams];
+};
+struct ViewImg {       // one view's image in the call's buffers
+    int W, H, tiles_x, gx, gy;
+    long long pix, tile, cell;
+};
+
+__device__ __forceinline__ ViewImg view_img(const ImgLayout& L, int view) {
+    const int b = L.n_cam == 1 ? view : view / L.n_cam, c = view - b * L.n_cam;
+    const CamImg& k = L.cam[c];
+    ViewImg v;
+    v.W = k.W;
+    v.H = k.H;
+    v.tiles_x = k.tiles_x;
+    v.gx = k.gx;
+    v.gy = k.gy;
+    v.pix = b * L.P + k.pix;
+    v.tile = b * L.T + k.tile;
+    v.cell = b * L.G + k.cell;
+    return v;
+}
+
+// the view of a coverage tile of the call (< 2^31 tiles), and the tile's index in the view
+__device__ __forceinline__ int view_of_tile(const ImgLayout& L, long long key, int& tile) {
+    const unsigned b = L.fd_T.div((unsigned)key);
+    const long long r = key - (long long)b * L.T;
+    int c = 0;
+    while (c + 1 < L.n_cam && L.cam[c + 1].tile <= r) ++c;
+    tile = (int)(r - L.cam[c].tile);
+    return (int)b * L.n_cam + c;
+}
+
 __device__ __forceinline__ void cover_tri(int view, int f, int N, int W, int H, const int* __restrict__ faces,
                                           const float2* __restrict__ p2d, CoverTri& t) {
     const float2* P = p2d + (long long)view * N;
@@ -251,23 +303,21 @@ __device__ __forceinline__ bool cover_record_test(const CovTileTri& e, int px, i
 }
 
 struct CovBins {
-    int tiles_x, T;
-    int* count;        // [V*T]
-    int* bins;         // [V*T*kCovCap]
+    int* count;        // [tiles of the call]
+    int* bins;         // [tiles of the call * kCovCap]
     CovTileTri* rec;   // [V*F]
-    unsigned char* cover;
-    const unsigned char* need;  // [V*T] tiles with a pixel still open (NULL: every tile)
-    int W, H;
+    unsigned char* cover;       // coverage image, the layout's pixels
+    const unsigned char* need;  // [tiles of the call] tiles with a pixel still open (NULL: every tile)
 };
 
 // the pixels of one tile that a triangle covers, written at once (a pair
 // beyond the tile's bin capacity)
-__device__ void cov_sweep(const CovBins& cb, int view, int tile, const CovTileTri& e) {
-    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
-    unsigned char* img = cb.cover + (long long)view * cb.H * cb.W;
-    for (int v = ty * kCovTile; v < min(ty * kCovTile + kCovTile, cb.H); ++v)
-        for (int u = tx * kCovTile; u < min(tx * kCovTile + kCovTile, cb.W); ++u)
-            if (cover_record_test(e, u, v)) img[(long long)v * cb.W + u] = 1;
+__device__ void cov_sweep(const CovBins& cb, const ViewImg& vi, int tile, const CovTileTri& e) {
+    const int ty = tile / vi.tiles_x, tx = tile - ty * vi.tiles_x;
+    unsigned char* img = cb.cover + vi.pix;
+    for (int v = ty * kCovTile; v < min(ty * kCovTile + kCovTile, vi.H); ++v)
+        for (int u = tx * kCovTile; u < min(tx * kCovTile + kCovTile, vi.W); ++u)
+            if (cover_record_test(e, u, v)) img[(long long)v * vi.W + u] = 1;
 }
 
 // Coverage from a per-pixel face hint (a renderer face buffer of the same
@@ -278,24 +328,27 @@ __device__ void cov_sweep(const CovBins& cb, int view, int tile, const CovTileTr
 // one warp per (view, 8x8 tile), two pixels per lane
 __global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys, const int* __restrict__ faces,
                                                   const float2* __restrict__ p2d, const int* __restrict__ hint,
-                                                  CovBins cb, unsigned char* __restrict__ need) {
+                                                  CovBins cb, unsigned char* __restrict__ need,
+                                                  const __grid_constant__ ImgLayout L) {
     const long long key = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (key >= n_keys) return;  // warp-uniform
-    const int view = (int)(key / cb.T), tile = (int)(key - (long long)view * cb.T);
-    const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+    int tile;
+    const int view = view_of_tile(L, key, tile);
+    const ViewImg vi = view_img(L, view);
+    const int ty = tile / vi.tiles_x, tx = tile - ty * vi.tiles_x;
     bool covered = true;
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int q = lane + 32 * h;
         const int px = tx * kCovTile + q % kCovTile, py = ty * kCovTile + q / kCovTile;
-        if (px >= cb.W || py >= cb.H) continue;
-        const long long pix = ((long long)view * cb.H + py) * cb.W + px;
+        if (px >= vi.W || py >= vi.H) continue;
+        const long long pix = vi.pix + (long long)py * vi.W + px;
         const int f = hint[pix];
         bool c = false;
         if (f >= 0 && f < F) {
             CoverTri t;
-            cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
+            cover_tri(view, f, N, vi.W, vi.H, faces, p2d, t);
             c = px >= t.x0 && px <= t.x1 && py >= t.y0 && py <= t.y1 && cover_test(t, px + 0.5f, py + 0.5f);
         }
         cb.cover[pix] = c ? 1 : 0;
@@ -310,12 +363,13 @@ __global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys
 // sharing one counter atomic; larger boxes are taken by the whole warp, a
 // tile per lane, reading the record back from global memory.
 __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
-                          CovBins cb) {
+                          CovBins cb, const __grid_constant__ ImgLayout L) {
     // grid (triangle blocks, views): no 64-bit division per thread
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
     const unsigned lane = threadIdx.x & 31;
     const bool live = fi < F;
     const int view = blockIdx.y;
+    const ViewImg vi = view_img(L, view);
     const long long i = (long long)view * F + fi;
     int f = 0;
     CoverTri t;
@@ -326,7 +380,7 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
     Footprint fp;
     if (live) {
         f = fi;
-        cover_tri(view, f, N, cb.W, cb.H, faces, p2d, t);
+        cover_tri(view, f, N, vi.W, vi.H, faces, p2d, t);
     }
     bool nonempty = live && t.x1 >= t.x0 && t.y1 >= t.y0;
     const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
@@ -335,14 +389,14 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
     if (cb.need && nt > 0 && nt <= kCovSmall) {  // a small box whose tiles are all covered already needs nothing
         bool any = false;
         for (int k = 0; k < nt; ++k)
-            any = any || cb.need[(long long)view * cb.T + (ty0 + k / ntx) * cb.tiles_x + tx0 + k % ntx];
+            any = any || cb.need[vi.tile + (ty0 + k / ntx) * vi.tiles_x + tx0 + k % ntx];
         if (!any) {
             nonempty = false;
             nt = 0;
         }
     }
     if (nonempty) {
-        fp = cover_footprint(t, cb.W, cb.H);
+        fp = cover_footprint(t, vi.W, vi.H);
         cb.rec[i] = cover_record(t, fp);
     }
     const bool big = nt > kCovSmall;
@@ -358,9 +412,9 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
             const int tx = tx0 + k % ntx, ty = ty0 + k / ntx;
             act = nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
                                                 max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1));
-            tile = ty * cb.tiles_x + tx;
-            if (act && cb.need && !cb.need[(long long)view * cb.T + tile]) act = false;
-            if (act) key = (long long)view * cb.T + tile;
+            tile = ty * vi.tiles_x + tx;
+            if (act && cb.need && !cb.need[vi.tile + tile]) act = false;
+            if (act) key = vi.tile + tile;
         }
         const unsigned same = __match_any_sync(0xffffffffu, key);
         if (!act) continue;
@@ -373,7 +427,7 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
         if (slot < kCovCap)
             cb.bins[key * kCovCap + slot] = f;
         else
-            cov_sweep(cb, view, tile, cb.rec[i]);
+            cov_sweep(cb, vi, tile, cb.rec[i]);
     }
     __syncwarp();  // the records of big triangles are read back by the other lanes
     unsigned pending = __ballot_sync(0xffffffffu, big);
@@ -381,6 +435,7 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
         const int src = __ffs(pending) - 1;
         pending &= pending - 1;
         const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
+        const ViewImg qi = view_img(L, qv);
         const CovTileTri q = cb.rec[(long long)qv * F + qf];
         const Footprint qfp = record_footprint(q);
         const int qx0 = q.bb.x & 0xffff, qx1 = q.bb.x >> 16, qy0 = q.bb.y & 0xffff, qy1 = q.bb.y >> 16;
@@ -391,14 +446,14 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
             if (!footprint_overlaps(qfp, max(tx * kCovTile, qx0), min(tx * kCovTile + kCovTile - 1, qx1),
                                     max(ty * kCovTile, qy0), min(ty * kCovTile + kCovTile - 1, qy1)))
                 continue;
-            const int tile = ty * cb.tiles_x + tx;
-            const long long key = (long long)qv * cb.T + tile;
+            const int tile = ty * qi.tiles_x + tx;
+            const long long key = qi.tile + tile;
             if (cb.need && !cb.need[key]) continue;
             const int slot = atomicAdd(cb.count + key, 1);
             if (slot < kCovCap)
                 cb.bins[key * kCovCap + slot] = qf;
             else
-                cov_sweep(cb, qv, tile, q);
+                cov_sweep(cb, qi, tile, q);
         }
     }
 }
@@ -408,16 +463,19 @@ __global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const i
 // the tile at the chunk after which all its pixels are covered.  Tiles
 // without entries (most of them when a coverage hint was given) cost one
 // count load instead of a CTA launch each.
-__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long long n_keys, CovBins cb) {
+__global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long long n_keys, CovBins cb,
+                                                                  const __grid_constant__ ImgLayout L) {
     __shared__ CovTileTri s_t[kCovTile * kCovTile];
     for (long long key = blockIdx.x; key < n_keys; key += gridDim.x) {
         const int n = min(cb.count[key], kCovCap);
         if (n == 0) continue;  // CTA-uniform
-        const int view = (int)(key / cb.T), tile = (int)(key - (long long)view * cb.T);
-        const int tx = tile % cb.tiles_x, ty = tile / cb.tiles_x;
+        int tile;
+        const int view = view_of_tile(L, key, tile);
+        const ViewImg vi = view_img(L, view);
+        const int ty = tile / vi.tiles_x, tx = tile - ty * vi.tiles_x;
         const int px = tx * kCovTile + (int)threadIdx.x % kCovTile, py = ty * kCovTile + (int)threadIdx.x / kCovTile;
-        const bool valid = px < cb.W && py < cb.H;
-        unsigned char* pix = cb.cover + ((long long)view * cb.H + py) * cb.W + px;
+        const bool valid = px < vi.W && py < vi.H;
+        unsigned char* pix = cb.cover + vi.pix + (long long)py * vi.W + px;
         bool covered = !valid || *pix;
         const CovTileTri* R = cb.rec + (long long)view * F;
         // every chunk starts with a barrier (so does the next tile: the staged
@@ -434,15 +492,17 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long lon
 }
 
 // boundary test of k_boundary against the coverage image instead of a face buffer
-__global__ void k_boundary_cover(int B, int C, int N, int W, int H, const float* __restrict__ p2d,
-                                 const unsigned char* __restrict__ cover, unsigned char* __restrict__ out) {
+__global__ void k_boundary_cover(int B, int C, int N, const __grid_constant__ ImgLayout L,
+                                 const float* __restrict__ p2d, const unsigned char* __restrict__ cover,
+                                 unsigned char* __restrict__ out) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)B * C * N) return;
-    const long long view = i / N;
+    const ViewImg vi = view_img(L, (int)(i / N));
+    const int W = vi.W, H = vi.H;
     const int u = (int)p2d[2 * i], v = (int)p2d[2 * i + 1];
     unsigned char r = 0;
     if (u - 1 >= 0 && u + 1 < W && v - 1 >= 0 && v + 1 < H) {
-        const unsigned char* img = cover + view * H * W;
+        const unsigned char* img = cover + vi.pix;
         for (int c = u - 1; c <= u + 1; ++c)
             for (int rr = v - 1; rr <= v + 1; ++rr)
                 if (!img[(long long)rr * W + c]) r = 1;
@@ -457,13 +517,15 @@ __device__ __forceinline__ float dt_decode(unsigned char x) {
 }
 
 // model -> data term per (frame, view, vertex) (MultiViewSilhouetteLossGPUOp.cu:11-138)
-__global__ void k_sil_points(int B, int C, int N, int U, int V, const float* __restrict__ p2d,
+__global__ void k_sil_points(int B, int C, int N, const __grid_constant__ ImgLayout L, const float* __restrict__ p2d,
                              const float* __restrict__ n2d, const unsigned char* __restrict__ isb,
                              const unsigned char* __restrict__ dt, const float* __restrict__ crops,
                              float* __restrict__ residual, float* __restrict__ dtgrad) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)B * C * N) return;
     const long long view = i / N;
+    const ViewImg vi = view_img(L, (int)view);
+    const int U = vi.W;
     const float* cr = crops + view * 7;
     const float2 border = make_float2(cr[0], cr[1]);
     const float scale = cr[2];
@@ -478,7 +540,7 @@ __global__ void k_sil_points(int B, int C, int N, int U, int V, const float* __r
     }
     const float fx = (pu - cmin.x) / scale + border.x, fy = (pv - cmin.y) / scale + border.y;
     const int x = (int)fx, y = (int)fy;
-    const unsigned char* D = dt + view * (long long)U * V;
+    const unsigned char* D = dt + vi.pix;
     float val = dt_decode(D[(long long)y * U + x]);
     const float f00 = dt_decode(D[(long long)(y - 1) * U + (x - 1)]), f01 = dt_decode(D[(long long)(y - 1) * U + x]);
     const float f02 = dt_decode(D[(long long)(y - 1) * U + (x + 1)]), f10 = dt_decode(D[(long long)y * U + (x - 1)]);
@@ -501,17 +563,16 @@ __global__ void k_sil_points(int B, int C, int N, int U, int V, const float* __r
     residual[i] = val * (1.f / (255.f));
 }
 
-// grid of boundary vertices per view: cell edge = search radius 30 * scale
+// grid of boundary vertices per view: cell edge = search radius 30 * scale;
+// a view's cells start at its layout cell offset
 struct SilGrid {
-    int gx, gy;       // cells per view
-    int* count;       // [views * cells]
-    int* start;       // [views * cells + 1] per view prefix
-    int* cursor;      // [views * cells]
+    int* count;       // [cells of the call]
+    int* start;       // [cells of the call + 1] per view prefix
+    int* cursor;      // [cells of the call]
     int* items;       // [views * N]
 };
 
-__device__ __forceinline__ bool grid_cell(const float* cr, int U, int V, int gx, int gy, float px, float py, int& cx,
-                                          int& cy) {
+__device__ __forceinline__ bool grid_cell(const float* cr, int gx, int gy, float px, float py, int& cx, int& cy) {
     // image-space box of the distance image, extended by one radius
     const float scale = cr[2], R = 30.f * scale;
     const float x0 = (0.f - cr[0]) * scale + cr[3] - R, y0 = (0.f - cr[1]) * scale + cr[4] - R;
@@ -522,23 +583,25 @@ __device__ __forceinline__ bool grid_cell(const float* cr, int U, int V, int gx,
     return true;
 }
 
-__global__ void k_grid_count(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
-                             const unsigned char* __restrict__ isb, const float* __restrict__ crops) {
+__global__ void k_grid_count(int B, int C, int N, const __grid_constant__ ImgLayout L, SilGrid g,
+                             const float* __restrict__ p2d, const unsigned char* __restrict__ isb,
+                             const float* __restrict__ crops) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)B * C * N || !isb[i]) return;
     const long long view = i / N;
+    const ViewImg vi = view_img(L, (int)view);
     int cx, cy;
-    if (!grid_cell(crops + view * 7, U, V, g.gx, g.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
-    atomicAdd(&g.count[view * g.gx * g.gy + cy * g.gx + cx], 1);
+    if (!grid_cell(crops + view * 7, vi.gx, vi.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
+    atomicAdd(&g.count[vi.cell + cy * vi.gx + cx], 1);
 }
 
 // exclusive scan of the cell counts, one CTA per view
-__global__ void k_grid_scan(SilGrid g) {
-    const int view = blockIdx.x;
-    const int cells = g.gx * g.gy;
+__global__ void k_grid_scan(SilGrid g, const __grid_constant__ ImgLayout L) {
+    const ViewImg vi = view_img(L, blockIdx.x);
+    const int cells = vi.gx * vi.gy;
     __shared__ int s_part[1024];
-    const int* cnt = g.count + (long long)view * cells;
-    int* st = g.start + (long long)view * cells;
+    const int* cnt = g.count + vi.cell;
+    int* st = g.start + vi.cell;
     // each thread scans a contiguous chunk
     const int per = (cells + blockDim.x - 1) / blockDim.x;
     const int lo = threadIdx.x * per, hi = min(cells, lo + per);
@@ -555,19 +618,21 @@ __global__ void k_grid_scan(SilGrid g) {
     int run = s_part[threadIdx.x] - sum;
     for (int c = lo; c < hi; ++c) {
         st[c] = run;
-        g.cursor[(long long)view * cells + c] = run;
+        g.cursor[vi.cell + c] = run;
         run += cnt[c];
     }
 }
 
-__global__ void k_grid_fill(int B, int C, int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
-                            const unsigned char* __restrict__ isb, const float* __restrict__ crops) {
+__global__ void k_grid_fill(int B, int C, int N, const __grid_constant__ ImgLayout L, SilGrid g,
+                            const float* __restrict__ p2d, const unsigned char* __restrict__ isb,
+                            const float* __restrict__ crops) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)B * C * N || !isb[i]) return;
     const long long view = i / N;
+    const ViewImg vi = view_img(L, (int)view);
     int cx, cy;
-    if (!grid_cell(crops + view * 7, U, V, g.gx, g.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
-    const int slot = atomicAdd(&g.cursor[view * g.gx * g.gy + cy * g.gx + cx], 1);
+    if (!grid_cell(crops + view * 7, vi.gx, vi.gy, p2d[2 * i], p2d[2 * i + 1], cx, cy)) return;
+    const int slot = atomicAdd(&g.cursor[vi.cell + cy * vi.gx + cx], 1);
     g.items[view * (long long)N + slot] = (int)(i % N);
 }
 
@@ -576,9 +641,11 @@ __global__ void k_grid_fill(int B, int C, int N, int U, int V, SilGrid g, const 
 // a boundary pixel (DT value 127 with at least 4 boundary pixels in its 5x5
 // window) takes the nearest boundary vertex within 30 * scale px (the
 // minimum (distance, id): the reference's first strictly smaller one).
-__device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N, int U, int V, const SilGrid& g,
-                                          const float* __restrict__ p2d, const unsigned char* __restrict__ D,
-                                          const float* __restrict__ crops, float& r0, float& r1, float& cl) {
+__device__ __forceinline__ void sil_pixel(long long view, const ViewImg& vi, int p, int dval, int N,
+                                          const SilGrid& g, const float* __restrict__ p2d,
+                                          const unsigned char* __restrict__ D, const float* __restrict__ crops,
+                                          float& r0, float& r1, float& cl) {
+    const int U = vi.W, V = vi.H;
     r0 = 0.f;
     r1 = 0.f;
     cl = -1.f;
@@ -597,13 +664,12 @@ __device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N
     float bestd = 30.f * scale;
     int best = -1;
     int cx, cy;
-    const int cells = g.gx * g.gy;
-    if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
-        for (int yy = max(cy - 1, 0); yy <= min(cy + 1, g.gy - 1); ++yy)
-            for (int xx = max(cx - 1, 0); xx <= min(cx + 1, g.gx - 1); ++xx) {
-                const int cell = yy * g.gx + xx;
-                const int s0 = g.start[view * cells + cell];
-                const int n = g.count[view * cells + cell];
+    if (grid_cell(cr, vi.gx, vi.gy, imgpos.x, imgpos.y, cx, cy)) {
+        for (int yy = max(cy - 1, 0); yy <= min(cy + 1, vi.gy - 1); ++yy)
+            for (int xx = max(cx - 1, 0); xx <= min(cx + 1, vi.gx - 1); ++xx) {
+                const long long cell = vi.cell + yy * vi.gx + xx;
+                const int s0 = g.start[cell];
+                const int n = g.count[cell];
                 for (int q = 0; q < n; ++q) {
                     const int v = g.items[view * (long long)N + s0 + q];
                     const float* pp = p2d + (view * (long long)N + v) * 2;
@@ -630,10 +696,11 @@ __device__ __forceinline__ void sil_pixel(long long view, int p, int dval, int N
 // vertices (accept dist < 30 * scale, then the smaller id on equal distance),
 // so the lane results merge into the same lexicographic minimum of
 // (distance, vertex) as the one-thread loop.
-__device__ __forceinline__ void sil_pixel_warp(long long view, int p, int N, int U, int V, const SilGrid& g,
+__device__ __forceinline__ void sil_pixel_warp(long long view, const ViewImg& vi, int p, int N, const SilGrid& g,
                                                const float* __restrict__ p2d, const unsigned char* __restrict__ D,
                                                const float* __restrict__ crops, int lane, float& r0, float& r1,
                                                float& cl) {
+    const int U = vi.W, V = vi.H;
     r0 = 0.f;
     r1 = 0.f;
     cl = -1.f;
@@ -650,18 +717,17 @@ __device__ __forceinline__ void sil_pixel_warp(long long view, int p, int N, int
     float bestd = 30.f * scale;
     int best = -1;
     int cx, cy;
-    const int cells = g.gx * g.gy;
-    if (grid_cell(cr, U, V, g.gx, g.gy, imgpos.x, imgpos.y, cx, cy)) {
+    if (grid_cell(cr, vi.gx, vi.gy, imgpos.x, imgpos.y, cx, cy)) {
         // lanes 0-8 load the 3x3 cells' ranges at once; the cells' vertices
         // are then dealt to the lanes through an inclusive prefix of the
         // counts, so the loads do not chain from cell to cell
         int cs = 0, cn = 0;
         if (lane < 9) {
             const int yy = cy - 1 + lane / 3, xx = cx - 1 + lane % 3;
-            if (yy >= 0 && yy < g.gy && xx >= 0 && xx < g.gx) {
-                const int cell = yy * g.gx + xx;
-                cs = g.start[view * cells + cell];
-                cn = g.count[view * cells + cell];
+            if (yy >= 0 && yy < vi.gy && xx >= 0 && xx < vi.gx) {
+                const long long cell = vi.cell + yy * vi.gx + xx;
+                cs = g.start[cell];
+                cn = g.count[cell];
             }
         }
         int pre = cn;
@@ -714,14 +780,17 @@ __device__ __forceinline__ void sil_pixel_warp(long long view, int p, int N, int
 // write their zero outputs; in the vec path the warp takes its boundary
 // pixels one at a time, all lanes together (sil_pixel_warp), instead of
 // leaving one lane to search while the others wait.
-__global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, int U, int V, SilGrid g, const float* __restrict__ p2d,
-                             const unsigned char* __restrict__ dt, const float* __restrict__ crops,
-                             float* __restrict__ residual1, float* __restrict__ closest, int vec) {
-    const int P = U * V;
-    const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+__global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_constant__ ImgLayout L, SilGrid g,
+                             const float* __restrict__ p2d, const unsigned char* __restrict__ dt,
+                             const float* __restrict__ crops, float* __restrict__ residual1,
+                             float* __restrict__ closest, int vec) {
     const long long view = blockIdx.y;
-    const unsigned char* D = dt + view * (long long)P;
-    const long long i0 = view * (long long)P + p0;
+    const ViewImg vi = view_img(L, (int)view);
+    const int P = vi.W * vi.H;
+    const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (4 * (int)(blockIdx.x * blockDim.x) >= P) return;  // blocks past a smaller view's pixels (CTA-uniform)
+    const unsigned char* D = dt + vi.pix;
+    const long long i0 = vi.pix + p0;
     if (vec) {  // P % 4 == 0 and aligned buffers: all four pixels of an active thread exist
         const bool active = p0 < P;  // no early exit: the warp's lanes all take part below
         int dv[4] = {0, 0, 0, 0};
@@ -750,7 +819,7 @@ __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, int U, int V, SilG
             if (lane == src) mine &= mine - 1;
             any = __ballot_sync(0xffffffffu, mine != 0);
             float a0, a1, cl;
-            sil_pixel_warp(view, p, N, U, V, g, p2d, D, crops, lane, a0, a1, cl);
+            sil_pixel_warp(view, vi, p, N, g, p2d, D, crops, lane, a0, a1, cl);
             if (lane == src) {
 #pragma unroll
                 for (int kk = 0; kk < 4; ++kk)
@@ -771,7 +840,7 @@ __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, int U, int V, SilG
     if (p0 >= P) return;
     for (int k = 0; k < 4 && p0 + k < P; ++k) {
         float r0, r1, cl;
-        sil_pixel(view, p0 + k, D[p0 + k], N, U, V, g, p2d, D, crops, r0, r1, cl);
+        sil_pixel(view, vi, p0 + k, D[p0 + k], N, g, p2d, D, crops, r0, r1, cl);
         residual1[2 * (i0 + k)] = r0;
         residual1[2 * (i0 + k) + 1] = r1;
         closest[i0 + k] = cl;
@@ -789,14 +858,15 @@ __global__ void k_sil_grad_points(long long n, const float* __restrict__ dtgrad,
 // four pixels per thread on a (pixel block, view) grid: one 16-byte load of
 // closest_vertex_id when the buffer allows (vec); the rare boundary pixels
 // scatter their residual gradient to the closest vertex
-__global__ void k_sil_grad_pixels(int N, int U, int V, const float* __restrict__ g1,
+__global__ void k_sil_grad_pixels(int N, const __grid_constant__ ImgLayout L, const float* __restrict__ g1,
                                   const float* __restrict__ closest, const float* __restrict__ crops,
                                   float* __restrict__ out, int vec) {
-    const int P = U * V;
+    const long long view = blockIdx.y;
+    const ViewImg vi = view_img(L, (int)view);
+    const int P = vi.W * vi.H;
     const int p0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (p0 >= P) return;
-    const long long view = blockIdx.y;
-    const long long i0 = view * (long long)P + p0;
+    const long long i0 = vi.pix + p0;
     float cl[4];
     if (vec) {
         const float4 c4 = *reinterpret_cast<const float4*>(closest + i0);
@@ -873,6 +943,73 @@ extern "C" hc_status hc_projected_mesh_boundary(void* stream, int32_t batch, int
     return HC_OK;
 }
 
+namespace {
+
+// The image layout of a call from its cameras' sizes (widths / heights [C],
+// host arrays).  Cameras of one size give the one-camera layout.
+hc_status make_layout(int32_t batch, int32_t n_cameras, const int32_t* widths, const int32_t* heights, ImgLayout& L,
+                      long long& views) {
+    HC_REQUIRE(batch > 0 && n_cameras > 0, "bad sizes");
+    HC_REQUIRE(widths && heights, "NULL image sizes");
+    bool uniform = true;
+    for (int c = 0; c < n_cameras; ++c) {
+        HC_REQUIRE(widths[c] > 2 && heights[c] > 2 && widths[c] < 32768 && heights[c] < 32768,
+                   "bad image size %dx%d of camera %d", widths[c], heights[c], c);
+        uniform = uniform && widths[c] == widths[0] && heights[c] == heights[0];
+    }
+    views = (long long)batch * n_cameras;
+    HC_REQUIRE(views <= 65535, "too many views in one call (%lld)", views);
+    const int nc = uniform ? 1 : n_cameras;
+    HC_REQUIRE(nc <= kMaxLayoutCams, "at most %d cameras of different image sizes in one call (got %d)",
+               kMaxLayoutCams, n_cameras);
+    memset(&L, 0, sizeof(L));
+    L.n_cam = nc;
+    long long pix = 0, tile = 0, cell = 0;
+    for (int c = 0; c < nc; ++c) {
+        CamImg& k = L.cam[c];
+        k.W = widths[c];
+        k.H = heights[c];
+        k.tiles_x = div_up(k.W, kCovTile);
+        k.gx = div_up(k.W, 30) + 3;
+        k.gy = div_up(k.H, 30) + 3;
+        k.pix = pix;
+        k.tile = tile;
+        k.cell = cell;
+        HC_REQUIRE((long long)k.W * k.H < (1ll << 31), "too many pixels in one view");
+        pix += (long long)k.W * k.H;
+        tile += (long long)k.tiles_x * div_up(k.H, kCovTile);
+        cell += (long long)k.gx * k.gy;
+    }
+    L.P = pix;
+    L.T = tile;
+    L.G = cell;
+    HC_REQUIRE(views / nc * L.T < (1ll << 31), "too many coverage tiles in one call");
+    L.fd_T = FastDiv((unsigned)L.T);
+    return HC_OK;
+}
+
+// widths / heights of n cameras of one size
+struct SameSize {
+    std::vector<int32_t> w, h;
+    SameSize(int n, int32_t width, int32_t height) : w((size_t)std::max(n, 0), width), h((size_t)std::max(n, 0), height) {}
+};
+
+// the layout's largest view, in pixels (the per-pixel grids span it)
+long long max_view_pixels(const ImgLayout& L) {
+    long long m = 0;
+    for (int c = 0; c < L.n_cam; ++c) m = std::max(m, (long long)L.cam[c].W * L.cam[c].H);
+    return m;
+}
+
+// every view's pixel count a multiple of 4 (so every view starts 4-aligned)
+bool pixels_by_four(const ImgLayout& L) {
+    for (int c = 0; c < L.n_cam; ++c)
+        if (((long long)L.cam[c].W * L.cam[c].H) % 4 != 0) return false;
+    return true;
+}
+
+}  // namespace
+
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
     DevBuf faces, p2d, cover, count, bins, rec, need;
@@ -910,32 +1047,46 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     return HC_OK;
 }
 
-extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch, int32_t n_cameras, int32_t width,
-                                              int32_t height) {
-    clear_error();
-    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 0 && height > 0, "bad sizes");
-    const size_t views = (size_t)batch * n_cameras;
-    HC_TRY(h->p2d.ensure(sizeof(float) * 2 * views * h->N));
-    HC_TRY(h->cover.ensure(views * (size_t)width * height));
-    const size_t tiles = (size_t)div_up(width, kCovTile) * div_up(height, kCovTile);
-    HC_TRY(h->count.ensure(sizeof(int) * views * tiles));
-    HC_TRY(h->bins.ensure(sizeof(int) * views * tiles * kCovCap));
-    HC_TRY(h->rec.ensure(sizeof(CovTileTri) * views * h->F));
-    HC_TRY(h->need.ensure(views * tiles));
+static hc_status mesh_boundary_reserve_layout(hc_mesh_boundary h, long long views, const ImgLayout& L) {
+    const size_t frames = (size_t)(views / L.n_cam);
+    HC_TRY(h->p2d.ensure(sizeof(float) * 2 * (size_t)views * h->N));
+    HC_TRY(h->cover.ensure(frames * (size_t)L.P));
+    HC_TRY(h->count.ensure(sizeof(int) * frames * (size_t)L.T));
+    HC_TRY(h->bins.ensure(sizeof(int) * frames * (size_t)L.T * kCovCap));
+    HC_TRY(h->rec.ensure(sizeof(CovTileTri) * (size_t)views * h->F));
+    HC_TRY(h->need.ensure(frames * (size_t)L.T));
     return HC_OK;
 }
 
+extern "C" hc_status hc_mesh_boundary_reserve_sized(hc_mesh_boundary h, int32_t batch, int32_t n_cameras,
+                                                    const int32_t* widths, const int32_t* heights) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    ImgLayout L;
+    long long views = 0;
+    HC_TRY(make_layout(batch, n_cameras, widths, heights, L, views));
+    return mesh_boundary_reserve_layout(h, views, L);
+}
+
+extern "C" hc_status hc_mesh_boundary_reserve(hc_mesh_boundary h, int32_t batch, int32_t n_cameras, int32_t width,
+                                              int32_t height) {
+    const SameSize sz(n_cameras, width, height);
+    return hc_mesh_boundary_reserve_sized(h, batch, n_cameras, sz.w.data(), sz.h.data());
+}
+
 static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
-                                   int32_t width, int32_t height, const float* points_global_space,
+                                   const int32_t* widths, const int32_t* heights, const float* points_global_space,
                                    const float* extrinsics, const float* intrinsics, const float* points_image_space,
                                    const int32_t* face_hint, uint8_t* is_boundary) {
-    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && width > 2 && height > 2 && width < 32768 && height < 32768,
-               "bad sizes");
+    HC_REQUIRE(h, "invalid handle");
     HC_REQUIRE(is_boundary && (points_image_space || (points_global_space && extrinsics && intrinsics)),
                "NULL pointer");
-    HC_TRY(hc_mesh_boundary_reserve(h, batch, n_cameras, width, height));
+    ImgLayout L;
+    long long views = 0;
+    HC_TRY(make_layout(batch, n_cameras, widths, heights, L, views));
+    HC_TRY(mesh_boundary_reserve_layout(h, views, L));
     cudaStream_t s = (cudaStream_t)stream;
-    const long long nv = (long long)batch * n_cameras * h->N;
+    const long long nv = views * h->N;
     const float* p2d = points_image_space;
     if (!p2d) {
         k_project<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, points_global_space, nullptr, extrinsics,
@@ -943,33 +1094,27 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
         HC_CHECK_LAUNCH();
         p2d = h->p2d.as<float>();
     }
-    const long long views = (long long)batch * n_cameras;
-    HC_REQUIRE(views <= 65535, "too many views in one call (%lld)", views);
+    const long long frames = views / L.n_cam;
+    const long long n_keys = frames * L.T;  // coverage tiles of the call
     CovBins cb;
-    cb.tiles_x = div_up(width, kCovTile);
-    cb.T = cb.tiles_x * div_up(height, kCovTile);
     cb.count = h->count.as<int>();
     cb.bins = h->bins.as<int>();
     cb.cover = h->cover.as<unsigned char>();
     cb.rec = h->rec.as<CovTileTri>();
     cb.need = nullptr;
-    cb.W = width;
-    cb.H = height;
     if (face_hint) {  // writes every pixel of the coverage image and the per-tile flags
-        const long long n_keys = views * cb.T;
         k_cov_hint<<<div_up(n_keys * 32, 256), 256, 0, s>>>(h->N, h->F, n_keys, h->faces.as<int>(),
                                                              reinterpret_cast<const float2*>(p2d), face_hint, cb,
-                                                             h->need.as<unsigned char>());
+                                                             h->need.as<unsigned char>(), L);
         HC_CHECK_LAUNCH();
         cb.need = h->need.as<unsigned char>();
     } else {
-        HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)views * width * height, s));
+        HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)(frames * L.P), s));
     }
-    HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)views * cb.T, s));
+    HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)n_keys, s));
     k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
-                                                                       reinterpret_cast<const float2*>(p2d), cb);
+                                                                       reinterpret_cast<const float2*>(p2d), cb, L);
     HC_CHECK_LAUNCH();
-    const long long n_keys = views * cb.T;
     {
         // persistent: as many CTAs as are resident at once (a second partial
         // wave would run its strided keys after everything else)
@@ -980,11 +1125,11 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
             per_sm <= 0)
             per_sm = 1;
         const long long grid = std::max<long long>(1, std::min<long long>(n_keys, (long long)sms * per_sm));
-        k_cov_tile<<<(unsigned)grid, kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb);
+        k_cov_tile<<<(unsigned)grid, kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb, L);
     }
     HC_CHECK_LAUNCH();
-    k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, width, height, p2d,
-                                                     h->cover.as<unsigned char>(), is_boundary);
+    k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, L, p2d, h->cover.as<unsigned char>(),
+                                                     is_boundary);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
@@ -994,8 +1139,9 @@ extern "C" hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, 
                                               const float* extrinsics, const float* intrinsics,
                                               const float* points_image_space, uint8_t* is_boundary) {
     clear_error();
-    return mesh_boundary_run(h, stream, batch, n_cameras, width, height, points_global_space, extrinsics, intrinsics,
-                             points_image_space, nullptr, is_boundary);
+    const SameSize sz(n_cameras, width, height);
+    return mesh_boundary_run(h, stream, batch, n_cameras, sz.w.data(), sz.h.data(), points_global_space, extrinsics,
+                             intrinsics, points_image_space, nullptr, is_boundary);
 }
 
 extern "C" hc_status hc_mesh_boundary_forward_hinted(hc_mesh_boundary h, void* stream, int32_t batch,
@@ -1005,8 +1151,19 @@ extern "C" hc_status hc_mesh_boundary_forward_hinted(hc_mesh_boundary h, void* s
                                                      const int32_t* face_hint, uint8_t* is_boundary) {
     clear_error();
     HC_REQUIRE(face_hint, "face_hint is NULL");
-    return mesh_boundary_run(h, stream, batch, n_cameras, width, height, points_global_space, extrinsics, intrinsics,
-                             points_image_space, face_hint, is_boundary);
+    const SameSize sz(n_cameras, width, height);
+    return mesh_boundary_run(h, stream, batch, n_cameras, sz.w.data(), sz.h.data(), points_global_space, extrinsics,
+                             intrinsics, points_image_space, face_hint, is_boundary);
+}
+
+extern "C" hc_status hc_mesh_boundary_forward_sized(hc_mesh_boundary h, void* stream, int32_t batch,
+                                                    int32_t n_cameras, const int32_t* widths, const int32_t* heights,
+                                                    const float* points_global_space, const float* extrinsics,
+                                                    const float* intrinsics, const float* points_image_space,
+                                                    const int32_t* face_hint, uint8_t* is_boundary) {
+    clear_error();
+    return mesh_boundary_run(h, stream, batch, n_cameras, widths, heights, points_global_space, extrinsics,
+                             intrinsics, points_image_space, face_hint, is_boundary);
 }
 
 struct hc_silhouette_s {
@@ -1014,8 +1171,9 @@ struct hc_silhouette_s {
     size_t need = 0;
 };
 
-static size_t grid_bytes(long long views, int gx, int gy, int N) {
-    const long long cells = views * gx * gy;
+// grid scratch of a call: cell counts, starts (+1), cursors, and the boundary
+// vertices of every view
+static size_t grid_bytes(long long views, long long cells, int N) {
     return sizeof(int) * (size_t)(3 * cells + 1 + views * (long long)N);
 }
 
@@ -1034,80 +1192,126 @@ extern "C" hc_status hc_silhouette_destroy(hc_silhouette h) {
     return HC_OK;
 }
 
+extern "C" hc_status hc_silhouette_reserve_sized(hc_silhouette h, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                 const int32_t* widths, const int32_t* heights) {
+    clear_error();
+    HC_REQUIRE(h && n_points > 0, "bad sizes");
+    ImgLayout L;
+    long long views = 0;
+    HC_TRY(make_layout(batch, n_cameras, widths, heights, L, views));
+    HC_TRY(h->grid.ensure(grid_bytes(views, views / L.n_cam * L.G, n_points)));
+    return HC_OK;
+}
+
 extern "C" hc_status hc_silhouette_reserve(hc_silhouette h, int32_t batch, int32_t n_cameras, int32_t n_points,
                                            int32_t resolution_u, int32_t resolution_v) {
-    clear_error();
-    HC_REQUIRE(h && batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 0 && resolution_v > 0, "bad sizes");
-    const int gx = div_up(resolution_u, 30) + 3, gy = div_up(resolution_v, 30) + 3;
-    HC_TRY(h->grid.ensure(grid_bytes((long long)batch * n_cameras, gx, gy, n_points)));
-    return HC_OK;
+    const SameSize sz(n_cameras, resolution_u, resolution_v);
+    return hc_silhouette_reserve_sized(h, batch, n_cameras, n_points, sz.w.data(), sz.h.data());
 }
 
 namespace {
 
-// Argument checks shared by both silhouette forward entry points; sets the
-// boundary-vertex grid's cells per view and the scratch bytes the call needs.
-hc_status sil_forward_plan(int32_t batch, int32_t n_cameras, int32_t n_points, int32_t resolution_u,
-                           int32_t resolution_v, const float* points_image_space, const float* normals_image_space,
+// Argument checks shared by the silhouette forward entry points; sets the
+// layout and the grid scratch bytes the call needs.
+hc_status sil_forward_plan(int32_t batch, int32_t n_cameras, int32_t n_points, const int32_t* widths,
+                           const int32_t* heights, const float* points_image_space, const float* normals_image_space,
                            const uint8_t* is_boundary, const uint8_t* distance_transform_image,
                            const float* multi_view_crops, const float* mv_dt_residual, const float* mv_dt_residual_1,
-                           const float* dt_image_gradient, const float* closest_vertex_id, SilGrid& g,
+                           const float* dt_image_gradient, const float* closest_vertex_id, ImgLayout& L,
                            size_t& need) {
-    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 2 && resolution_v > 2, "bad sizes");
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0, "bad sizes");
     HC_REQUIRE(points_image_space && normals_image_space && is_boundary && distance_transform_image &&
                    multi_view_crops && mv_dt_residual && mv_dt_residual_1 && dt_image_gradient && closest_vertex_id,
                "NULL pointer");
-    const long long views = (long long)batch * n_cameras;
-    HC_REQUIRE(views <= 65535 && (long long)resolution_u * resolution_v < (1ll << 31),
-               "too many views or pixels in one call");
-    g.gx = div_up(resolution_u, 30) + 3;
-    g.gy = div_up(resolution_v, 30) + 3;
-    need = grid_bytes(views, g.gx, g.gy, n_points);
+    long long views = 0;
+    HC_TRY(make_layout(batch, n_cameras, widths, heights, L, views));
+    need = grid_bytes(views, views / L.n_cam * L.G, n_points);
     return HC_OK;
 }
 
 // The launches of one silhouette forward, the grid laid out in the scratch at
 // `base` (at least the planned bytes).  The cell counts are cleared first:
 // the scratch may hold a previous call's grid.
-hc_status sil_forward_run(cudaStream_t s, int* base, SilGrid g, int32_t batch, int32_t n_cameras, int32_t n_points,
-                          int32_t resolution_u, int32_t resolution_v, const float* points_image_space,
-                          const float* normals_image_space, const uint8_t* is_boundary,
-                          const uint8_t* distance_transform_image, const float* multi_view_crops,
-                          float* mv_dt_residual, float* mv_dt_residual_1, float* dt_image_gradient,
-                          float* closest_vertex_id) {
-    const int U = resolution_u, V = resolution_v, N = n_points;
+hc_status sil_forward_run(cudaStream_t s, int* base, const ImgLayout& L, int32_t batch, int32_t n_cameras,
+                          int32_t n_points, const float* points_image_space, const float* normals_image_space,
+                          const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                          const float* multi_view_crops, float* mv_dt_residual, float* mv_dt_residual_1,
+                          float* dt_image_gradient, float* closest_vertex_id) {
+    const int N = n_points;
     const long long views = (long long)batch * n_cameras;
-    const long long cells = views * g.gx * g.gy;
+    const long long cells = views / L.n_cam * L.G;
+    SilGrid g;
     g.count = base;
     g.start = base + cells;
     g.cursor = base + 2 * cells + 1;
     g.items = base + 3 * cells + 1;
     HC_CUDA(cudaMemsetAsync(g.count, 0, sizeof(int) * (size_t)cells, s));
     const long long np = views * N;
-    k_sil_points<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, points_image_space, normals_image_space,
+    k_sil_points<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, L, points_image_space, normals_image_space,
                                                  is_boundary, distance_transform_image, multi_view_crops,
                                                  mv_dt_residual, dt_image_gradient);
     HC_CHECK_LAUNCH();
-    k_grid_count<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+    k_grid_count<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, L, g, points_image_space, is_boundary,
                                                  multi_view_crops);
     HC_CHECK_LAUNCH();
-    k_grid_scan<<<(unsigned)views, 1024, 0, s>>>(g);
+    k_grid_scan<<<(unsigned)views, 1024, 0, s>>>(g, L);
     HC_CHECK_LAUNCH();
-    k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, U, V, g, points_image_space, is_boundary,
+    k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, L, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
     {
-        const int vec = ((long long)U * V) % 4 == 0 && ((uintptr_t)distance_transform_image & 3) == 0 &&
+        const int vec = pixels_by_four(L) && ((uintptr_t)distance_transform_image & 3) == 0 &&
                         ((uintptr_t)mv_dt_residual_1 & 15) == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
-        k_sil_pixels<<<dim3(div_up((long long)U * V, 4 * 256), (unsigned)views), 256, 0, s>>>(
-            N, U, V, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
+        k_sil_pixels<<<dim3(div_up(max_view_pixels(L), 4 * 256), (unsigned)views), 256, 0, s>>>(
+            N, L, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
             closest_vertex_id, vec);
     }
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
 
+hc_status sil_backward_run(cudaStream_t s, int32_t batch, int32_t n_cameras, int32_t n_points, const int32_t* widths,
+                           const int32_t* heights, const float* mv_dt_grad, const float* mv_dt_grad_1,
+                           const float* dt_image_grad, const float* closest_vertex_id, const float* multi_view_crops,
+                           float* points_image_space_grad) {
+    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0, "bad sizes");
+    HC_REQUIRE(mv_dt_grad && mv_dt_grad_1 && dt_image_grad && closest_vertex_id && multi_view_crops &&
+                   points_image_space_grad,
+               "NULL pointer");
+    ImgLayout L;
+    long long views = 0;
+    HC_TRY(make_layout(batch, n_cameras, widths, heights, L, views));
+    const long long np = views * n_points;
+    k_sil_grad_points<<<div_up(np, 256), 256, 0, s>>>(np, dt_image_grad, mv_dt_grad, points_image_space_grad);
+    HC_CHECK_LAUNCH();
+    const int vec = pixels_by_four(L) && ((uintptr_t)closest_vertex_id & 15) == 0;
+    k_sil_grad_pixels<<<dim3(div_up(max_view_pixels(L), 4 * 256), (unsigned)views), 256, 0, s>>>(
+        n_points, L, mv_dt_grad_1, closest_vertex_id, multi_view_crops, points_image_space_grad, vec);
+    HC_CHECK_LAUNCH();
+    return HC_OK;
+}
+
 }  // namespace
+
+extern "C" hc_status hc_silhouette_forward_sized(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
+                                                 int32_t n_points, const int32_t* widths, const int32_t* heights,
+                                                 const float* points_image_space, const float* normals_image_space,
+                                                 const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                                 const float* multi_view_crops, float* mv_dt_residual,
+                                                 float* mv_dt_residual_1, float* dt_image_gradient,
+                                                 float* closest_vertex_id) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    ImgLayout L;
+    size_t need = 0;
+    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, widths, heights, points_image_space, normals_image_space,
+                            is_boundary, distance_transform_image, multi_view_crops, mv_dt_residual,
+                            mv_dt_residual_1, dt_image_gradient, closest_vertex_id, L, need));
+    HC_TRY(h->grid.ensure(need));
+    return sil_forward_run((cudaStream_t)stream, h->grid.as<int>(), L, batch, n_cameras, n_points,
+                           points_image_space, normals_image_space, is_boundary, distance_transform_image,
+                           multi_view_crops, mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id);
+}
 
 extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
                                            int32_t n_points, int32_t resolution_u, int32_t resolution_v,
@@ -1116,18 +1320,11 @@ extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_
                                            const float* multi_view_crops, float* mv_dt_residual,
                                            float* mv_dt_residual_1, float* dt_image_gradient,
                                            float* closest_vertex_id) {
-    clear_error();
-    HC_REQUIRE(h, "invalid handle");
-    SilGrid g;
-    size_t need = 0;
-    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, resolution_u, resolution_v, points_image_space,
-                            normals_image_space, is_boundary, distance_transform_image, multi_view_crops,
-                            mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id, g, need));
-    HC_TRY(h->grid.ensure(need));
-    return sil_forward_run((cudaStream_t)stream, h->grid.as<int>(), g, batch, n_cameras, n_points, resolution_u,
-                           resolution_v, points_image_space, normals_image_space, is_boundary,
-                           distance_transform_image, multi_view_crops, mv_dt_residual, mv_dt_residual_1,
-                           dt_image_gradient, closest_vertex_id);
+    const SameSize sz(n_cameras, resolution_u, resolution_v);
+    return hc_silhouette_forward_sized(h, stream, batch, n_cameras, n_points, sz.w.data(), sz.h.data(),
+                                       points_image_space, normals_image_space, is_boundary,
+                                       distance_transform_image, multi_view_crops, mv_dt_residual, mv_dt_residual_1,
+                                       dt_image_gradient, closest_vertex_id);
 }
 
 extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
@@ -1136,22 +1333,21 @@ extern "C" hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t
                                             const float* closest_vertex_id, const float* multi_view_crops,
                                             float* points_image_space_grad) {
     clear_error();
-    HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0 && resolution_u > 0 && resolution_v > 0, "bad sizes");
-    HC_REQUIRE(mv_dt_grad && mv_dt_grad_1 && dt_image_grad && closest_vertex_id && multi_view_crops &&
-                   points_image_space_grad,
-               "NULL pointer");
-    cudaStream_t s = (cudaStream_t)stream;
-    const long long np = (long long)batch * n_cameras * n_points;
-    k_sil_grad_points<<<div_up(np, 256), 256, 0, s>>>(np, dt_image_grad, mv_dt_grad, points_image_space_grad);
-    HC_CHECK_LAUNCH();
-    const long long views = (long long)batch * n_cameras, P = (long long)resolution_u * resolution_v;
-    HC_REQUIRE(views <= 65535 && P < (1ll << 31), "too many views or pixels in one call");
-    const int vec = P % 4 == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
-    k_sil_grad_pixels<<<dim3(div_up(P, 4 * 256), (unsigned)views), 256, 0, s>>>(
-        n_points, resolution_u, resolution_v, mv_dt_grad_1, closest_vertex_id, multi_view_crops,
-        points_image_space_grad, vec);
-    HC_CHECK_LAUNCH();
-    return HC_OK;
+    const SameSize sz(n_cameras, resolution_u, resolution_v);
+    return sil_backward_run((cudaStream_t)stream, batch, n_cameras, n_points, sz.w.data(), sz.h.data(), mv_dt_grad,
+                            mv_dt_grad_1, dt_image_grad, closest_vertex_id, multi_view_crops,
+                            points_image_space_grad);
+}
+
+extern "C" hc_status hc_silhouette_backward_sized(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                                  const int32_t* widths, const int32_t* heights,
+                                                  const float* mv_dt_grad, const float* mv_dt_grad_1,
+                                                  const float* dt_image_grad, const float* closest_vertex_id,
+                                                  const float* multi_view_crops, float* points_image_space_grad) {
+    clear_error();
+    return sil_backward_run((cudaStream_t)stream, batch, n_cameras, n_points, widths, heights, mv_dt_grad,
+                            mv_dt_grad_1, dt_image_grad, closest_vertex_id, multi_view_crops,
+                            points_image_space_grad);
 }
 
 // ---------------------------------------------------------------------------
@@ -1198,11 +1394,12 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
                                                   float* mv_dt_residual_1, float* dt_image_gradient,
                                                   float* closest_vertex_id) {
     clear_error();
-    SilGrid g;
+    ImgLayout L;
     size_t need = 0;
-    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, resolution_u, resolution_v, points_image_space,
+    const SameSize sz(n_cameras, resolution_u, resolution_v);
+    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, sz.w.data(), sz.h.data(), points_image_space,
                             normals_image_space, is_boundary, distance_transform_image, multi_view_crops,
-                            mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id, g, need));
+                            mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id, L, need));
     HC_REQUIRE(need <= kSilStaticBytes,
                "hc_silhouette_forward_static: %lld views x %d points at %dx%d need %zu bytes of grid scratch; the "
                "static scratch holds %zu bytes (use hc_silhouette_forward)",
@@ -1211,8 +1408,7 @@ extern "C" hc_status hc_silhouette_forward_static(void* stream, int32_t batch, i
     HC_TRY(sil_static_base(&base));
     // the array keeps the previous call's contents: sil_forward_run clears the
     // cell counts before the grid is built
-    return sil_forward_run((cudaStream_t)stream, base, g, batch, n_cameras, n_points, resolution_u, resolution_v,
-                           points_image_space, normals_image_space, is_boundary, distance_transform_image,
-                           multi_view_crops, mv_dt_residual, mv_dt_residual_1, dt_image_gradient,
-                           closest_vertex_id);
+    return sil_forward_run((cudaStream_t)stream, base, L, batch, n_cameras, n_points, points_image_space,
+                           normals_image_space, is_boundary, distance_transform_image, multi_view_crops,
+                           mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id);
 }

@@ -11,6 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -106,6 +107,31 @@ class MeshBoundaryEngine:
     def reserve(self, B, Cn, width, height):
         _lib.call("hc_mesh_boundary_reserve", self._h, B, Cn, int(width), int(height))
 
+    def reserve_sized(self, B, Cn, widths, heights):
+        w, h = _sizes(widths, heights, Cn)
+        _lib.call("hc_mesh_boundary_reserve_sized", self._h, B, Cn, w.ctypes.data, h.ctypes.data)
+
+    def forward_sized(self, points_global_space, extrinsics, intrinsics, widths, heights, points_image_space=None,
+                      out=None, face_hint=None):
+        """Cameras of different sizes (widths / heights [C]): is_boundary [B,C,N]
+        (uint8); ``face_hint`` [B, pixels of a frame] int32 or None."""
+        p = _f32(points_global_space, "points_global_space")
+        ex, it = _f32(extrinsics, "extrinsics"), _f32(intrinsics, "intrinsics")
+        B = p.shape[0]
+        Cn = ex.reshape(B, -1).shape[1] // 12
+        w, h = _sizes(widths, heights, Cn)
+        if out is None:
+            out = torch.empty((B, Cn, self.N), device=p.device, dtype=torch.uint8)
+        if face_hint is not None and (face_hint.dtype != torch.int32 or not face_hint.is_contiguous()
+                                      or face_hint.numel() != B * int((w.astype(np.int64) * h).sum())):
+            raise ValueError("face_hint must be a contiguous int32 [B, pixels of a frame] tensor")
+        pis = _f32(points_image_space, "points_image_space") if points_image_space is not None else None
+        P = _lib.ptr
+        _lib.call("hc_mesh_boundary_forward_sized", self._h, _stream(), B, Cn, w.ctypes.data, h.ctypes.data, P(p),
+                  P(ex), P(it), P(pis) if pis is not None else None, P(face_hint) if face_hint is not None else None,
+                  P(out))
+        return out
+
     def forward(self, points_global_space, extrinsics, intrinsics, width: int, height: int,
                 points_image_space=None, out=None, face_hint=None):
         """is_boundary [B,C,N] (uint8).  ``face_hint`` [B,C,H,W] int32 (a renderer
@@ -167,6 +193,32 @@ class SilhouetteEngine:
     def reserve(self, B, Cn, N, U, V):
         _lib.call("hc_silhouette_reserve", self._h, B, Cn, N, U, V)
 
+    def reserve_sized(self, B, Cn, N, widths, heights):
+        w, h = _sizes(widths, heights, Cn)
+        _lib.call("hc_silhouette_reserve_sized", self._h, B, Cn, N, w.ctypes.data, h.ctypes.data)
+
+    def forward_sized(self, points, normals, is_boundary, dt, crops, widths, heights):
+        """Cameras of different sizes (widths U / heights V [C]): ``dt`` [B, pixels
+        of a frame] uint8 (each camera's V_c x U_c image in camera order);
+        returns (mv_dt_residual [B,C,N], mv_dt_residual_1 [B, pixels, 2],
+        dt_image_gradient [B,C,N,2], closest_vertex_id [B, pixels])."""
+        p, n = _f32(points, "points_image_space"), _f32(normals, "normals_image_space")
+        isb = is_boundary.detach().to(torch.uint8).contiguous()
+        dt = dt.detach().to(torch.uint8).contiguous()
+        cr = _f32(crops, "multi_view_crops")
+        B, Cn, N = p.shape[0], p.shape[1], p.shape[2]
+        w, h = _sizes(widths, heights, Cn)
+        pf = int((w.astype(np.int64) * h).sum())
+        if dt.numel() != B * pf:
+            raise ValueError(f"distance images must hold B x {pf} pixels")
+        dev = p.device
+        res, res1 = torch.empty((B, Cn, N), device=dev), torch.empty((B, pf, 2), device=dev)
+        dtg, cid = torch.empty((B, Cn, N, 2), device=dev), torch.empty((B, pf), device=dev)
+        P = _lib.ptr
+        _lib.call("hc_silhouette_forward_sized", self._h, _stream(), B, Cn, N, w.ctypes.data, h.ctypes.data, P(p),
+                  P(n), P(isb), P(dt), P(cr), P(res), P(res1), P(dtg), P(cid))
+        return res, res1, dtg, cid
+
     def forward(self, points, normals, is_boundary, dt, crops):
         p, n = _f32(points, "points_image_space"), _f32(normals, "normals_image_space")
         isb = is_boundary.detach().to(torch.uint8).contiguous()
@@ -194,6 +246,26 @@ def silhouette_backward(g, g1, dt_image_grad, closest_vertex_id, crops):
     P = _lib.ptr
     _lib.call("hc_silhouette_backward", _stream(), B, Cn, N, U, V, P(g), P(g1), P(dtg), P(cid), P(cr), P(out))
     return out
+
+
+def silhouette_backward_sized(g, g1, dt_image_grad, closest_vertex_id, crops, widths, heights):
+    """Adjoint of ``SilhouetteEngine.forward_sized``: g [B,C,N], g1 [B, pixels, 2]."""
+    g, g1 = _f32(g, "mv_dt_grad"), _f32(g1, "mv_dt_grad_1")
+    dtg, cid, cr = _f32(dt_image_grad, "dt_image_grad"), _f32(closest_vertex_id, "closest"), _f32(crops, "crops")
+    B, Cn, N = g.shape
+    w, h = _sizes(widths, heights, Cn)
+    out = torch.empty((B, Cn, N, 2), device=g.device)
+    P = _lib.ptr
+    _lib.call("hc_silhouette_backward_sized", _stream(), B, Cn, N, w.ctypes.data, h.ctypes.data, P(g), P(g1), P(dtg),
+              P(cid), P(cr), P(out))
+    return out
+
+
+def _sizes(widths, heights, n):
+    """Per-camera image sizes as int32 host arrays [n]."""
+    w = np.ascontiguousarray(np.broadcast_to(np.asarray(widths, np.int32), (n,)))
+    h = np.ascontiguousarray(np.broadcast_to(np.asarray(heights, np.int32), (n,)))
+    return w, h
 
 
 class _SilFn(torch.autograd.Function):

@@ -509,23 +509,39 @@ def skinning_scene(subdiv: int, n_skel: int, batch: int, seed: int, k: int = 4, 
                 dofs=dofs, disp=rng.normal(0.0, 1.0, size=(batch, verts.shape[0], 3)).astype(np.float32))
 
 
+def ellipse_dt(width: int, height: int, r: np.random.Generator, scale: float = 1.0) -> np.ndarray:
+    """uint8 distance-transform image [H,W] of a random ellipse (centre +-64 px,
+    semi-axes U[80,200] px at 512 px, scaled by ``scale``)."""
+    cx = width / 2 + r.uniform(-64, 64) * scale
+    cy = height / 2 + r.uniform(-64, 64) * scale
+    a, bb = r.uniform(80, 200) * scale, r.uniform(80, 200) * scale
+    th = r.uniform(0, np.pi)
+    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
+    x, y = xx + 0.5 - cx, yy + 0.5 - cy
+    u = (math.cos(th) * x + math.sin(th) * y) / a
+    v = (-math.sin(th) * x + math.cos(th) * y) / bb
+    return encode_dt((u * u + v * v) <= 1.0)
+
+
 def silhouette_masks(batch: int, views: int, width: int, height: int, seed: int, scale: float = 1.0) -> np.ndarray:
     """uint8 distance-transform images [B,C,H,W] of seeded random ellipses
     (centre +-64 px, semi-axes U[80,200] px at 512 px, scaled by ``scale``)."""
     out = np.empty((batch, views, height, width), np.uint8)
     for b in range(batch):
         for c in range(views):
-            r = rng_for(seed, 100 * b + c)
-            cx = width / 2 + r.uniform(-64, 64) * scale
-            cy = height / 2 + r.uniform(-64, 64) * scale
-            a, bb = r.uniform(80, 200) * scale, r.uniform(80, 200) * scale
-            th = r.uniform(0, np.pi)
-            yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
-            x, y = xx + 0.5 - cx, yy + 0.5 - cy
-            u = (math.cos(th) * x + math.sin(th) * y) / a
-            v = (-math.sin(th) * x + math.cos(th) * y) / bb
-            out[b, c] = encode_dt((u * u + v * v) <= 1.0)
+            out[b, c] = ellipse_dt(width, height, rng_for(seed, 100 * b + c), scale)
     return out
+
+
+# per-view image sizes of the batched mixed-resolution configuration (W x H)
+MIXED_SIZES = ((512, 512), (768, 1024), (1024, 1024), (1536, 1024))
+
+
+def mixed_camera_sizes(views: int, seed: int) -> tuple[list[int], list[int]]:
+    """Per-camera (widths, heights) drawn uniformly from MIXED_SIZES."""
+    r = rng_for(seed, 999)
+    pick = r.integers(0, len(MIXED_SIZES), size=views)
+    return [MIXED_SIZES[k][0] for k in pick], [MIXED_SIZES[k][1] for k in pick]
 
 
 def identity_crops(batch: int, views: int, width: int, height: int) -> np.ndarray:
@@ -534,7 +550,7 @@ def identity_crops(batch: int, views: int, width: int, height: int) -> np.ndarra
     return np.tile(c, (batch, views, 1))
 
 
-def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int, width: int, height: int, seed: int,
+def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int, width, height, seed: int,
                 fx: float | None = None, ring_radius: float = 3.0 * MM, k: int = 4, pose_amplitude: float = 0.5,
                 delta_rot_std: float = 0.05, delta_t_std: float = 0.01 * MM, n_masks: int | None = None,
                 first_frame: int = 0) -> dict:
@@ -548,6 +564,12 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
     images (``target_u8`` uniform bytes, ``target`` = byte / 255 in float32, the value
     ``hc_image_u8_to_f32`` computes on the device); silhouette distance-transform images of
     seeded random ellipses (``n_masks`` distinct ones, default one per view, reused across frames).
+
+    ``width`` / ``height`` may be per-camera sequences: each camera then has
+    its own image size, focal length fx = fy = 600 min(W, H) / 512 (unless
+    ``fx`` is given) and centred principal point, and the per-pixel arrays
+    (``target``, ``target_u8``, ``dt``) are [B, pixels of a frame, ...] with
+    the frame's cameras concatenated in order.
 
     ``frames`` frames starting at frame ``first_frame`` of the seed's
     sequence: the character, cameras and masks depend on the seed alone and
@@ -563,12 +585,32 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
     skin_idx, skin_w = skinning_weights(verts, sk, k, rng)
     fr = range(first_frame, first_frame + frames)
     dofs = np.stack([random_pose(sk, rng_for(seed, b), pose_amplitude) for b in fr])
-    if fx is None:
-        fx = 600.0 * min(width, height) / 512.0
-    ex, it = camera_ring(views, ring_radius, fx, width, height)
+    sized = np.ndim(width) > 0 or np.ndim(height) > 0
+    ws = [int(x) for x in np.broadcast_to(np.asarray(width), (views,))]
+    hs = [int(x) for x in np.broadcast_to(np.asarray(height), (views,))]
     nm = views if n_masks is None else n_masks
-    masks = silhouette_masks(1, nm, width, height, seed=seed, scale=min(width, height) / 512.0)[0]
-    dt = np.stack([masks[np.arange(views) % nm]] * frames)
+    if not sized:
+        W, H = ws[0], hs[0]
+        if fx is None:
+            fx = 600.0 * min(W, H) / 512.0
+        ex, it = camera_ring(views, ring_radius, fx, W, H)
+        masks = silhouette_masks(1, nm, W, H, seed=seed, scale=min(W, H) / 512.0)[0]
+        dt = np.stack([masks[np.arange(views) % nm]] * frames)
+        crops = identity_crops(frames, views, W, H)
+    else:
+        ex, it = [], []
+        for c in range(views):
+            f_c = fx if fx is not None else 600.0 * min(ws[c], hs[c]) / 512.0
+            e1, i1 = camera_ring(views, ring_radius, f_c, ws[c], hs[c])
+            ex.append(e1[12 * c:12 * c + 12])
+            it.append(i1[9 * c:9 * c + 9])
+        ex, it = np.concatenate(ex), np.concatenate(it)
+        masks = [ellipse_dt(ws[c], hs[c], rng_for(seed, c % nm), min(ws[c], hs[c]) / 512.0).reshape(-1)
+                 for c in range(views)]
+        dt = np.stack([np.concatenate(masks)] * frames)
+        crops = np.stack([np.stack([np.array([0, 0, 1, 0, 0, ws[c], hs[c]], np.float32) for c in range(views)])]
+                         * frames)
+    P_frame = int(sum(w * h for w, h in zip(ws, hs)))
     # the appearance is shared by all frames (one parameter, its gradient
     # summed over frames and ranks); pose, node deltas, lighting and targets
     # are per frame
@@ -580,7 +622,8 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
         per["dT"].append(r.normal(0.0, delta_t_std, size=(n_nodes, 3)).astype(np.float32))
         per["dA"].append(r.normal(0.0, delta_rot_std, size=(n_nodes, 3)).astype(np.float32))
         per["sh"].append(sh_coefficients(views, r))
-        per["target_u8"].append(r.integers(0, 256, size=(views, height, width, 3), dtype=np.uint8))
+        shape = (P_frame, 3) if sized else (views, hs[0], ws[0], 3)
+        per["target_u8"].append(r.integers(0, 256, size=shape, dtype=np.uint8))
     per = {key: np.stack(v) for key, v in per.items()}
     target_u8 = per["target_u8"]
     return dict(verts=verts, faces=faces, graph=graph, markers=markers, marker_node=mk_nodes, skeleton=sk,
@@ -592,5 +635,6 @@ def chain_scene(subdiv: int, n_nodes: int, n_skel: int, frames: int, views: int,
                 extr=np.tile(ex[None], (frames, 1)), intr=np.tile(it[None], (frames, 1)),
                 texcoords=spherical_uvs(verts, faces),
                 target=target_u8.astype(np.float32) / np.float32(255.0), target_u8=target_u8,
-                dt=dt, crops=identity_crops(frames, views, width, height),
-                N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=width, H=height, first_frame=first_frame)
+                dt=dt, crops=crops,
+                N=N, F=faces.shape[0], M=n_nodes, B=frames, C=views, W=ws if sized else ws[0],
+                H=hs if sized else hs[0], P_frame=P_frame, first_frame=first_frame)

@@ -456,6 +456,21 @@ hc_status hc_mesh_boundary_forward_hinted(hc_mesh_boundary h, void* stream, int3
                                           const float* extrinsics, const float* intrinsics,
                                           const float* points_image_space, const int32_t* face_hint,
                                           uint8_t* is_boundary);
+/* hc_mesh_boundary_forward for cameras of different image sizes (no
+ * reference counterpart: the reference needs one op instance per resolution).
+ * widths / heights: host arrays [C]; per-pixel data of a frame are its
+ * cameras' images concatenated in camera order (row-major H_c x W_c), as for
+ * hc_renderer_create_multires.  face_hint [B, pixels of a frame] int32 or
+ * NULL (then as hc_mesh_boundary_forward).  Cameras of one size behave as
+ * hc_mesh_boundary_forward(_hinted); mixed sizes take at most 32 cameras per
+ * call.  Each camera's flags are those of the single-size op at its size. */
+hc_status hc_mesh_boundary_reserve_sized(hc_mesh_boundary h, int32_t batch, int32_t n_cameras,
+                                         const int32_t* widths, const int32_t* heights);
+hc_status hc_mesh_boundary_forward_sized(hc_mesh_boundary h, void* stream, int32_t batch, int32_t n_cameras,
+                                         const int32_t* widths, const int32_t* heights,
+                                         const float* points_global_space, const float* extrinsics,
+                                         const float* intrinsics, const float* points_image_space,
+                                         const int32_t* face_hint, uint8_t* is_boundary);
 /* The same boundary test with coverage taken from a renderer face buffer
  * [B,C,H,W] (-1 = empty) instead of the op's own 2-D raster.  No separate
  * reference counterpart: the renderer's ray test and the 2-D barycentric test
@@ -491,6 +506,29 @@ hc_status hc_silhouette_backward(void* stream, int32_t batch, int32_t n_cameras,
                                  const float* mv_dt_grad_1, const float* dt_image_grad,
                                  const float* closest_vertex_id, const float* multi_view_crops,
                                  float* points_image_space_grad);
+
+/* The silhouette loss and its adjoint for cameras of different image sizes
+ * (no reference counterpart: the reference needs one op instance per
+ * resolution).  widths (U) / heights (V): host arrays [C]; the distance
+ * images and the per-pixel outputs hold a frame's cameras concatenated in
+ * camera order, each row-major V_c x U_c: distance_transform_image
+ * [B, pixels of a frame] uint8, mv_dt_residual_1 [B, pixels of a frame, 2],
+ * closest_vertex_id [B, pixels of a frame].  Cameras of one size behave as
+ * hc_silhouette_forward / _backward; mixed sizes take at most 32 cameras per
+ * call.  Each camera's results are those of the single-size op at its size. */
+hc_status hc_silhouette_reserve_sized(hc_silhouette h, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                      const int32_t* widths, const int32_t* heights);
+hc_status hc_silhouette_forward_sized(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
+                                      int32_t n_points, const int32_t* widths, const int32_t* heights,
+                                      const float* points_image_space, const float* normals_image_space,
+                                      const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                      const float* multi_view_crops, float* mv_dt_residual, float* mv_dt_residual_1,
+                                      float* dt_image_gradient, float* closest_vertex_id);
+hc_status hc_silhouette_backward_sized(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                       const int32_t* widths, const int32_t* heights, const float* mv_dt_grad,
+                                       const float* mv_dt_grad_1, const float* dt_image_grad,
+                                       const float* closest_vertex_id, const float* multi_view_crops,
+                                       float* points_image_space_grad);
 
 /*
  * hc_silhouette_forward without allocation.  No counterpart in the reference.

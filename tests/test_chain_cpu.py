@@ -53,3 +53,32 @@ def test_chain_step_calls(recorder):
     assert args["hc_pose2eg_backward"][7] == args["hc_eg_backward"][9]
     assert args["hc_pose2eg_backward"][8] == args["hc_eg_backward"][10]
     assert np.isfinite(sc["dofs"]).all()
+
+
+def test_chain_step_calls_mixed_sizes_vertex_dq(recorder):
+    """Cameras of different sizes and per-vertex DQ skinning: the sized
+    boundary / silhouette entry points with the per-camera size arrays, flat
+    per-pixel buffers of a frame, and the DQ adjoint fed by the summed vertex
+    gradient."""
+    from deepcharacters_b200.chain import DeformRenderChain
+    ws, hs = [32, 48, 64], [32, 64, 48]
+    sc = S.chain_scene(1, 12, 4, 2, 3, ws, hs, seed=3)
+    assert sc["dt"].shape == (2, sum(w * h for w, h in zip(ws, hs)))
+    ch = DeformRenderChain(sc, "cpu", 2, 3, ws, hs, deformation="dq")
+    assert ch.multires and ch.buf["face"].shape == (2, ch.P_frame) and ch.buf["res1"].shape == (2, ch.P_frame, 2)
+    recorder.clear()
+    ch.step()
+    names = [n for n, _ in recorder]
+    assert names == ["hc_dq_skinning_forward", "hc_renderer_forward_l1", "hc_camera_projection_forward",
+                     "hc_camera_projection_forward", "hc_mesh_boundary_forward_sized", "hc_silhouette_forward_sized",
+                     "hc_sum_squares_loss", "hc_sum_squares_loss", "hc_silhouette_backward_sized",
+                     "hc_camera_projection_backward", "hc_renderer_backward_l1", "hc_add_inplace",
+                     "hc_dq_skinning_backward"]
+    args = dict(recorder)
+    import ctypes
+    w = args["hc_mesh_boundary_forward_sized"][4]
+    assert list((ctypes.c_int32 * 3).from_address(w)) == ws
+    assert args["hc_sum_squares_loss"][1] == 2 * ch.P_frame * 2
+    v = args["hc_dq_skinning_forward"][5]
+    assert args["hc_renderer_forward_l1"][3] == v and args["hc_dq_skinning_backward"][4] == v
+    assert args["hc_dq_skinning_backward"][3] == args["hc_add_inplace"][2]
