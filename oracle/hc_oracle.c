@@ -42,3 +42,6 @@
 #undef SFX
 #undef OUTT
 #undef HCO_FORWARD_ONLY
+
+/* host kinematics and Pose2EG, float only (the reference computes them in float) */
+#include "hc_oracle_fk.inc"

@@ -81,6 +81,22 @@ int hco_eg_forward_f64d(int B, int N, int M, int Mk, int F, const float* base, c
                         const float* dT, const float* dA, const float* sT, const float* sA, const float* disp,
                         double* out_v, double* out_n, double* out_m, double* out_g);
 
+
+/* The reference's host kinematics in float (Skeletool joint / dof / skeleton
+ * update with the dual-quaternion joint chain, DQSkinningGPUOp.cpp:257-347;
+ * see hc_oracle_fk.inc): dofs [B,D] -> global joint positions / axes [B,J,3]
+ * and the skinning joints' dual quaternions [B,S,8] (x, y, z, w rotation, then
+ * x, y, z, w translation).  joint_scale / skin_scale may be NULL (ones). */
+int hco_fk_f32(int B, int J, const int32_t* parent, const int32_t* type, const float* offset, const float* axis,
+               const float* joint_scale, int D, const int32_t* dof_offsets, const int32_t* dof_joint,
+               const float* dof_weight, int S, const int32_t* skin_joint, const float* skin_scale,
+               const float* dofs, float* joint_position, float* joint_axis, float* dual_quaternions);
+/* Pose2EmbeddedGraphCpu's node loop (Pose2EmbeddedGraphCPUOp.cpp:196-290) in
+ * float on given joint dual quaternions [B,S,8]: skin_index / skin_weight
+ * [N,K], node_vertex [M] -> skinned_t, skinned_a (Z-Y-X Euler) [B,M,3]. */
+int hco_pose2eg_f32(int B, int S, int N, int K, const int32_t* skin_index, const float* skin_weight, int M,
+                    const int32_t* node_vertex, const float* dual_quaternions, float* skinned_t, float* skinned_a);
+
 #ifdef __cplusplus
 }
 #endif

@@ -606,3 +606,44 @@ def texel_table(texcoords, TH, TW):
         sl = out[y0:y1, x0:x1]
         sl[hit] = np.stack([np.full(hit.sum(), f), aa[hit], bb[hit], 1 - aa[hit] - bb[hit]], 1)
     return out
+
+
+# ---------------------------------------------------------------------------
+# host kinematics in float, the reference's procedure (hc_oracle_fk.inc)
+# ---------------------------------------------------------------------------
+def fk_f32(ch, dofs):
+    """Global joint positions / axes [B,J,3] and skinning-joint dual
+    quaternions [B,S,8] by the reference's dual-quaternion joint chain in float."""
+    i32 = lambda a: _c(a, np.int32)  # noqa: E731
+    f32 = lambda a: None if a is None else _c(a, np.float32)  # noqa: E731
+    dofs = f32(np.atleast_2d(dofs))
+    B, J, S, D = dofs.shape[0], ch.n_joints, ch.n_skin, ch.n_dofs
+    arr = [i32(ch.parent), i32(ch.joint_type), f32(ch.offset), f32(ch.axis), f32(ch.joint_scale),
+           i32(ch.dof_offsets), i32(ch.dof_joint), f32(ch.dof_weight), i32(ch.skin_joint), f32(ch.skin_scale)]
+    pos, ax, dq = np.zeros((B, J, 3), np.float32), np.zeros((B, J, 3), np.float32), np.zeros((B, S, 8), np.float32)
+    fn = oracle_lib().hco_fk_f32
+    vp_ = C.c_void_p
+    p = lambda a: vp_(None) if a is None else vp_(_p(a))  # noqa: E731
+    st = fn(B, J, p(arr[0]), p(arr[1]), p(arr[2]), p(arr[3]), p(arr[4]), D, p(arr[5]), p(arr[6]), p(arr[7]), S,
+            p(arr[8]), p(arr[9]), p(dofs), p(pos), p(ax), p(dq))
+    if st != 0:
+        raise RuntimeError("oracle fk failed")
+    return pos, ax, dq
+
+
+def pose2eg_f32(ch, dq, node_vertex, weights):
+    """Pose2EmbeddedGraphCpu's node blend + Euler angles in float on the given
+    joint dual quaternions [B,S,8]: (skinned_t, skinned_a) [B,M,3]."""
+    dq = _c(dq, np.float32)
+    nv = _c(node_vertex, np.int32)
+    si, w = _c(ch.skin_index, np.int32), _c(weights, np.float32)
+    B, S = dq.shape[:2]
+    N, K = si.shape
+    M = nv.shape[0]
+    t, a = np.zeros((B, M, 3), np.float32), np.zeros((B, M, 3), np.float32)
+    vp_ = C.c_void_p
+    st = oracle_lib().hco_pose2eg_f32(B, S, N, K, vp_(_p(si)), vp_(_p(w)), M, vp_(_p(nv)), vp_(_p(dq)), vp_(_p(t)),
+                                      vp_(_p(a)))
+    if st != 0:
+        raise RuntimeError("oracle pose2eg failed")
+    return t, a

@@ -193,3 +193,26 @@ def test_pose2eg_backward_matches_fp64_finite_differences(scene):
         fd[:, d] = (loss(p) - loss(m)) / (2 * h)
     assert np.abs(fd).max() > 1.0
     assert nrel(ours, fd) < 1e-4, nrel(ours, fd)
+
+
+def test_device_kinematics_match_the_float_reference_procedure(scene):
+    """The device kinematics and node skinning against the float restatement
+    of the reference's own procedure (dual-quaternion joint chain and
+    Pose2EmbeddedGraphCpu's node loop, oracle/hc_oracle_fk.inc): both in
+    float, so they agree to a few float roundings."""
+    sc, ch = scene
+    eng = SkinningEngine(ch)
+    _, _, gp, ga, dq, _ = eng.dq_forward(_t(sc["dofs"]), _t(sc["weights"]))
+    pos, ax, dq32 = O.fk_f32(ch, sc["dofs"])
+    assert nrel(gp, pos) < 1e-6 and nrel(ga, ax) < 1e-6
+    d = dq.cpu().numpy()
+    sign = np.where((d[..., :4] * dq32[..., :4]).sum(-1, keepdims=True) < 0, -1.0, 1.0)
+    assert nrel(d * sign, dq32) < 1e-6
+    rng = np.random.default_rng(5)
+    nodes = rng.choice(ch.base_vertices.shape[0], size=50, replace=False).astype(np.int32)
+    w0 = sc["weights"][0]
+    t, a, _ = eng.pose2eg(_t(sc["dofs"]), torch.from_numpy(nodes).to(DEV), _t(w0))
+    t32, a32 = O.pose2eg_f32(ch, dq32, nodes, w0)
+    assert nrel(t, t32) < 1e-5
+    da = a.cpu().numpy().astype(np.float64) - a32
+    assert np.abs(np.arctan2(np.sin(da), np.cos(da))).max() < 1e-4
