@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys
 // to kCovSmall tiles are binned by their own thread, lanes that hit the same tile
 // sharing one counter atomic; larger boxes are taken by the whole warp, a
 // tile per lane, reading the record back from global memory.
-__global__ void __launch_bounds__(256, 5) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
+__global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
                           CovBins cb, const __grid_constant__ ImgLayout L) {
     // grid (triangle blocks, views): no 64-bit division per thread
     const int fi = blockIdx.x * blockDim.x + threadIdx.x;
