@@ -276,6 +276,31 @@ def kernel_bytes(sc, frames, covered):
             "render_grad": V * 4 * P + 32 * covered + frames * (24 * N + 12 * F + 24 * N)}
 
 
+def issue_roofline(kern_ms, views, clocks, device):
+    """Instruction-issue ceiling of the two raster kernels (they are
+    issue-bound, not HBM-bound): ncu's warp instructions per view of each
+    (profiles/issue.json, a small capture of the same kernels; the count
+    grows with the views rendered) x the views of this launch / the live
+    kernel time, against the SMs' issue rate (4 warp instructions per SM per
+    clock) at the SM clock sampled during the timed region."""
+    path = os.path.join(ROOT, "profiles", "issue.json")
+    if not os.path.exists(path):
+        return {}
+    ij = json.load(open(path))
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = sms * 4 * mhz * 1e6 / 1e9  # G warp instructions / s
+    out = {"issue_peak_ginst_s": peak, "issue_peak_basis": f"{sms} SMs x 4 warp inst/clk x {mhz:.0f} MHz"}
+    for k, ms in kern_ms.items():
+        rec = ij.get("k_" + k)
+        if not rec:
+            continue
+        ach = rec["warp_inst_per_view"] * views / (ms / 1e3) / 1e9
+        out[k] = {"achieved_ginst_s": ach, "frac": ach / peak, "lanes_per_inst": rec["lanes_per_inst"],
+                  "warp_inst_per_view": rec["warp_inst_per_view"], "capture": rec.get("capture")}
+    return out
+
+
 def one_view_scene(sc):
     """The scene arrays of frame 0, camera 0 (shapes of a 1-frame 1-view chain)."""
     d = dict(sc)
@@ -438,6 +463,7 @@ def run_ours(args, world, rank, local):
     issue = {"resolve_pixels_per_s": frames * VIEWS * RES * RES / (kern_ms["resolve"] / 1e3),
              "resolve_bin_entries_per_s": binned / (kern_ms["resolve"] / 1e3),
              "bin_entries_per_covered_pixel": binned / max(covered, 1)}
+    issue.update(issue_roofline(kern_ms, frames * VIEWS, clocks, local))
 
     unbatched = None if args.no_unbatched or world > 1 else run_unbatched(ch, sc, dev, frames, parity, 2)
     # e2e: public API, pinned host inputs copied every step, losses read back
