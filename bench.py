@@ -276,7 +276,7 @@ def kernel_bytes(sc, frames, covered):
             "render_grad": V * 4 * P + 32 * covered + frames * (24 * N + 12 * F + 24 * N)}
 
 
-def issue_roofline(kern_ms, views, clocks, device):
+def issue_roofline(kern_ms, views, clocks, device, adjoint="parity"):
     """Instruction-issue ceiling of the two raster kernels (they are
     issue-bound, not HBM-bound): ncu's warp instructions per view of each
     (profiles/issue.json, a small capture of the same kernels; the count
@@ -292,7 +292,7 @@ def issue_roofline(kern_ms, views, clocks, device):
     peak = sms * 4 * mhz * 1e6 / 1e9  # G warp instructions / s
     out = {"issue_peak_ginst_s": peak, "issue_peak_basis": f"{sms} SMs x 4 warp inst/clk x {mhz:.0f} MHz"}
     for k, ms in kern_ms.items():
-        rec = ij.get("k_" + k)
+        rec = ij.get("k_" + k + ("_exact" if k == "render_grad" and adjoint == "exact" else ""))
         if not rec:
             continue
         ach = rec["warp_inst_per_view"] * views / (ms / 1e3) / 1e9
@@ -463,7 +463,7 @@ def run_ours(args, world, rank, local):
     issue = {"resolve_pixels_per_s": frames * VIEWS * RES * RES / (kern_ms["resolve"] / 1e3),
              "resolve_bin_entries_per_s": binned / (kern_ms["resolve"] / 1e3),
              "bin_entries_per_covered_pixel": binned / max(covered, 1)}
-    issue.update(issue_roofline(kern_ms, frames * VIEWS, clocks, local))
+    issue.update(issue_roofline(kern_ms, frames * VIEWS, clocks, local, args.adjoint))
 
     unbatched = None if args.no_unbatched or world > 1 else run_unbatched(ch, sc, dev, frames, parity, 2)
     # e2e: public API, pinned host inputs copied every step, losses read back
