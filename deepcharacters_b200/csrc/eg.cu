@@ -33,12 +33,17 @@ __device__ __forceinline__ float3 mtv(const float* M, float3 v) {  // M^T v, M r
                        M[2] * v.x + M[5] * v.y + M[8] * v.z);
 }
 
-// per (frame, node) table: R_delta (9), t_delta (3), R_skinned (9), t_skinned (3)
-struct NodeRT {
+// per (frame, node) table: R_delta (9), t_delta (3), R_skinned (9),
+// t_skinned (3) and the node's base position g (3), 16-byte aligned so that a
+// row of it is one vector load: rows 0-2 hold (R_delta, t_delta), rows 3-5
+// (R_skinned, t_skinned), row 6 g
+struct __align__(16) NodeRT {
     float rd[9];
     float td[3];
     float rs[9];
     float ts[3];
+    float g[3];
+    float pad;
 };
 
 __global__ void k_eg_nodes(int B, int M, const float* __restrict__ base, const int* __restrict__ node_vertex,
@@ -61,6 +66,11 @@ __global__ void k_eg_nodes(int B, int M, const float* __restrict__ base, const i
         t.td[k] = dT[3 * i + k];
         t.ts[k] = sT[3 * i + k];
     }
+    const float3 gb = ld3(base + 3LL * node_vertex[n]);
+    t.g[0] = gb.x;
+    t.g[1] = gb.y;
+    t.g[2] = gb.z;
+    t.pad = 0.f;
     tab[i] = t;
     if (dA_copy) st3(dA_copy + 3 * i, da);
     if (sA_copy) st3(sA_copy + 3 * i, sa);
@@ -73,38 +83,80 @@ __global__ void k_eg_nodes(int B, int M, const float* __restrict__ base, const i
     }
 }
 
-__global__ void k_eg_vertices(int B, int N, int M, const float* __restrict__ base, const int* __restrict__ node_vertex,
-                              const int* __restrict__ v2n_off, const int* __restrict__ v2n_size,
-                              const int* __restrict__ v2n_idx, const float* __restrict__ v2n_w,
-                              const NodeRT* __restrict__ tab, const float* __restrict__ disp,
-                              float* __restrict__ out, float* __restrict__ vnr_out) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * N) return;
-    const int b = (int)(i / N), v = (int)(i % N);
-    const int off = v2n_off[v], cnt = v2n_size[v];
-    const float3 vb = ld3(base + 3LL * v);
-    const NodeRT* T = tab + (long long)b * M;
+// Deformed vertices (EmbeddedGraphGPUOp.cu:50-125), grid (vertex blocks,
+// frames).  The block's vertex -> node entries (a contiguous range of the
+// packed CSR) are staged in shared memory by coalesced loads; each (vertex,
+// node) pair then reads the node's rotation / translation rows as float4
+// loads of the 16-byte aligned table and the vertex as one float4.  Sums in
+// the reference's order: v_nr = sum_k w_k (R_dk (v - g_k) + g_k + t_dk) +
+// disp, then sum_k w_k (R_sk v_nr + t_sk).
+constexpr int kEgBlock = 128;
+constexpr int kEgStage = 8 * kEgBlock;  // staged (node, weight) entries per block
+
+__global__ void __launch_bounds__(kEgBlock) k_eg_vertices(int B, int N, int M, const float4* __restrict__ base4,
+                                                          const int* __restrict__ poff, const int* __restrict__ pidx,
+                                                          const float* __restrict__ pw, const NodeRT* __restrict__ tab,
+                                                          const float* __restrict__ disp, float* __restrict__ out,
+                                                          float* __restrict__ vnr_out) {
+    __shared__ int s_idx[kEgStage];
+    __shared__ float s_w[kEgStage];
+    const int b = blockIdx.y;
+    const int v0 = blockIdx.x * kEgBlock, v1 = min(v0 + kEgBlock, N);
+    const int e0 = poff[v0], e1 = poff[v1];
+    const bool staged = e1 - e0 <= kEgStage;  // block-uniform
+    if (staged)
+        for (int e = e0 + (int)threadIdx.x; e < e1; e += kEgBlock) {
+            s_idx[e - e0] = pidx[e];
+            s_w[e - e0] = pw[e];
+        }
+    __syncthreads();
+    const int v = v0 + (int)threadIdx.x;
+    if (v >= N) return;
+    const long long i = (long long)b * N + v;
+    const int off = poff[v], cnt = poff[v + 1] - off;
+    const int* I = staged ? s_idx + (off - e0) : pidx + off;
+    const float* Wt = staged ? s_w + (off - e0) : pw + off;
+    const float4 vb4 = base4[v];
+    const float3 vb = make_float3(vb4.x, vb4.y, vb4.z);
+    const float4* T = reinterpret_cast<const float4*>(tab + (long long)b * M);
+    constexpr int kRows = sizeof(NodeRT) / sizeof(float4);
     float3 vnr = make_float3(0.f, 0.f, 0.f);
     for (int k = 0; k < cnt; ++k) {
-        const int n = v2n_idx[off + k];
-        const float w = v2n_w[off + k];
-        const float3 g = ld3(base + 3LL * node_vertex[n]);
+        const float4* q = T + (long long)I[k] * kRows;
+        const float w = Wt[k];
+        const float4 a = q[0], c = q[1], d = q[2], gg = q[6];
         R33 R;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) R.m[q] = T[n].rd[q];
-        vnr += w * (mv(R, vb - g) + g + make_float3(T[n].td[0], T[n].td[1], T[n].td[2]));
+        R.m[0] = a.x;
+        R.m[1] = a.y;
+        R.m[2] = a.z;
+        R.m[3] = a.w;
+        R.m[4] = c.x;
+        R.m[5] = c.y;
+        R.m[6] = c.z;
+        R.m[7] = c.w;
+        R.m[8] = d.x;
+        const float3 g = make_float3(gg.x, gg.y, gg.z);
+        vnr += w * (mv(R, vb - g) + g + make_float3(d.y, d.z, d.w));
     }
     vnr += ld3(disp + 3 * i);
-    float3 d = make_float3(0.f, 0.f, 0.f);
+    float3 dsum = make_float3(0.f, 0.f, 0.f);
     for (int k = 0; k < cnt; ++k) {
-        const int n = v2n_idx[off + k];
-        const float w = v2n_w[off + k];
+        const float4* q = T + (long long)I[k] * kRows;
+        const float w = Wt[k];
+        const float4 a = q[3], c = q[4], d = q[5];
         R33 R;
-#pragma unroll
-        for (int q = 0; q < 9; ++q) R.m[q] = T[n].rs[q];
-        d += w * (mv(R, vnr) + make_float3(T[n].ts[0], T[n].ts[1], T[n].ts[2]));
+        R.m[0] = a.x;
+        R.m[1] = a.y;
+        R.m[2] = a.z;
+        R.m[3] = a.w;
+        R.m[4] = c.x;
+        R.m[5] = c.y;
+        R.m[6] = c.z;
+        R.m[7] = c.w;
+        R.m[8] = d.x;
+        dsum += w * (mv(R, vnr) + make_float3(d.y, d.z, d.w));
     }
-    st3(out + 3 * i, d);
+    st3(out + 3 * i, dsum);
     if (vnr_out) st3(vnr_out + 3 * i, vnr);
 }
 
@@ -264,6 +316,7 @@ struct hc_eg_s {
     int N = 0, M = 0, Mk = 0, F = 0;
     int full_skinned_grad = 0;
     DevBuf base, node_vertex, v2n_off, v2n_size, v2n_idx, v2n_w, n2v_off, n2v_size, n2v_idx, n2v_w;
+    DevBuf base4, v2n_poff, v2n_pidx, v2n_pw;  // float4 base vertices; the vertex -> node CSR packed in vertex order
     DevBuf markers, m2n, n2m, faces, vf, vf_id;
     DevBuf tab, u, vnr;
 };
@@ -338,6 +391,30 @@ extern "C" hc_status hc_eg_create(hc_eg* out, int32_t n_vertices, const float* b
         UP(markers, base_markers, 3LL * n_markers);
         UP(m2n, marker_to_node, n_markers);
     }
+    {
+        // the vertex -> node lists packed contiguously in vertex order (the
+        // vertex kernel stages a block's range in one coalesced sweep), and
+        // the base vertices padded to float4
+        std::vector<int> poff((size_t)n_vertices + 1, 0), pidx;
+        std::vector<float> pw;
+        std::vector<float4> b4((size_t)n_vertices);
+        for (int v = 0; v < n_vertices; ++v) {
+            for (int k = 0; k < v2n_sizes[v]; ++k) {
+                pidx.push_back(v2n_indices[v2n_offsets[v] + k]);
+                pw.push_back(v2n_weights[v2n_offsets[v] + k]);
+            }
+            poff[v + 1] = (int)pidx.size();
+            b4[v] = make_float4(base_vertices[3 * v], base_vertices[3 * v + 1], base_vertices[3 * v + 2], 0.f);
+        }
+        if (pidx.empty()) {
+            pidx.push_back(0);
+            pw.push_back(0.f);
+        }
+        UP(v2n_poff, poff.data(), poff.size());
+        UP(v2n_pidx, pidx.data(), pidx.size());
+        UP(v2n_pw, pw.data(), pw.size());
+        UP(base4, b4.data(), b4.size());
+    }
 #undef UP
     if (st != HC_OK) {
         delete h;
@@ -352,7 +429,7 @@ extern "C" hc_status hc_eg_destroy(hc_eg h) {
     if (!h) return HC_OK;
     DevBuf* bufs[] = {&h->base, &h->node_vertex, &h->v2n_off, &h->v2n_size, &h->v2n_idx, &h->v2n_w, &h->n2v_off,
                       &h->n2v_size, &h->n2v_idx, &h->n2v_w, &h->markers, &h->m2n, &h->n2m, &h->faces, &h->vf,
-                      &h->vf_id, &h->tab, &h->u, &h->vnr};
+                      &h->vf_id, &h->tab, &h->u, &h->vnr, &h->base4, &h->v2n_poff, &h->v2n_pidx, &h->v2n_pw};
     for (DevBuf* b : bufs) b->release();
     delete h;
     return HC_OK;
@@ -395,10 +472,10 @@ extern "C" hc_status hc_eg_forward(hc_eg h, void* stream, int32_t batch, const f
                                                nodes_skinned_translation, nodes_skinned_rotation, tab, deformed_graph,
                                                d_delta_rotation, d_skinned_rotation);
     HC_CHECK_LAUNCH();
-    k_eg_vertices<<<div_up(BN, 128), 128, 0, s>>>(batch, h->N, h->M, h->base.as<float>(), h->node_vertex.as<int>(),
-                                                  h->v2n_off.as<int>(), h->v2n_size.as<int>(), h->v2n_idx.as<int>(),
-                                                  h->v2n_w.as<float>(), tab, vertex_displacements, deformed_vertices,
-                                                  nullptr);
+    HC_REQUIRE(batch <= 65535, "too many frames in one call (%d)", batch);
+    k_eg_vertices<<<dim3(div_up(h->N, kEgBlock), batch), kEgBlock, 0, s>>>(
+        batch, h->N, h->M, h->base4.as<float4>(), h->v2n_poff.as<int>(), h->v2n_pidx.as<int>(),
+        h->v2n_pw.as<float>(), tab, vertex_displacements, deformed_vertices, nullptr);
     HC_CHECK_LAUNCH();
     if (deformed_normals) {
         k_eg_normals<<<div_up(BN, 128), 128, 0, s>>>(batch, h->N, h->faces.as<int3>(), h->vf.as<int>(),
@@ -446,10 +523,10 @@ extern "C" hc_status hc_eg_backward(hc_eg h, void* stream, int32_t batch, const 
         HC_TRY(h->u.ensure(sizeof(float) * 3 * (size_t)BN));
         // v_nr of every vertex (the outer sum's argument); the deformed output
         // goes to the scratch u buffer and is overwritten below
-        k_eg_vertices<<<div_up(BN, 128), 128, 0, s>>>(batch, h->N, h->M, h->base.as<float>(), h->node_vertex.as<int>(),
-                                                      h->v2n_off.as<int>(), h->v2n_size.as<int>(), h->v2n_idx.as<int>(),
-                                                      h->v2n_w.as<float>(), tab, vertex_displacements,
-                                                      h->u.as<float>(), h->vnr.as<float>());
+        HC_REQUIRE(batch <= 65535, "too many frames in one call (%d)", batch);
+        k_eg_vertices<<<dim3(div_up(h->N, kEgBlock), batch), kEgBlock, 0, s>>>(
+            batch, h->N, h->M, h->base4.as<float4>(), h->v2n_poff.as<int>(), h->v2n_pidx.as<int>(),
+            h->v2n_pw.as<float>(), tab, vertex_displacements, h->u.as<float>(), h->vnr.as<float>());
         HC_CHECK_LAUNCH();
     }
     k_eg_grad_vertex<<<div_up(BN, 128), 128, 0, s>>>(batch, h->N, h->M, h->v2n_off.as<int>(), h->v2n_size.as<int>(),

@@ -102,6 +102,8 @@ struct Skel {
     const int* skin_idx;   // [N,K] skinning joint per vertex slot
     const float* base_v;   // [N,3]
     const float* base_n;   // [N,3]
+    const float4* base_v4;  // [N] the same, padded to float4 (one 16-byte load per vertex)
+    const float4* base_n4;  // [N]
 };
 
 // Forward kinematics, one CTA per frame: the joint parameters and every
@@ -276,51 +278,126 @@ __device__ __forceinline__ void dq_blend(const Skel& sk, int b, int v, const flo
     }
 }
 
-__global__ void k_dq_skin(Skel sk, int B, const float* __restrict__ dq, const float* __restrict__ w,
-                          float* __restrict__ out_v, float* __restrict__ out_n, float* __restrict__ w_copy) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * sk.N) return;
-    const int b = (int)(i / sk.N), v = (int)(i % sk.N);
-    float4 br, bt;
-    dq_blend(sk, b, v, dq, w, br, bt);
+// Shared-memory staging of a skinning block (grid (vertex blocks, frames),
+// blockDim.x vertices of one frame): the frame's joint table (`table_floats`
+// floats per skinning joint) and the block's K joint indices and weights per
+// vertex, copied by coalesced loads (16-byte vectors when `vec`: K a multiple
+// of 4 and 16-byte aligned arrays).  Returns the block's first vertex.
+__device__ __forceinline__ int stage_skin_block(const Skel& sk, int b, const float* __restrict__ table,
+                                                int table_floats, const float* __restrict__ w, int vec,
+                                                float* s_tab, float* s_w, int* s_idx) {
+    const float* t0 = table + (long long)b * sk.S * table_floats;
+    for (int j = threadIdx.x; j < sk.S * table_floats; j += blockDim.x) s_tab[j] = t0[j];
+    const int v0 = blockIdx.x * blockDim.x;
+    const int n = min((int)blockDim.x, sk.N - v0) * sk.K;
+    const int* gi = sk.skin_idx + (long long)v0 * sk.K;
+    const float* gw = w + ((long long)b * sk.N + v0) * sk.K;
+    if (vec) {
+        for (int e = threadIdx.x; e < n / 4; e += blockDim.x) {
+            reinterpret_cast<int4*>(s_idx)[e] = reinterpret_cast<const int4*>(gi)[e];
+            reinterpret_cast<float4*>(s_w)[e] = reinterpret_cast<const float4*>(gw)[e];
+        }
+    } else {
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            s_idx[e] = gi[e];
+            s_w[e] = gw[e];
+        }
+    }
+    __syncthreads();
+    return v0;
+}
+
+// dynamic shared memory of a skinning block
+__host__ __device__ constexpr size_t skin_block_smem(int S, int table_floats, int K, int threads) {
+    return sizeof(float) * ((size_t)S * table_floats + 2 * (size_t)threads * K);
+}
+
+constexpr int kSkinBlock = 128;
+
+// DQ skinning (DQSkinningGPUOp.cu:56-120), grid (vertex blocks, frames): the
+// frame's joint dual quaternions ([S][8]) and the block's top-K joint
+// indices and weights staged in shared memory, the base vertex and normal
+// read as one float4 each.  The blend runs the reference's slot loop on the
+// staged values: sign-aligned to the first dual quaternion, normalised when
+// its norm exceeds 1e-6, the same operations in the same order
+// (bit-identical to the reference kernel on the same inputs).
+__global__ void __launch_bounds__(kSkinBlock) k_dq_skin(Skel sk, int B, const float* __restrict__ dq,
+                                                        const float* __restrict__ w, float* __restrict__ out_v,
+                                                        float* __restrict__ out_n, float* __restrict__ w_copy,
+                                                        int vec) {
+    extern __shared__ float s_dyn[];
+    float* s_dq = s_dyn;
+    float* s_w = s_dq + sk.S * 8;
+    int* s_idx = reinterpret_cast<int*>(s_w + kSkinBlock * sk.K);
+    const int b = blockIdx.y;
+    const int v0 = stage_skin_block(sk, b, dq, 8, w, vec, s_dq, s_w, s_idx);
+    const int v = v0 + (int)threadIdx.x;
+    if (v >= sk.N) return;
+    const long long i = (long long)b * sk.N + v;
+    const int* I = s_idx + threadIdx.x * sk.K;
+    const float* Wt = s_w + threadIdx.x * sk.K;
+    float4 br = make_float4(0.f, 0.f, 0.f, 0.f), bt = br, first = br;
+    for (int k = 0; k < sk.K; ++k) {
+        const float* q = s_dq + I[k] * 8;
+        const float wk = Wt[k];
+        const float4 r = make_float4(q[0], q[1], q[2], q[3]), t = make_float4(q[4], q[5], q[6], q[7]);
+        float sign = 1.0f;
+        if (k == 0) first = r;
+        if (dot4(first, r) < 0.f && k != 0) sign = -1.0f;
+        br = add4(br, mul4(mul4(r, wk), sign));
+        bt = add4(bt, mul4(mul4(t, wk), sign));
+    }
     float scale = 1.f;
     const float len = sqrtf(dot4(br, br));
     if (len > 0.000001f) scale = 1.f / len;
     br = mul4(br, scale);
     bt = mul4(bt, scale);
-    const float3 p = dq_rot(br, ld3(sk.base_v + 3LL * v)) + dq_trans(br, bt);
+    const float4 bv = sk.base_v4[v], bn = sk.base_n4[v];
+    const float3 p = dq_rot(br, make_float3(bv.x, bv.y, bv.z)) + dq_trans(br, bt);
     float R[9];
     dq_rotmat(br, R);
-    const float3 n0 = ld3(sk.base_n + 3LL * v);
+    const float3 n0 = make_float3(bn.x, bn.y, bn.z);
     const float3 rn = make_float3(R[0] * n0.x + R[1] * n0.y + R[2] * n0.z, R[3] * n0.x + R[4] * n0.y + R[5] * n0.z,
                                   R[6] * n0.x + R[7] * n0.y + R[8] * n0.z);
     const float nr = 1.f / sqrtf(dot(rn, rn));
     st3(out_v + 3 * i, p);
     st3(out_n + 3 * i, rn * nr);
     if (w_copy)
-        for (int k = 0; k < sk.K; ++k) w_copy[i * sk.K + k] = w[i * sk.K + k];
+        for (int k = 0; k < sk.K; ++k) w_copy[i * sk.K + k] = Wt[k];
 }
 
-__global__ void k_lbs_skin(Skel sk, int B, const float* __restrict__ xf12, const float* __restrict__ w,
-                           const float* __restrict__ disp, float* __restrict__ out_v, float* __restrict__ out_n,
-                           float* __restrict__ w_copy) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)B * sk.N) return;
-    const int b = (int)(i / sk.N), v = (int)(i % sk.N);
+// LBS skinning (LBSkinningGPUOp.cu:49-96), grid (vertex blocks, frames): the
+// frame's joint transforms ([S][12]: rotation row-major, translation) and the
+// block's slots staged as in k_dq_skin; the reference's slot loop in its order.
+__global__ void __launch_bounds__(kSkinBlock) k_lbs_skin(Skel sk, int B, const float* __restrict__ xf12,
+                                                         const float* __restrict__ w, const float* __restrict__ disp,
+                                                         float* __restrict__ out_v, float* __restrict__ out_n,
+                                                         float* __restrict__ w_copy, int vec) {
+    extern __shared__ float s_dyn[];
+    float* s_xf = s_dyn;
+    float* s_w = s_xf + sk.S * 12;
+    int* s_idx = reinterpret_cast<int*>(s_w + kSkinBlock * sk.K);
+    const int b = blockIdx.y;
+    const int v0 = stage_skin_block(sk, b, xf12, 12, w, vec, s_xf, s_w, s_idx);
+    const int v = v0 + (int)threadIdx.x;
+    if (v >= sk.N) return;
+    const long long i = (long long)b * sk.N + v;
+    const int* I = s_idx + threadIdx.x * sk.K;
+    const float* Wt = s_w + threadIdx.x * sk.K;
     float R[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float3 t = make_float3(0.f, 0.f, 0.f);
     for (int k = 0; k < sk.K; ++k) {
-        const int s = sk.skin_idx[(long long)v * sk.K + k];
-        const float wk = w[i * sk.K + k];
-        const float* X = xf12 + ((long long)b * sk.S + s) * 12;
+        const float wk = Wt[k];
+        const float* X = s_xf + I[k] * 12;
         for (int c = 0; c < 9; ++c) R[c] = R[c] + X[c] * wk;
         t = t + make_float3(X[9], X[10], X[11]) * wk;
     }
     // the reference indexes the base mesh with the frame offset
     // (LBSkinningGPUOp.cu:83-84), out of bounds for B > 1; the base mesh is
     // shared by all frames here
-    const float3 p = ld3(sk.base_v + 3LL * v) + ld3(disp + 3 * i);
-    const float3 n0 = ld3(sk.base_n + 3LL * v);
+    const float4 bv = sk.base_v4[v], bn = sk.base_n4[v];
+    const float3 p = make_float3(bv.x, bv.y, bv.z) + ld3(disp + 3 * i);
+    const float3 n0 = make_float3(bn.x, bn.y, bn.z);
     const float3 o = make_float3(R[0] * p.x + R[1] * p.y + R[2] * p.z, R[3] * p.x + R[4] * p.y + R[5] * p.z,
                                  R[6] * p.x + R[7] * p.y + R[8] * p.z) + t;
     const float3 on = make_float3(R[0] * n0.x + R[1] * n0.y + R[2] * n0.z, R[3] * n0.x + R[4] * n0.y + R[5] * n0.z,
@@ -328,7 +405,7 @@ __global__ void k_lbs_skin(Skel sk, int B, const float* __restrict__ xf12, const
     st3(out_v + 3 * i, o);
     st3(out_n + 3 * i, on);
     if (w_copy)
-        for (int k = 0; k < sk.K; ++k) w_copy[i * sk.K + k] = w[i * sk.K + k];
+        for (int k = 0; k < sk.K; ++k) w_copy[i * sk.K + k] = Wt[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -741,7 +818,7 @@ struct hc_skin_s {
     int J = 0, D = 0, S = 0, K = 0, N = 0, E = 0;
     int parity = 1;
     DevBuf parent, type, offset, axis, jscale, dof_off, dof_joint, dof_w, skin_joint, skin_scale, t0inv, in_chain,
-        skin_idx, base_v, base_n;
+        skin_idx, base_v, base_n, base_v4, base_n4;
     DevBuf joints, params, skin_xf, mom, lbs_xf, gpos, gaxis, dq_ws, gdq;
     Skel skel() const {
         Skel s;
@@ -765,9 +842,29 @@ struct hc_skin_s {
         s.skin_idx = skin_idx.as<int>();
         s.base_v = base_v.as<float>();
         s.base_n = base_n.as<float>();
+        s.base_v4 = base_v4.as<float4>();
+        s.base_n4 = base_n4.as<float4>();
         return s;
     }
 };
+
+// Opt a kernel in to more than 48 KB of dynamic shared memory, once per device.
+template <typename K>
+static hc_status skin_allow_smem(K kernel, size_t bytes) {
+    static unsigned long long done = 0;  // one bit per device
+    if (bytes <= (48u << 10)) return HC_OK;
+    int dev = 0;
+    HC_CUDA(cudaGetDevice(&dev));
+    if (dev < 64 && (done >> dev & 1ull)) return HC_OK;
+    HC_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (dev < 64) done |= 1ull << dev;
+    return HC_OK;
+}
+
+// the skinning slots can be staged as int4 / float4: K a multiple of 4, 16-byte aligned arrays
+static int slots_by_four(const hc_skin_s* h, const float* weights) {
+    return h->K % 4 == 0 && ((uintptr_t)weights & 15) == 0 && ((uintptr_t)h->skin_idx.ptr & 15) == 0;
+}
 
 extern "C" hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_t* parent, const int32_t* joint_type,
                                     const float* offset, const float* axis, const float* joint_scale, int32_t n_dofs,
@@ -780,6 +877,8 @@ extern "C" hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_
     *out = nullptr;
     HC_REQUIRE(n_joints > 0 && n_dofs > 0 && n_skin > 0 && n_vertices > 0 && k > 0, "empty skeleton or mesh");
     HC_REQUIRE(n_skin <= 1024, "at most 1024 skinning joints (got %d)", n_skin);
+    HC_REQUIRE(skin_block_smem(n_skin, 12, k, kSkinBlock) <= (200u << 10),
+               "%d skinning joints with %d per vertex exceed the staged skinning block", n_skin, k);
     HC_REQUIRE(parent && joint_type && offset && axis && dof_offsets && dof_joint && dof_weight && skin_joint &&
                    base_vertices && base_normals && skin_index,
                "NULL skeleton / mesh array");
@@ -852,6 +951,15 @@ extern "C" hc_status hc_skin_create(hc_skin* out, int32_t n_joints, const int32_
     UP(skin_idx, skin_index, (long long)n_vertices * k);
     UP(base_v, base_vertices, 3LL * n_vertices);
     UP(base_n, base_normals, 3LL * n_vertices);
+    {
+        std::vector<float4> bv4((size_t)n_vertices), bn4((size_t)n_vertices);
+        for (int v = 0; v < n_vertices; ++v) {
+            bv4[v] = make_float4(base_vertices[3 * v], base_vertices[3 * v + 1], base_vertices[3 * v + 2], 0.f);
+            bn4[v] = make_float4(base_normals[3 * v], base_normals[3 * v + 1], base_normals[3 * v + 2], 0.f);
+        }
+        UP(base_v4, bv4.data(), bv4.size());
+        UP(base_n4, bn4.data(), bn4.size());
+    }
 #undef UP
     if (st != HC_OK) {
         delete h;
@@ -921,9 +1029,11 @@ extern "C" hc_status hc_dq_skinning_forward(hc_skin h, void* stream, int32_t bat
     const int BS = batch * h->S;
     k_dq_from_xf<<<div_up(BS, 128), 128, 0, s>>>(BS, h->skin_xf.as<Xf>(), dual_quaternions);
     HC_CHECK_LAUNCH();
-    k_dq_skin<<<div_up((long long)batch * h->N, 128), 128, 0, s>>>(h->skel(), batch, dual_quaternions,
-                                                                    skinning_weights, skinned_vertex_positions,
-                                                                    skinned_vertex_normals, output_skinning_weights);
+    HC_REQUIRE(batch <= 65535, "too many frames in one call (%d)", batch);
+    HC_TRY(skin_allow_smem(k_dq_skin, skin_block_smem(h->S, 8, h->K, kSkinBlock)));
+    k_dq_skin<<<dim3(div_up(h->N, kSkinBlock), batch), kSkinBlock, skin_block_smem(h->S, 8, h->K, kSkinBlock), s>>>(
+        h->skel(), batch, dual_quaternions, skinning_weights, skinned_vertex_positions, skinned_vertex_normals,
+        output_skinning_weights, slots_by_four(h, skinning_weights));
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
@@ -976,10 +1086,11 @@ extern "C" hc_status hc_lb_skinning_forward(hc_skin h, void* stream, int32_t bat
     const int BS = batch * h->S;
     k_xf_to_lbs<<<div_up(BS, 128), 128, 0, s>>>(BS, h->skin_xf.as<Xf>(), transformation);
     HC_CHECK_LAUNCH();
-    k_lbs_skin<<<div_up((long long)batch * h->N, 128), 128, 0, s>>>(h->skel(), batch, transformation,
-                                                                     skinning_weights, displacement,
-                                                                     skinned_vertex_positions, skinned_vertex_normals,
-                                                                     output_skinning_weights);
+    HC_REQUIRE(batch <= 65535, "too many frames in one call (%d)", batch);
+    HC_TRY(skin_allow_smem(k_lbs_skin, skin_block_smem(h->S, 12, h->K, kSkinBlock)));
+    k_lbs_skin<<<dim3(div_up(h->N, kSkinBlock), batch), kSkinBlock, skin_block_smem(h->S, 12, h->K, kSkinBlock), s>>>(
+        h->skel(), batch, transformation, skinning_weights, displacement, skinned_vertex_positions,
+        skinned_vertex_normals, output_skinning_weights, slots_by_four(h, skinning_weights));
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
