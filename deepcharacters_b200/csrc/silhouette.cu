@@ -136,8 +136,9 @@ __global__ void k_boundary(int B, int C, int N, int W, int H, const float* __res
 // raster (Skeletool/Mesh/CUDABasedRasterization.cu:80-145): every pixel of a
 // triangle's clamped bounding box whose centre has image-space barycentrics
 // within [-0.001, 1.001] is marked covered.  The barycentric expressions keep
-// the reference's operation order, so coverage is bit-identical; only
-// "covered" is ever written, so unordered stores need no atomics.  Pixels
+// the reference's operation order, so coverage is bit-identical.  The binned
+// passes only ever write "covered", so their unordered stores need no
+// atomics (the hinted set-up, a kernel before them, also writes "open").  Pixels
 // outside a triangle's conservative footprint (widened by the -0.001
 // tolerance and the test's rounding error, see Footprint) are never tested
 // against it: they cannot pass the exact test.
@@ -308,7 +309,18 @@ struct CovBins {
     CovTileTri* rec;   // [V*F]
     unsigned char* cover;       // coverage image, the layout's pixels
     const unsigned char* need;  // [tiles of the call] tiles with a pixel still open (NULL: every tile)
+    const int* need_sum;        // [tiles of the call] per view: inclusive 2-D prefix sums of need (NULL: none)
 };
+
+// needed tiles of a view in the tile box [tx0, tx1] x [ty0, ty1] (inclusive),
+// from the view's 2-D prefix sums S (row-major, tiles_x per row)
+__device__ __forceinline__ int need_in_box(const int* S, int tiles_x, int tx0, int ty0, int tx1, int ty1) {
+    const int a = S[ty1 * tiles_x + tx1];
+    const int b = ty0 > 0 ? S[(ty0 - 1) * tiles_x + tx1] : 0;
+    const int c = tx0 > 0 ? S[ty1 * tiles_x + tx0 - 1] : 0;
+    const int d = ty0 > 0 && tx0 > 0 ? S[(ty0 - 1) * tiles_x + tx0 - 1] : 0;
+    return a - b - c + d;
+}
 
 // the pixels of one tile that a triangle covers, written at once (a pair
 // beyond the tile's bin capacity)
@@ -320,42 +332,81 @@ __device__ void cov_sweep(const CovBins& cb, const ViewImg& vi, int tile, const 
             if (cover_record_test(e, u, v)) img[(long long)v * vi.W + u] = 1;
 }
 
-// Coverage from a per-pixel face hint (a renderer face buffer of the same
-// views): a pixel is covered when the reference's 2-D test passes for its hint
-// face, which is checked here exactly; every other pixel stays open for the
-// binned passes, and a tile is marked as needing them when it has an open
-// pixel.  Any hint gives the same coverage; a good one only saves work.
-// one warp per (view, 8x8 tile), two pixels per lane
-__global__ void __launch_bounds__(256) k_cov_hint(int N, int F, long long n_keys, const int* __restrict__ faces,
-                                                  const float2* __restrict__ p2d, const int* __restrict__ hint,
-                                                  CovBins cb, unsigned char* __restrict__ need,
-                                                  const __grid_constant__ ImgLayout L) {
-    const long long key = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (key >= n_keys) return;  // warp-uniform
-    int tile;
-    const int view = view_of_tile(L, key, tile);
+// Boundary flags from a per-pixel face hint (a renderer face buffer of the
+// same views).  The flag of a vertex reads coverage only in the 3x3 window
+// around its projection, and a window pixel is covered when the reference's
+// 2-D test passes for its hint face, which is checked here exactly.  A vertex
+// whose window lies in the image with all nine pixels covered that way is not
+// on the boundary.  Every other window pixel is written open (0) to the
+// coverage image and its tile is marked as needing the binned passes; the
+// vertex is flagged kPending and resolved from the coverage image after them.
+// Any hint gives the flags of the unhinted op; a good one only saves work.
+// Pixels outside every pending window are never read, so the binned passes
+// need not see them, and every value written here is the same from every
+// window that holds the pixel.
+constexpr unsigned char kPending = 2;
+
+__global__ void k_bnd_hint(long long n, int N, int F, const __grid_constant__ ImgLayout L,
+                           const float2* __restrict__ p2d, const int* __restrict__ faces,
+                           const int* __restrict__ hint, unsigned char* __restrict__ cover,
+                           unsigned char* __restrict__ need, unsigned char* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int view = (int)(i / N);
     const ViewImg vi = view_img(L, view);
-    const int ty = tile / vi.tiles_x, tx = tile - ty * vi.tiles_x;
-    bool covered = true;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int q = lane + 32 * h;
-        const int px = tx * kCovTile + q % kCovTile, py = ty * kCovTile + q / kCovTile;
-        if (px >= vi.W || py >= vi.H) continue;
-        const long long pix = vi.pix + (long long)py * vi.W + px;
-        const int f = hint[pix];
-        bool c = false;
-        if (f >= 0 && f < F) {
-            CoverTri t;
-            cover_tri(view, f, N, vi.W, vi.H, faces, p2d, t);
-            c = px >= t.x0 && px <= t.x1 && py >= t.y0 && py <= t.y1 && cover_test(t, px + 0.5f, py + 0.5f);
-        }
-        cb.cover[pix] = c ? 1 : 0;
-        covered = covered && c;
+    const int W = vi.W, H = vi.H;
+    const float2 q = p2d[i];
+    const int u = (int)q.x, v = (int)q.y;
+    unsigned char r = 0;
+    if (u - 1 >= 0 && u + 1 < W && v - 1 >= 0 && v + 1 < H) {
+        int last = -1;
+        CoverTri t;
+        for (int rr = v - 1; rr <= v + 1; ++rr)
+            for (int c = u - 1; c <= u + 1; ++c) {
+                const long long pix = vi.pix + (long long)rr * W + c;
+                const int f = hint[pix];
+                bool cov = false;
+                if (f >= 0 && f < F) {
+                    if (f != last) {  // neighbouring pixels mostly share their hint face
+                        cover_tri(view, f, N, W, H, faces, p2d, t);
+                        last = f;
+                    }
+                    cov = c >= t.x0 && c <= t.x1 && rr >= t.y0 && rr <= t.y1 && cover_test(t, c + 0.5f, rr + 0.5f);
+                }
+                cover[pix] = cov ? 1 : 0;
+                if (!cov) {
+                    need[vi.tile + (long long)(rr / kCovTile) * vi.tiles_x + c / kCovTile] = 1;
+                    r = kPending;
+                }
+            }
     }
-    const bool all = __all_sync(0xffffffffu, covered);
-    if (lane == 0) need[key] = all ? 0 : 1;
+    out[i] = r;
+}
+
+// Per view, the inclusive 2-D prefix sums of the needed-tile flags (one CTA
+// per view: rows, then columns), so that the binning pass drops a triangle
+// whose tile box holds no needed tile with four loads.
+__global__ void k_need_sum(const __grid_constant__ ImgLayout L, const unsigned char* __restrict__ need,
+                           int* __restrict__ sum) {
+    const ViewImg vi = view_img(L, blockIdx.x);
+    const int tx = vi.tiles_x, ty = (vi.H + kCovTile - 1) / kCovTile;
+    const unsigned char* nd = need + vi.tile;
+    int* S = sum + vi.tile;
+    for (int y = threadIdx.x; y < ty; y += blockDim.x) {
+        int acc = 0;
+        for (int x = 0; x < tx; ++x) {
+            acc += nd[y * tx + x];
+            S[y * tx + x] = acc;
+        }
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < tx; x += blockDim.x) {
+        int acc = 0;
+        for (int y = 0; y < ty; ++y) {
+            acc += S[y * tx + x];
+            S[y * tx + x] = acc;
+        }
+    }
 }
 
 // One thread per (view, triangle): its record, then its tiles.  Boxes of up
@@ -386,14 +437,10 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
     const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
     const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
     int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
-    if (cb.need && nt > 0 && nt <= kCovSmall) {  // a small box whose tiles are all covered already needs nothing
-        bool any = false;
-        for (int k = 0; k < nt; ++k)
-            any = any || cb.need[vi.tile + (ty0 + k / ntx) * vi.tiles_x + tx0 + k % ntx];
-        if (!any) {
-            nonempty = false;
-            nt = 0;
-        }
+    if (cb.need_sum && nt > 0 &&  // a box without a needed tile needs nothing
+        need_in_box(cb.need_sum + vi.tile, vi.tiles_x, tx0, ty0, t.x1 / kCovTile, t.y1 / kCovTile) == 0) {
+        nonempty = false;
+        nt = 0;
     }
     if (nonempty) {
         fp = cover_footprint(t, vi.W, vi.H);
@@ -491,12 +538,14 @@ __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long lon
     }
 }
 
-// boundary test of k_boundary against the coverage image instead of a face buffer
+// boundary test of k_boundary against the coverage image instead of a face
+// buffer; after k_bnd_hint only its pending vertices are evaluated
 __global__ void k_boundary_cover(int B, int C, int N, const __grid_constant__ ImgLayout L,
                                  const float* __restrict__ p2d, const unsigned char* __restrict__ cover,
-                                 unsigned char* __restrict__ out) {
+                                 bool pending_only, unsigned char* __restrict__ out) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)B * C * N) return;
+    if (pending_only && out[i] != kPending) return;
     const ViewImg vi = view_img(L, (int)(i / N));
     const int W = vi.W, H = vi.H;
     const int u = (int)p2d[2 * i], v = (int)p2d[2 * i + 1];
@@ -1012,7 +1061,7 @@ bool pixels_by_four(const ImgLayout& L) {
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover, count, bins, rec, need;
+    DevBuf faces, p2d, cover, count, bins, rec, need, need_sum;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -1043,6 +1092,7 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     h->bins.release();
     h->rec.release();
     h->need.release();
+    h->need_sum.release();
     delete h;
     return HC_OK;
 }
@@ -1055,6 +1105,7 @@ static hc_status mesh_boundary_reserve_layout(hc_mesh_boundary h, long long view
     HC_TRY(h->bins.ensure(sizeof(int) * frames * (size_t)L.T * kCovCap));
     HC_TRY(h->rec.ensure(sizeof(CovTileTri) * (size_t)views * h->F));
     HC_TRY(h->need.ensure(frames * (size_t)L.T));
+    HC_TRY(h->need_sum.ensure(sizeof(int) * frames * (size_t)L.T));
     return HC_OK;
 }
 
@@ -1102,12 +1153,19 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     cb.cover = h->cover.as<unsigned char>();
     cb.rec = h->rec.as<CovTileTri>();
     cb.need = nullptr;
-    if (face_hint) {  // writes every pixel of the coverage image and the per-tile flags
-        k_cov_hint<<<div_up(n_keys * 32, 256), 256, 0, s>>>(h->N, h->F, n_keys, h->faces.as<int>(),
-                                                             reinterpret_cast<const float2*>(p2d), face_hint, cb,
-                                                             h->need.as<unsigned char>(), L);
+    cb.need_sum = nullptr;
+    if (face_hint) {
+        // final flags of the vertices whose window the hint covers; open
+        // window pixels and their tiles for the binned passes
+        HC_CUDA(cudaMemsetAsync(h->need.ptr, 0, (size_t)n_keys, s));
+        k_bnd_hint<<<div_up(nv, 256), 256, 0, s>>>(nv, h->N, h->F, L, reinterpret_cast<const float2*>(p2d),
+                                                   h->faces.as<int>(), face_hint, h->cover.as<unsigned char>(),
+                                                   h->need.as<unsigned char>(), is_boundary);
+        HC_CHECK_LAUNCH();
+        k_need_sum<<<(unsigned)views, 128, 0, s>>>(L, h->need.as<unsigned char>(), h->need_sum.as<int>());
         HC_CHECK_LAUNCH();
         cb.need = h->need.as<unsigned char>();
+        cb.need_sum = h->need_sum.as<int>();
     } else {
         HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)(frames * L.P), s));
     }
@@ -1129,7 +1187,7 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     }
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, L, p2d, h->cover.as<unsigned char>(),
-                                                     is_boundary);
+                                                     face_hint != nullptr, is_boundary);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }

@@ -445,9 +445,11 @@ hc_status hc_mesh_boundary_forward(hc_mesh_boundary h, void* stream, int32_t bat
                                    const float* points_image_space, uint8_t* is_boundary);
 /* hc_mesh_boundary_forward with a per-pixel face hint: face_hint [B,C,H,W]
  * int32, e.g. the face buffer of hc_renderer_forward for the same vertices,
- * cameras and resolution.  A pixel whose hint face passes the op's own 2-D
- * coverage test (checked exactly) is covered; every other pixel and the tiles
- * that hold one go through the full binned coverage.  The flags are
+ * cameras and resolution.  A vertex's flag reads the 3x3 pixel window around
+ * its projection; a window pixel whose hint face passes the op's own 2-D
+ * coverage test (checked exactly) is covered, and only the other pixels of
+ * those windows, with the tiles that hold them, go through the full binned
+ * coverage.  The flags are
  * bit-identical to hc_mesh_boundary_forward for every hint (out-of-range ids
  * count as no hint); a hint that matches the coverage only saves work.  No
  * reference counterpart (the reference op rasterises the whole mesh again). */
