@@ -232,7 +232,10 @@ __device__ __forceinline__ Footprint footprint(float3 p0, float3 p1, float3 p2, 
         const float len = sqrtf(ex * ex + ey * ey);
         if (!(len > 1e-6f)) ok = false;
         const float inv = ok ? sg / len : 0.f;
-        const float margin = kEdgeMargin + (ok ? rel_margin * fabsf(area) / len + num_err / len : 0.f);
+        // (the widenings are skipped when both are zero: 0 / len is not
+        // folded away by the compiler, and adds nothing)
+        const bool widen = ok && (rel_margin != 0.f || num_err != 0.f);
+        const float margin = kEdgeMargin + (widen ? rel_margin * fabsf(area) / len + num_err / len : 0.f);
         // signed distance of (x, y) from the edge u -> w, positive on the inside
         fp.a[k] = -ey * inv;
         fp.b[k] = ex * inv;

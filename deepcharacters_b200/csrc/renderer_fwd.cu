@@ -286,18 +286,22 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
     int maxnt = my_nt;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
+    int cx = 0, cy = 0;  // column / row of tile k in the box, stepped without a division
     for (int k = 0; k < maxnt; ++k) {
         bool act = k < my_nt;
         long long key = -1;
+        const int tx = tx0 + cx, ty = ty0 + cy;
+        if (++cx == ntx) {
+            cx = 0;
+            ++cy;
+        }
         if (act) {
-            const int tx = tx0 + k % ntx;
-            const int ty = ty0 + k / ntx;
             // tiles of the box that the triangle's footprint misses get no entry
             act = nt == 1 || footprint_overlaps(fp, max(tx * TS, x0), min(tx * TS + TS - 1, x1), max(ty * TS, y0),
                                                 min(ty * TS + TS - 1, y1));
             if (act) key = tile_base + ty * tiles_x + tx;
         }
-        const unsigned same = __match_any_sync(0xffffffffu, key);
+        const unsigned same = __match_any_sync(0xffffffffu, (int)key);  // tiles of the call fit 31 bits
         if (!act) continue;
         const int leader = __ffs(same) - 1;
         const int rank = __popc(same & ((1u << lane) - 1u));
@@ -325,9 +329,18 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
         }
         const int qtx0 = qx0 / TS, qty0 = qy0 / TS, qntx = qx1 / TS - qtx0 + 1;
         const int qnt = qntx * (qy1 / TS - qty0 + 1);
+        // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32
+        const int step_r = 32 / qntx, step_c = 32 - step_r * qntx;
+        int cr = (int)lane / qntx, cc = (int)lane - cr * qntx;
         for (int k = lane; k < qnt; k += 32) {
-            const int tx = qtx0 + k % qntx;
-            const int ty = qty0 + k / qntx;
+            const int tx = qtx0 + cc;
+            const int ty = qty0 + cr;
+            cc += step_c;
+            cr += step_r;
+            if (cc >= qntx) {
+                cc -= qntx;
+                ++cr;
+            }
             if (!footprint_overlaps(qfp, max(tx * TS, qx0), min(tx * TS + TS - 1, qx1), max(ty * TS, qy0),
                                     min(ty * TS + TS - 1, qy1)))
                 continue;
@@ -970,6 +983,7 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     k_project_vertices<<<div_up((long long)V * N, 256), 256, 0, s>>>(V, C, N, verts, cams, ws.proj.as<float4>());
     HC_CHECK_LAUNCH();
     HC_REQUIRE(V <= 65535, "too many views in one call (%d)", V);
+    HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
     k_bin<<<dim3(div_up(F, 256), V), 256, 0, s>>>(
         V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), ws.proj.as<float4>(), cams, tf, tv, tstate,
         ws.bins.as<int>(),
