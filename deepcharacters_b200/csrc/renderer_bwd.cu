@@ -72,28 +72,12 @@ __device__ __forceinline__ float3 unit3(int k) {
     return make_float3(k == 0 ? 1.f : 0.f, k == 1 ? 1.f : 0.f, k == 2 ? 1.f : 0.f);
 }
 
-// cross(e_k, b) and cross(a, e_k) for the unit vector e_k.  The general form
-// multiplies by 0 and 1, which the compiler must keep (0 * x is not 0 for
-// every float); those products are exact, so these permutations give the
-// same values without them.
-__device__ __forceinline__ float3 ucross_l(float3 b, int k) {
-    return k == 0 ? make_float3(0.f, -b.z, b.y) : (k == 1 ? make_float3(b.z, 0.f, -b.x) : make_float3(-b.y, b.x, 0.f));
-}
-__device__ __forceinline__ float3 ucross_r(float3 a, int k) {
-    return k == 0 ? make_float3(0.f, a.z, -a.y) : (k == 1 ? make_float3(-a.z, 0.f, a.x) : make_float3(a.y, -a.x, 0.f));
-}
-__device__ __forceinline__ float comp3(float3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
-
 // d(a, b)/d(v0, v1, v2): the barycentric Jacobian of the reference's
 // dJBCDVerpos (RendererUtil.h:670-861) for a = dot(N, C1)/|N|^2 (weight of
 // v0) and b = dot(N, C2)/|N|^2 (weight of v1), in unscaled (mm) coordinates,
 // contracted with the gradient w.r.t. the three barycentrics as it is formed:
 // gp[var] = g.x * ja[var] + g.y * jb[var] + g.z * (-ja[var] - jb[var]), the
 // reference's 3x9 product, one column at a time (no 2 x 9 row arrays live).
-// The perturbation of vertex `vert` along axis k enters as the unit vector
-// e_k: the cross products with it (dN, and dE x vp) and dot(dv0, N) are
-// written as the exact values they take, and every product of two computed
-// values keeps its form, so the arithmetic that rounds is the reference's.
 // Leaves gp at zero for grazing rays or degenerate triangles.
 __device__ __forceinline__ void bary_jacobian_apply(float3 o, float3 d, float3 v0, float3 v1, float3 v2, float3 g,
                                                     float gp[9]) {
@@ -118,26 +102,21 @@ __device__ __forceinline__ void bary_jacobian_apply(float3 o, float3 d, float3 v
     const float inv_den2 = -1.f / (denom * denom);
 #pragma unroll
     for (int var = 0; var < 9; ++var) {
-        const int vert = var / 3, k = var % 3;
-        const float3 ek = unit3(k);
+        const int vert = var / 3;
+        const float3 ek = unit3(var % 3);
         const float3 z = make_float3(0.f, 0.f, 0.f);
         float3 dN;
-        if (vert == 0) dN = ucross_r(e02, k) + ucross_l(e01, k);
-        else if (vert == 1) dN = ucross_l(e02, k);
-        else dN = ucross_r(e01, k);
+        if (vert == 0) dN = cross(-ek, e02) + cross(e01, -ek);
+        else if (vert == 1) dN = cross(ek, e02);
+        else dN = cross(e01, ek);
+        const float3 dv0 = vert == 0 ? ek : z;
         const float3 dv1 = vert == 1 ? ek : z;
         const float3 dv2 = vert == 2 ? ek : z;
-        // dot(dv0, N) is N_k for vertex 0 and zero otherwise
-        const float dt = vert == 0 ? inv_ndr2 * dot(dN, d) * v0moN + inv_ndr * (comp3(N, k) + dot(v0mo, dN))
-                                   : inv_ndr2 * dot(dN, d) * v0moN + inv_ndr * dot(v0mo, dN);
+        const float dt = inv_ndr2 * dot(dN, d) * v0moN + inv_ndr * (dot(dv0, N) + dot(v0mo, dN));
+        const float3 dE0 = dv2 - dv1, dE1 = dv0 - dv2;
         const float nd = 2.f * dot(N, dN);
-        // cross(dE0, vp0) + cross(E0, dt d - dv1) with dE0 = dv2 - dv1, and
-        // cross(dE1, vp1) + cross(E1, dt d - dv2) with dE1 = dv0 - dv2
-        const float3 c0 = cross(E0, dt * d - dv1), c1 = cross(E1, dt * d - dv2);
-        const float3 s0 = vert == 1 ? c0 - ucross_l(vp0, k) : (vert == 2 ? ucross_l(vp0, k) + c0 : c0);
-        const float3 s1 = vert == 0 ? ucross_l(vp1, k) + c1 : (vert == 2 ? c1 - ucross_l(vp1, k) : c1);
-        const float dtmp0 = dot(dN, C0) + dot(N, s0);
-        const float dtmp1 = dot(dN, C1) + dot(N, s1);
+        const float dtmp0 = dot(dN, C0) + dot(N, cross(dE0, vp0) + cross(E0, dt * d - dv1));
+        const float dtmp1 = dot(dN, C1) + dot(N, cross(dE1, vp1) + cross(E1, dt * d - dv2));
         const float ja = dtmp0 * inv_den + tmp0 * inv_den2 * nd;
         const float jb = dtmp1 * inv_den + tmp1 * inv_den2 * nd;
         gp[var] = g.x * ja + g.y * jb + g.z * (-ja - jb);
