@@ -382,7 +382,8 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
 #pragma unroll
     for (int k = 0; k < 9; ++k) gp[k] = 0.f;
     float3 gA = make_float3(0.f, 0.f, 0.f), gnu = make_float3(0.f, 0.f, 0.f);
-    // carried from the first half of the pixel work (no target reads) to the second
+    // carried from the first half of the pixel work to the second (with cp.async
+    // staging the first half reads no staged target: its copies are in flight)
     float3 d = make_float3(0.f, 0.f, 1.f), v0 = d, v1 = d, v2 = d, G = d, frag = d;
     float3 gbc = make_float3(0.f, 0.f, 0.f);  // d loss / d (a, b, c)
     if (f >= 0) {
@@ -405,7 +406,14 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         if (A.l1_state) {  // d L1 / d render (k_l1_grad's arithmetic)
             G = make_float3(0.f, 0.f, 0.f);
             if (!A.l1_mask || A.l1_mask[pix]) {
-                const float3 r = ld3(A.l1_render + 3 * pix), t = ld3(A.target + 3 * pix);
+                const float3 r = ld3(A.l1_render + 3 * pix);
+                float3 t;
+                if (tma) {  // this tile's target is in shared memory already (the centre tap)
+                    const float4 c = s_tgt[(py - ty0 + A.ifs) * e_st + (px - tx0 + A.ifs)];
+                    t = make_float3(c.x, c.y, c.z);
+                } else {
+                    t = ld3(A.target + 3 * pix);
+                }
                 G = make_float3(l1_grad(l1_diff(r.x, t.x), l1_scale), l1_grad(l1_diff(r.y, t.y), l1_scale),
                                 l1_grad(l1_diff(r.z, t.z), l1_scale));
             }
