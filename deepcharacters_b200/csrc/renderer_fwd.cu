@@ -280,35 +280,21 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
     BinSink sink{TS, cap, tile_state, bins, spill, spill_cap, spill_keys, spill_tile_cap, stats};
     unsigned long long nbinned = 0;
     const unsigned lane = threadIdx.x & 31;
-    // boxes of up to kBinSmall tiles: lanes walk their tile lists in lock
-    // step and lanes that hit the same tile share one counter atomic
+    // boxes of up to kBinSmall tiles: each lane walks its own box
     const int my_nt = big ? 0 : nt;
-    int maxnt = my_nt;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
     int cx = 0, cy = 0;  // column / row of tile k in the box, stepped without a division
-    for (int k = 0; k < maxnt; ++k) {
-        bool act = k < my_nt;
-        long long key = -1;
+    for (int k = 0; k < my_nt; ++k) {
         const int tx = tx0 + cx, ty = ty0 + cy;
         if (++cx == ntx) {
             cx = 0;
             ++cy;
         }
-        if (act) {
-            // tiles of the box that the triangle's footprint misses get no entry
-            act = nt == 1 || footprint_overlaps(fp, max(tx * TS, x0), min(tx * TS + TS - 1, x1), max(ty * TS, y0),
-                                                min(ty * TS + TS - 1, y1));
-            if (act) key = tile_base + ty * tiles_x + tx;
-        }
-        const unsigned same = __match_any_sync(0xffffffffu, (int)key);  // tiles of the call fit 31 bits
-        if (!act) continue;
-        const int leader = __ffs(same) - 1;
-        const int rank = __popc(same & ((1u << lane) - 1u));
-        int base = 0;
-        if ((int)lane == leader) base = atomicAdd(&tile_state[key].x, __popc(same));
-        base = __shfl_sync(same, base, leader);
-        nbinned += sink.place(base + rank, key, view, (int)(key - tile_base), f);
+        // tiles of the box that the triangle's footprint misses get no entry
+        if (nt > 1 && !footprint_overlaps(fp, max(tx * TS, x0), min(tx * TS + TS - 1, x1), max(ty * TS, y0),
+                                          min(ty * TS + TS - 1, y1)))
+            continue;
+        const long long key = tile_base + ty * tiles_x + tx;
+        nbinned += sink.place(atomicAdd(&tile_state[key].x, 1), key, view, (int)(key - tile_base), f);
     }
     // larger boxes: the warp takes them one at a time, a tile per lane
     unsigned pending = __ballot_sync(0xffffffffu, big);
