@@ -410,9 +410,9 @@ __global__ void k_need_sum(const __grid_constant__ ImgLayout L, const unsigned c
 }
 
 // One thread per (view, triangle): its record, then its tiles.  Boxes of up
-// to kCovSmall tiles are binned by their own thread, lanes that hit the same tile
-// sharing one counter atomic; larger boxes are taken by the whole warp, a
-// tile per lane, reading the record back from global memory.
+// to kCovSmall tiles are binned by their own thread, one counter atomic per
+// entry; larger boxes are taken by the whole warp, a tile per lane, reading
+// the record back from global memory.
 __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
                           CovBins cb, const __grid_constant__ ImgLayout L) {
     // grid (triangle blocks, views): no 64-bit division per thread
@@ -448,29 +448,20 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
     }
     const bool big = nt > kCovSmall;
     const int my_nt = big ? 0 : nt;
-    int maxnt = my_nt;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxnt = max(maxnt, __shfl_xor_sync(0xffffffffu, maxnt, o));
-    for (int k = 0; k < maxnt; ++k) {
-        bool act = k < my_nt;
-        long long key = -1;
-        int tile = 0;
-        if (act) {
-            const int tx = tx0 + k % ntx, ty = ty0 + k / ntx;
-            act = nt == 1 || footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
-                                                max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1));
-            tile = ty * vi.tiles_x + tx;
-            if (act && cb.need && !cb.need[vi.tile + tile]) act = false;
-            if (act) key = vi.tile + tile;
+    int cx = 0, cy = 0;  // column / row of tile k in the box, stepped without a division
+    for (int k = 0; k < my_nt; ++k) {  // each lane walks its own small box
+        const int tx = tx0 + cx, ty = ty0 + cy;
+        if (++cx == ntx) {
+            cx = 0;
+            ++cy;
         }
-        const unsigned same = __match_any_sync(0xffffffffu, key);
-        if (!act) continue;
-        const int leader = __ffs(same) - 1;
-        const int rank = __popc(same & ((1u << lane) - 1u));
-        int base = 0;
-        if ((int)lane == leader) base = atomicAdd(cb.count + key, __popc(same));
-        base = __shfl_sync(same, base, leader);
-        const int slot = base + rank;
+        if (nt > 1 && !footprint_overlaps(fp, max(tx * kCovTile, t.x0), min(tx * kCovTile + kCovTile - 1, t.x1),
+                                          max(ty * kCovTile, t.y0), min(ty * kCovTile + kCovTile - 1, t.y1)))
+            continue;
+        const int tile = ty * vi.tiles_x + tx;
+        if (cb.need && !cb.need[vi.tile + tile]) continue;
+        const long long key = vi.tile + tile;
+        const int slot = atomicAdd(cb.count + key, 1);
         if (slot < kCovCap)
             cb.bins[key * kCovCap + slot] = f;
         else
@@ -488,8 +479,17 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
         const int qx0 = q.bb.x & 0xffff, qx1 = q.bb.x >> 16, qy0 = q.bb.y & 0xffff, qy1 = q.bb.y >> 16;
         const int qtx0 = qx0 / kCovTile, qty0 = qy0 / kCovTile, qntx = qx1 / kCovTile - qtx0 + 1;
         const int qnt = qntx * (qy1 / kCovTile - qty0 + 1);
+        // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32
+        const int step_r = 32 / qntx, step_c = 32 - step_r * qntx;
+        int cr = (int)lane / qntx, cc = (int)lane - cr * qntx;
         for (int k = lane; k < qnt; k += 32) {
-            const int tx = qtx0 + k % qntx, ty = qty0 + k / qntx;
+            const int tx = qtx0 + cc, ty = qty0 + cr;
+            cc += step_c;
+            cr += step_r;
+            if (cc >= qntx) {
+                cc -= qntx;
+                ++cr;
+            }
             if (!footprint_overlaps(qfp, max(tx * kCovTile, qx0), min(tx * kCovTile + kCovTile - 1, qx1),
                                     max(ty * kCovTile, qy0), min(ty * kCovTile + kCovTile - 1, qy1)))
                 continue;
