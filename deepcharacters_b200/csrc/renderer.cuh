@@ -153,6 +153,22 @@ __device__ __forceinline__ bool ray_tri(float3 ro_s, float3 dir, const TriS& T, 
     return true;
 }
 
+// Barycentrics of a pixel's known winner: the operations of ray_tri that
+// form a and b, without the sign and window checks that the winner has
+// passed (so the values are ray_tri's).
+__device__ __forceinline__ void winner_bary(float3 ro_s, float3 dir, const TriS& T, float num, float& a, float& b) {
+    const float ndr = dot(dir, T.n);
+    const float t = num / ndr;
+    const float3 P = ro_s + t * dir;
+    float3 C = cross(T.s2 - T.s1, P - T.s1);
+    a = dot(T.n, C);
+    C = cross(T.s0 - T.s2, P - T.s2);
+    b = dot(T.n, C);
+    const float denom = dot(T.n, T.n);
+    a /= denom;
+    b /= denom;
+}
+
 // Hit accepted by the depth pass: barycentric window of
 // CUDABasedRasterization.cu:243 and the quantised depth int(t * 1e4) of :247-250.
 __device__ __forceinline__ bool raster_hit(float3 ro_s, float3 dir, const TriS& T, float num,

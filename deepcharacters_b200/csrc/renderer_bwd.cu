@@ -10,8 +10,8 @@
 //  * the barycentric Jacobian is the exact rank-1 form (below) instead of the
 //    reference's 3x9 product (which is kept as the parity mode);
 //  * per-vertex contributions (position, colour, pixel-normal gradients) are
-//    merged inside each warp (lanes matched by vertex id, one leader sums its
-//    group) before one global reduction per vertex per warp;
+//    merged inside each warp (lanes matched by face id, a leader sums up to
+//    8 members) before one global reduction per vertex and leader;
 //  * SH gradients are reduced over the CTA (warp shuffles) before one atomic
 //    per coefficient;
 //  * the shaded-mode normal chain is split in two: pixels accumulate the
@@ -610,9 +610,11 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         }
     }
     // per-vertex contributions, merged inside the warp: lanes are matched by
-    // face id (a face fixes all three vertices) and the lowest lane of each
-    // group sums the group's rows from shared memory and issues one reduction
-    // per value and vertex
+    // face id (a face fixes all three vertices), and every 8th member of a
+    // group (by lane order) sums its own row and the next 7 members' rows from
+    // shared memory and issues one reduction per value and vertex.  The cap
+    // bounds the loop (unrolled, its loads issue together) at the cost of a
+    // second set of reductions for the rare group of more than 8 lanes.
     {
         float* row = s_red[warp][lane];
 #pragma unroll
@@ -631,11 +633,13 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         }
         __syncwarp();
         const unsigned grp = __match_any_sync(0xffffffffu, f);
-        if (f >= 0 && lane == __ffs(grp) - 1) {
+        const int rank = __popc(grp & ((1u << lane) - 1u));
+        if (f >= 0 && rank % 8 == 0) {  // leader of up to 8 members: itself and the next 7
             float4 acc[NROW / 4];
 #pragma unroll
             for (int k = 0; k < NROW / 4; ++k) acc[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (unsigned mm = grp; mm; mm &= mm - 1) {
+            unsigned mm = grp & ~((1u << lane) - 1u);
+            for (int q = 0; q < 8 && mm; ++q, mm &= mm - 1) {
                 const float4* r = reinterpret_cast<const float4*>(s_red[warp][__ffs(mm) - 1]);
 #pragma unroll
                 for (int k = 0; k < NROW / 4; ++k) {

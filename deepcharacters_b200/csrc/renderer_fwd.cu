@@ -795,9 +795,8 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                 Tw = tri_from(tri_frame[(long long)b * A.F + best_f]);
                 wnum = tri_view[(long long)view * A.F + best_f].num;
             }
-            int dq;
-            float a = 0.f, bb = 0.f;
-            raster_hit(ro_s, dir, Tw, wnum, dq, a, bb);
+            float a, bb;
+            winner_bary(ro_s, dir, Tw, wnum, a, bb);
             // every load of the shading before the first store of the pixel
             const float3 col = shade_pixel(A, cam, view, b, best_f, a, bb, dir);
             A.face[pix] = best_f;
