@@ -455,7 +455,8 @@ def run_ours(args, world, rank, local):
     traffic_path = os.path.join(ROOT, "profiles", "traffic.json")
     traffic = None
     if os.path.exists(traffic_path):
-        tj = json.load(open(traffic_path)).get("k_" + dom)
+        tj = json.load(open(traffic_path)).get("k_" + dom + ("_exact" if dom == "render_grad" and args.adjoint == "exact"
+                                                            else ""))
         if tj:  # ncu DRAM bytes per view of a smaller capture, scaled to this launch's views
             traffic = tj["dram_bytes_per_view"] * frames * VIEWS
     # issue-rate view of the tile resolve: pixels resolved and bin entries
