@@ -75,6 +75,10 @@ _SIGS: dict[str, list] = {
     "hc_silhouette_reserve_sized": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp],
     "hc_silhouette_forward_sized": [vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp] + [vp] * 9,
     "hc_silhouette_backward_sized": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp] + [vp] * 6,
+    "hc_silhouette_forward_sumsq_sized": [vp, vp, C.c_int32, C.c_int32, C.c_int32, vp, vp] + [vp] * 9
+    + [C.c_float, vp, vp],
+    "hc_silhouette_backward_scaled_sized": [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_float,
+                                            vp, vp, vp, vp],
     "hc_sum_squares_loss": [vp, C.c_int64, vp, C.c_float, vp, vp, vp],
     "hc_add_inplace": [vp, C.c_int64, vp, vp],
     "hc_image_u8_to_f32": [vp, C.c_int64, vp, vp],

@@ -115,7 +115,7 @@ class DeformRenderChain:
             vnormal=e(B, C, N, 3), grad_img=None if fused_l1 else e(*img, 3),
             p2d=e(B, C, N, 2), n2d=e(B, C, N, 2), isb=e(B, C, N, dt=torch.uint8),
             res=e(B, C, N), res1=e(*img, 2), dtg=e(B, C, N, 2), cid=e(*img),
-            g_res=e(B, C, N), g_res1=e(*img, 2), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
+            g_res=e(B, C, N), gp2d=e(B, C, N, 2), gv_sil=e(B, N, 3),
             gv=e(B, N, 3), gcol=e(B, N, 3), gsh=e(B, C, 27),
             gdofs=torch.zeros((B, self.skin.D), device=dev))
         if deformation == "eg":
@@ -163,33 +163,30 @@ class DeformRenderChain:
         L("hc_camera_projection_forward", s, B, C, N, P(o["v"]), P(o["n"]), P(i["extr"]), P(i["intr"]), 0,
           P(o["n2d"]))
         # the renderer's face buffer of the same views is the coverage hint
+        ws, hs = self.widths.ctypes.data, self.heights.ctypes.data
         if self.multires:
-            ws, hs = self.widths.ctypes.data, self.heights.ctypes.data
             L("hc_mesh_boundary_forward_sized", self.mb.handle, s, B, C, ws, hs, P(o["v"]), P(i["extr"]),
               P(i["intr"]), P(o["p2d"]), P(o["face"]), P(o["isb"]))
-            L("hc_silhouette_forward_sized", self.sil.handle, s, B, C, N, ws, hs, P(o["p2d"]), P(o["n2d"]),
-              P(o["isb"]), P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
         else:
             L("hc_mesh_boundary_forward_hinted", self.mb.handle, s, B, C, W, H, P(o["v"]), P(i["extr"]),
               P(i["intr"]), P(o["p2d"]), P(o["face"]), P(o["isb"]))
-            L("hc_silhouette_forward", self.sil.handle, s, B, C, N, W, H, P(o["p2d"]), P(o["n2d"]), P(o["isb"]),
-              P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]))
+        # the per-pixel residual's squared loss is formed inside the silhouette
+        # forward (the residual is non-zero only on the target's silhouette),
+        # and its adjoint reads the residual itself (silhouette_backward)
+        L("hc_silhouette_forward_sumsq_sized", self.sil.handle, s, B, C, N, ws, hs, P(o["p2d"]), P(o["n2d"]),
+          P(o["isb"]), P(i["dt"]), P(i["crops"]), P(o["res"]), P(o["res1"]), P(o["dtg"]), P(o["cid"]),
+          self.w_sil1, self.ws.data_ptr() + 24, self.loss.data_ptr() + 8)
         L("hc_sum_squares_loss", s, B * C * N, P(o["res"]), self.w_sil, self.ws.data_ptr() + 16,
           self.loss.data_ptr() + 4, P(o["g_res"]))
-        L("hc_sum_squares_loss", s, B * self.P_frame * 2, P(o["res1"]), self.w_sil1, self.ws.data_ptr() + 24,
-          self.loss.data_ptr() + 8, P(o["g_res1"]))
 
     def silhouette_backward(self):
         """Silhouette adjoint and the camera-projection adjoint to vertex positions."""
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
         B, C, H, W, N = self.B, self.C, self.H, self.W, self.N
-        if self.multires:
-            L("hc_silhouette_backward_sized", s, B, C, N, self.widths.ctypes.data, self.heights.ctypes.data,
-              P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]), P(i["crops"]), P(o["gp2d"]))
-        else:
-            L("hc_silhouette_backward", s, B, C, N, W, H, P(o["g_res"]), P(o["g_res1"]), P(o["dtg"]), P(o["cid"]),
-              P(i["crops"]), P(o["gp2d"]))
+        # d (w1 sum res1^2) / d res1 = 2 w1 res1, applied to the residual as it is read
+        L("hc_silhouette_backward_scaled_sized", s, B, C, N, self.widths.ctypes.data, self.heights.ctypes.data,
+          P(o["g_res"]), P(o["res1"]), 2.0 * self.w_sil1, P(o["dtg"]), P(o["cid"]), P(i["crops"]), P(o["gp2d"]))
         L("hc_camera_projection_backward", s, B, C, N, P(o["gp2d"]), P(o["v"]), P(i["extr"]), P(i["intr"]), 1,
           P(o["gv_sil"]))
 

@@ -337,12 +337,14 @@ __device__ void cov_sweep(const CovBins& cb, const ViewImg& vi, int tile, const 
 // around its projection, and a window pixel is covered when the reference's
 // 2-D test passes for its hint face, which is checked here exactly.  A vertex
 // whose window lies in the image with all nine pixels covered that way is not
-// on the boundary.  Every other window pixel is written open (0) to the
-// coverage image and its tile is marked as needing the binned passes; the
-// vertex is flagged kPending and resolved from the coverage image after them.
+// on the boundary.  Otherwise the window's pixels are written to the
+// coverage image (covered 1, open 0), the tiles of its open pixels are marked
+// as needing the binned passes, and the vertex is flagged kPending and
+// resolved from the coverage image after them.
 // Any hint gives the flags of the unhinted op; a good one only saves work.
-// Pixels outside every pending window are never read, so the binned passes
-// need not see them, and every value written here is the same from every
+// Pixels outside every pending window are never read again, so only pending
+// windows are written (the binned passes may see stale values elsewhere,
+// which decide nothing), and every value written here is the same from every
 // window that holds the pixel.
 constexpr unsigned char kPending = 2;
 
@@ -361,10 +363,13 @@ __global__ void k_bnd_hint(long long n, int N, int F, const __grid_constant__ Im
     if (u - 1 >= 0 && u + 1 < W && v - 1 >= 0 && v + 1 < H) {
         int last = -1;
         CoverTri t;
-        for (int rr = v - 1; rr <= v + 1; ++rr)
-            for (int c = u - 1; c <= u + 1; ++c) {
-                const long long pix = vi.pix + (long long)rr * W + c;
-                const int f = hint[pix];
+        unsigned open = 0;  // bit 3 j + k: window pixel (row j, column k) is open
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int rr = v - 1 + j, c = u - 1 + k;
+                const int f = hint[vi.pix + (long long)rr * W + c];
                 bool cov = false;
                 if (f >= 0 && f < F) {
                     if (f != last) {  // neighbouring pixels mostly share their hint face
@@ -373,30 +378,50 @@ __global__ void k_bnd_hint(long long n, int N, int F, const __grid_constant__ Im
                     }
                     cov = c >= t.x0 && c <= t.x1 && rr >= t.y0 && rr <= t.y1 && cover_test(t, c + 0.5f, rr + 0.5f);
                 }
-                cover[pix] = cov ? 1 : 0;
-                if (!cov) {
-                    need[vi.tile + (long long)(rr / kCovTile) * vi.tiles_x + c / kCovTile] = 1;
-                    r = kPending;
-                }
+                open |= (cov ? 0u : 1u) << (3 * j + k);
             }
+        if (open) {  // only a pending window's pixels are read again
+            r = kPending;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int rr = v - 1 + j, c = u - 1 + k;
+                    const bool op = (open >> (3 * j + k)) & 1u;
+                    cover[vi.pix + (long long)rr * W + c] = op ? 0 : 1;
+                    if (op) need[vi.tile + (long long)(rr / kCovTile) * vi.tiles_x + c / kCovTile] = 1;
+                }
+        }
     }
     out[i] = r;
 }
 
-// Per view, the inclusive 2-D prefix sums of the needed-tile flags (one CTA
-// per view: rows, then columns), so that the binning pass drops a triangle
-// whose tile box holds no needed tile with four loads.
-__global__ void k_need_sum(const __grid_constant__ ImgLayout L, const unsigned char* __restrict__ need,
-                           int* __restrict__ sum) {
+// Per view, the inclusive 2-D prefix sums of the needed-tile flags, so that
+// the binning pass drops a triangle whose tile box holds no needed tile with
+// four loads.  One CTA per view: a warp per row (shuffle prefix sums over 32
+// tiles at a time, carried along the row), then a thread per column down the
+// rows.
+constexpr int kNeedSumThreads = 512;
+__global__ void __launch_bounds__(kNeedSumThreads) k_need_sum(const __grid_constant__ ImgLayout L,
+                                                              const unsigned char* __restrict__ need,
+                                                              int* __restrict__ sum) {
     const ViewImg vi = view_img(L, blockIdx.x);
     const int tx = vi.tiles_x, ty = (vi.H + kCovTile - 1) / kCovTile;
     const unsigned char* nd = need + vi.tile;
     int* S = sum + vi.tile;
-    for (int y = threadIdx.x; y < ty; y += blockDim.x) {
-        int acc = 0;
-        for (int x = 0; x < tx; ++x) {
-            acc += nd[y * tx + x];
-            S[y * tx + x] = acc;
+    const int lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+    for (int y = threadIdx.x >> 5; y < ty; y += nwarp) {
+        int carry = 0;
+        for (int x0 = 0; x0 < tx; x0 += 32) {  // warp-uniform
+            const int x = x0 + lane;
+            int v = x < tx ? nd[y * tx + x] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += u;
+            }
+            if (x < tx) S[y * tx + x] = carry + v;
+            carry += __shfl_sync(0xffffffffu, v, 31);
         }
     }
     __syncthreads();
@@ -832,7 +857,7 @@ __device__ __forceinline__ void sil_pixel_warp(long long view, const ViewImg& vi
 __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_constant__ ImgLayout L, SilGrid g,
                              const float* __restrict__ p2d, const unsigned char* __restrict__ dt,
                              const float* __restrict__ crops, float* __restrict__ residual1,
-                             float* __restrict__ closest, int vec) {
+                             float* __restrict__ closest, int vec, double* __restrict__ sumsq1) {
     const long long view = blockIdx.y;
     const ViewImg vi = view_img(L, (int)view);
     const int P = vi.W * vi.H;
@@ -884,16 +909,32 @@ __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_const
             reinterpret_cast<float4*>(residual1 + 2 * i0)[1] = make_float4(r[4], r[5], r[6], r[7]);
             *reinterpret_cast<float4*>(closest + i0) = make_float4(c[0], c[1], c[2], c[3]);
         }
+        if (sumsq1) {  // launch-uniform: the squared residuals, one reduction per warp that has any
+            float q = 0.f;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) q += r[k] * r[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+            if (lane == 0 && q != 0.f) atomicAdd(sumsq1, (double)q);
+        }
         return;
     }
     if (p0 >= P) return;
+    float q = 0.f;
     for (int k = 0; k < 4 && p0 + k < P; ++k) {
         float r0, r1, cl;
         sil_pixel(view, vi, p0 + k, D[p0 + k], N, g, p2d, D, crops, r0, r1, cl);
         residual1[2 * (i0 + k)] = r0;
         residual1[2 * (i0 + k) + 1] = r1;
         closest[i0 + k] = cl;
+        q += r0 * r0 + r1 * r1;
     }
+    if (sumsq1 && q != 0.f) atomicAdd(sumsq1, (double)q);
+}
+
+// the squared-residual loss of the fused forward: weight x the accumulated sum
+__global__ void k_sil_loss1(float weight, const double* __restrict__ sumsq1, float* __restrict__ loss) {
+    *loss = (float)(weight * *sumsq1);
 }
 
 __global__ void k_sil_grad_points(long long n, const float* __restrict__ dtgrad, const float* __restrict__ g,
@@ -908,7 +949,7 @@ __global__ void k_sil_grad_points(long long n, const float* __restrict__ dtgrad,
 // closest_vertex_id when the buffer allows (vec); the rare boundary pixels
 // scatter their residual gradient to the closest vertex
 __global__ void k_sil_grad_pixels(int N, const __grid_constant__ ImgLayout L, const float* __restrict__ g1,
-                                  const float* __restrict__ closest, const float* __restrict__ crops,
+                                  float s1, const float* __restrict__ closest, const float* __restrict__ crops,
                                   float* __restrict__ out, int vec) {
     const long long view = blockIdx.y;
     const ViewImg vi = view_img(L, (int)view);
@@ -932,8 +973,8 @@ __global__ void k_sil_grad_pixels(int N, const __grid_constant__ ImgLayout L, co
         if (cv < 0) continue;
         const float scale = crops[view * 7 + 2];
         float* o = out + (view * N + cv) * 2;
-        atomicAdd(o, g1[2 * (i0 + k)] / (30.f * scale));
-        atomicAdd(o + 1, g1[2 * (i0 + k) + 1] / (30.f * scale));
+        atomicAdd(o, s1 * g1[2 * (i0 + k)] / (30.f * scale));  // (s1 x g) exact for s1 = 1
+        atomicAdd(o + 1, s1 * g1[2 * (i0 + k) + 1] / (30.f * scale));
     }
 }
 
@@ -1162,7 +1203,7 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
                                                    h->faces.as<int>(), face_hint, h->cover.as<unsigned char>(),
                                                    h->need.as<unsigned char>(), is_boundary);
         HC_CHECK_LAUNCH();
-        k_need_sum<<<(unsigned)views, 128, 0, s>>>(L, h->need.as<unsigned char>(), h->need_sum.as<int>());
+        k_need_sum<<<(unsigned)views, kNeedSumThreads, 0, s>>>(L, h->need.as<unsigned char>(), h->need_sum.as<int>());
         HC_CHECK_LAUNCH();
         cb.need = h->need.as<unsigned char>();
         cb.need_sum = h->need_sum.as<int>();
@@ -1294,7 +1335,8 @@ hc_status sil_forward_run(cudaStream_t s, int* base, const ImgLayout& L, int32_t
                           int32_t n_points, const float* points_image_space, const float* normals_image_space,
                           const uint8_t* is_boundary, const uint8_t* distance_transform_image,
                           const float* multi_view_crops, float* mv_dt_residual, float* mv_dt_residual_1,
-                          float* dt_image_gradient, float* closest_vertex_id) {
+                          float* dt_image_gradient, float* closest_vertex_id, float weight_1 = 0.f,
+                          double* sumsq_1 = nullptr, float* loss_1 = nullptr) {
     const int N = n_points;
     const long long views = (long long)batch * n_cameras;
     const long long cells = views / L.n_cam * L.G;
@@ -1317,21 +1359,26 @@ hc_status sil_forward_run(cudaStream_t s, int* base, const ImgLayout& L, int32_t
     k_grid_fill<<<div_up(np, 256), 256, 0, s>>>(batch, n_cameras, N, L, g, points_image_space, is_boundary,
                                                 multi_view_crops);
     HC_CHECK_LAUNCH();
+    if (sumsq_1) HC_CUDA(cudaMemsetAsync(sumsq_1, 0, sizeof(double), s));
     {
         const int vec = pixels_by_four(L) && ((uintptr_t)distance_transform_image & 3) == 0 &&
                         ((uintptr_t)mv_dt_residual_1 & 15) == 0 && ((uintptr_t)closest_vertex_id & 15) == 0;
         k_sil_pixels<<<dim3(div_up(max_view_pixels(L), 4 * 256), (unsigned)views), 256, 0, s>>>(
             N, L, g, points_image_space, distance_transform_image, multi_view_crops, mv_dt_residual_1,
-            closest_vertex_id, vec);
+            closest_vertex_id, vec, sumsq_1);
     }
     HC_CHECK_LAUNCH();
+    if (loss_1) {
+        k_sil_loss1<<<1, 1, 0, s>>>(weight_1, sumsq_1, loss_1);
+        HC_CHECK_LAUNCH();
+    }
     return HC_OK;
 }
 
 hc_status sil_backward_run(cudaStream_t s, int32_t batch, int32_t n_cameras, int32_t n_points, const int32_t* widths,
                            const int32_t* heights, const float* mv_dt_grad, const float* mv_dt_grad_1,
                            const float* dt_image_grad, const float* closest_vertex_id, const float* multi_view_crops,
-                           float* points_image_space_grad) {
+                           float* points_image_space_grad, float scale_1 = 1.f) {
     HC_REQUIRE(batch > 0 && n_cameras > 0 && n_points > 0, "bad sizes");
     HC_REQUIRE(mv_dt_grad && mv_dt_grad_1 && dt_image_grad && closest_vertex_id && multi_view_crops &&
                    points_image_space_grad,
@@ -1344,7 +1391,7 @@ hc_status sil_backward_run(cudaStream_t s, int32_t batch, int32_t n_cameras, int
     HC_CHECK_LAUNCH();
     const int vec = pixels_by_four(L) && ((uintptr_t)closest_vertex_id & 15) == 0;
     k_sil_grad_pixels<<<dim3(div_up(max_view_pixels(L), 4 * 256), (unsigned)views), 256, 0, s>>>(
-        n_points, L, mv_dt_grad_1, closest_vertex_id, multi_view_crops, points_image_space_grad, vec);
+        n_points, L, mv_dt_grad_1, scale_1, closest_vertex_id, multi_view_crops, points_image_space_grad, vec);
     HC_CHECK_LAUNCH();
     return HC_OK;
 }
@@ -1369,6 +1416,27 @@ extern "C" hc_status hc_silhouette_forward_sized(hc_silhouette h, void* stream, 
     return sil_forward_run((cudaStream_t)stream, h->grid.as<int>(), L, batch, n_cameras, n_points,
                            points_image_space, normals_image_space, is_boundary, distance_transform_image,
                            multi_view_crops, mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id);
+}
+
+extern "C" hc_status hc_silhouette_forward_sumsq_sized(
+    hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras, int32_t n_points, const int32_t* widths,
+    const int32_t* heights, const float* points_image_space, const float* normals_image_space,
+    const uint8_t* is_boundary, const uint8_t* distance_transform_image, const float* multi_view_crops,
+    float* mv_dt_residual, float* mv_dt_residual_1, float* dt_image_gradient, float* closest_vertex_id,
+    float weight_1, double* sumsq_1, float* loss_1) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    HC_REQUIRE(sumsq_1 && loss_1, "NULL pointer");
+    ImgLayout L;
+    size_t need = 0;
+    HC_TRY(sil_forward_plan(batch, n_cameras, n_points, widths, heights, points_image_space, normals_image_space,
+                            is_boundary, distance_transform_image, multi_view_crops, mv_dt_residual,
+                            mv_dt_residual_1, dt_image_gradient, closest_vertex_id, L, need));
+    HC_TRY(h->grid.ensure(need));
+    return sil_forward_run((cudaStream_t)stream, h->grid.as<int>(), L, batch, n_cameras, n_points,
+                           points_image_space, normals_image_space, is_boundary, distance_transform_image,
+                           multi_view_crops, mv_dt_residual, mv_dt_residual_1, dt_image_gradient, closest_vertex_id,
+                           weight_1, sumsq_1, loss_1);
 }
 
 extern "C" hc_status hc_silhouette_forward(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
@@ -1406,6 +1474,19 @@ extern "C" hc_status hc_silhouette_backward_sized(void* stream, int32_t batch, i
     return sil_backward_run((cudaStream_t)stream, batch, n_cameras, n_points, widths, heights, mv_dt_grad,
                             mv_dt_grad_1, dt_image_grad, closest_vertex_id, multi_view_crops,
                             points_image_space_grad);
+}
+
+extern "C" hc_status hc_silhouette_backward_scaled_sized(void* stream, int32_t batch, int32_t n_cameras,
+                                                         int32_t n_points, const int32_t* widths,
+                                                         const int32_t* heights, const float* mv_dt_grad,
+                                                         const float* mv_dt_grad_1, float scale_1,
+                                                         const float* dt_image_grad, const float* closest_vertex_id,
+                                                         const float* multi_view_crops,
+                                                         float* points_image_space_grad) {
+    clear_error();
+    return sil_backward_run((cudaStream_t)stream, batch, n_cameras, n_points, widths, heights, mv_dt_grad,
+                            mv_dt_grad_1, dt_image_grad, closest_vertex_id, multi_view_crops,
+                            points_image_space_grad, scale_1);
 }
 
 // ---------------------------------------------------------------------------

@@ -532,6 +532,34 @@ hc_status hc_silhouette_backward_sized(void* stream, int32_t batch, int32_t n_ca
                                        const float* closest_vertex_id, const float* multi_view_crops,
                                        float* points_image_space_grad);
 
+/* The silhouette loss with the squared loss of its per-pixel residual fused
+ * in (no reference counterpart; the reference graph squares and sums the
+ * residual image with TF ops, HPCMeshDL.py:669-688).
+ * hc_silhouette_forward_sumsq_sized is hc_silhouette_forward_sized that also
+ * forms sum(mv_dt_residual_1^2) while it writes the residual, into *sumsq_1
+ * (a device double, cleared by the call), and writes the loss
+ * weight_1 * sum into *loss_1 (a device float).  Only pixels on the target's
+ * silhouette have a non-zero residual, so no pass over the residual image
+ * follows.  hc_silhouette_backward_scaled_sized is
+ * hc_silhouette_backward_sized with the residual's upstream gradient given as
+ * scale_1 x mv_dt_grad_1: passing the residual itself and scale_1 = 2 weight_1
+ * gives the squared loss's adjoint without a dense gradient image (the same
+ * values as forming 2 w x residual first: the product is rounded once either
+ * way). */
+hc_status hc_silhouette_forward_sumsq_sized(hc_silhouette h, void* stream, int32_t batch, int32_t n_cameras,
+                                            int32_t n_points, const int32_t* widths, const int32_t* heights,
+                                            const float* points_image_space, const float* normals_image_space,
+                                            const uint8_t* is_boundary, const uint8_t* distance_transform_image,
+                                            const float* multi_view_crops, float* mv_dt_residual,
+                                            float* mv_dt_residual_1, float* dt_image_gradient,
+                                            float* closest_vertex_id, float weight_1, double* sumsq_1,
+                                            float* loss_1);
+hc_status hc_silhouette_backward_scaled_sized(void* stream, int32_t batch, int32_t n_cameras, int32_t n_points,
+                                              const int32_t* widths, const int32_t* heights,
+                                              const float* mv_dt_grad, const float* mv_dt_grad_1, float scale_1,
+                                              const float* dt_image_grad, const float* closest_vertex_id,
+                                              const float* multi_view_crops, float* points_image_space_grad);
+
 /*
  * hc_silhouette_forward without allocation.  No counterpart in the reference.
  * For callers that cannot allocate device memory themselves: a TensorFlow

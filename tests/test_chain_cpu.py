@@ -32,7 +32,7 @@ def test_chain_step_calls(recorder):
     names = [n for n, _ in recorder]
     assert names == ["hc_pose2eg_forward", "hc_eg_forward", "hc_renderer_forward_l1",
                      "hc_camera_projection_forward", "hc_camera_projection_forward", "hc_mesh_boundary_forward_hinted",
-                     "hc_silhouette_forward", "hc_sum_squares_loss", "hc_sum_squares_loss", "hc_silhouette_backward",
+                     "hc_silhouette_forward_sumsq_sized", "hc_sum_squares_loss", "hc_silhouette_backward_scaled_sized",
                      "hc_camera_projection_backward", "hc_renderer_backward_l1", "hc_add_inplace", "hc_eg_backward",
                      "hc_pose2eg_backward"]
     args = dict(recorder)
@@ -52,6 +52,11 @@ def test_chain_step_calls(recorder):
     # joint angles: the EG's skinned-transform gradients feed the node-skinning adjoint
     assert args["hc_pose2eg_backward"][7] == args["hc_eg_backward"][9]
     assert args["hc_pose2eg_backward"][8] == args["hc_eg_backward"][10]
+    # the per-pixel residual's squared loss is fused into the silhouette forward, and
+    # its adjoint reads the residual itself with the factor 2 w1
+    fw, bw = args["hc_silhouette_forward_sumsq_sized"], args["hc_silhouette_backward_scaled_sized"]
+    assert bw[7] == fw[13] and abs(bw[8] - 2 * ch.w_sil1) < 1e-12 and fw[16] == ch.w_sil1
+    assert args["hc_sum_squares_loss"][1] == 2 * 2 * sc["N"]
     assert np.isfinite(sc["dofs"]).all()
 
 
@@ -70,15 +75,16 @@ def test_chain_step_calls_mixed_sizes_vertex_dq(recorder):
     ch.step()
     names = [n for n, _ in recorder]
     assert names == ["hc_dq_skinning_forward", "hc_renderer_forward_l1", "hc_camera_projection_forward",
-                     "hc_camera_projection_forward", "hc_mesh_boundary_forward_sized", "hc_silhouette_forward_sized",
-                     "hc_sum_squares_loss", "hc_sum_squares_loss", "hc_silhouette_backward_sized",
+                     "hc_camera_projection_forward", "hc_mesh_boundary_forward_sized",
+                     "hc_silhouette_forward_sumsq_sized", "hc_sum_squares_loss", "hc_silhouette_backward_scaled_sized",
                      "hc_camera_projection_backward", "hc_renderer_backward_l1", "hc_add_inplace",
                      "hc_dq_skinning_backward"]
     args = dict(recorder)
     import ctypes
     w = args["hc_mesh_boundary_forward_sized"][4]
     assert list((ctypes.c_int32 * 3).from_address(w)) == ws
-    assert args["hc_sum_squares_loss"][1] == 2 * ch.P_frame * 2
+    assert list((ctypes.c_int32 * 3).from_address(args["hc_silhouette_forward_sumsq_sized"][5])) == ws
+    assert list((ctypes.c_int32 * 3).from_address(args["hc_silhouette_backward_scaled_sized"][5])) == hs
     v = args["hc_dq_skinning_forward"][5]
     assert args["hc_renderer_forward_l1"][3] == v and args["hc_dq_skinning_backward"][4] == v
     assert args["hc_dq_skinning_backward"][3] == args["hc_add_inplace"][2]

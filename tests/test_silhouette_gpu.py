@@ -217,3 +217,39 @@ def test_mesh_boundary_hint_changes_no_flag(scene):
                 hinted = eng.forward(scene["verts"], ex, it, width, height, face_hint=hint)
                 torch.cuda.synchronize()
                 assert torch.equal(hinted, full), (width, height, k, int((hinted != full).sum()))
+
+
+def test_fused_squared_loss_matches_the_separate_passes(scene):
+    """hc_silhouette_forward_sumsq_sized gives the outputs of the plain
+    forward and the loss of hc_sum_squares_loss over its residual image;
+    hc_silhouette_backward_scaled_sized on (residual, 2 w) gives the adjoint
+    of the plain backward on the gradient image 2 w x residual."""
+    import ctypes as C
+    from deepcharacters_b200 import _lib
+    p2d, n2d, isb, dt, crops = _sil_inputs(scene)
+    B, Cn, N = p2d.shape[0], p2d.shape[1], p2d.shape[2]
+    ws = np.full(Cn, RES, np.int32)
+    eng = SilhouetteEngine()
+    plain = eng.forward(p2d, n2d, isb, dt, crops)
+    outs = [torch.empty_like(t) for t in plain]
+    acc = torch.zeros(2, dtype=torch.float64, device=DEV)
+    loss = torch.zeros(2, device=DEV)
+    w1 = 1e-3
+    P = _lib.ptr
+    _lib.call("hc_silhouette_forward_sumsq_sized", eng.handle, None, B, Cn, N, ws.ctypes.data, ws.ctypes.data,
+              P(p2d), P(n2d), P(isb), P(dt), P(crops), *(P(t) for t in outs), w1, P(acc), P(loss))
+    g1 = torch.empty_like(plain[1])
+    _lib.call("hc_sum_squares_loss", None, g1.numel(), P(plain[1]), w1, P(acc[1:]), P(loss[1:]), P(g1))
+    torch.cuda.synchronize()
+    for a, b in zip(outs, plain):
+        assert torch.equal(a, b)
+    assert int((plain[3] >= 0).sum()) > 0 and float(loss[1]) > 0
+    assert abs(float(loss[0]) - float(loss[1])) <= 1e-6 * float(loss[1])
+    g = torch.randn(plain[0].shape, device=DEV, generator=torch.Generator(DEV).manual_seed(3))
+    ref = silhouette_backward(g, g1, plain[2], plain[3], crops)
+    out = torch.empty_like(ref)
+    _lib.call("hc_silhouette_backward_scaled_sized", None, B, Cn, N, ws.ctypes.data, ws.ctypes.data, P(g),
+              P(plain[1]), 2.0 * w1, P(plain[2]), P(plain[3]), P(crops), P(out))
+    torch.cuda.synchronize()
+    assert float(ref.abs().max()) > 0
+    assert nrel(out, ref) < 1e-6  # float atomics: equal up to summation order
