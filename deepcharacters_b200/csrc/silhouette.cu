@@ -310,7 +310,17 @@ struct CovBins {
     unsigned char* cover;       // coverage image, the layout's pixels
     const unsigned char* need;  // [tiles of the call] tiles with a pixel still open (NULL: every tile)
     const int* need_sum;        // [tiles of the call] per view: inclusive 2-D prefix sums of need (NULL: none)
+    int* tiles;                 // [tiles of the call]: the tiles that received an entry, in no order
+    int* n_tiles;               // their number (cleared before the binning pass)
 };
+
+// a bin slot of tile `key`; the tile's first slot also lists the tile for the
+// tile pass (tile keys of a call fit 31 bits)
+__device__ __forceinline__ int cov_claim(const CovBins& cb, long long key) {
+    const int slot = atomicAdd(cb.count + key, 1);
+    if (slot == 0) cb.tiles[atomicAdd(cb.n_tiles, 1)] = (int)key;
+    return slot;
+}
 
 // needed tiles of a view in the tile box [tx0, tx1] x [ty0, ty1] (inclusive),
 // from the view's 2-D prefix sums S (row-major, tiles_x per row)
@@ -348,7 +358,9 @@ __device__ void cov_sweep(const CovBins& cb, const ViewImg& vi, int tile, const 
 // window that holds the pixel.
 constexpr unsigned char kPending = 2;
 
-__global__ void k_bnd_hint(long long n, int N, int F, const __grid_constant__ ImgLayout L,
+// (6 CTAs of 256 per SM: the kernel waits on dependent gathers, and more
+// resident warps hide them better than the registers they cost)
+__global__ void __launch_bounds__(256, 6) k_bnd_hint(long long n, int N, int F, const __grid_constant__ ImgLayout L,
                            const float2* __restrict__ p2d, const int* __restrict__ faces,
                            const int* __restrict__ hint, unsigned char* __restrict__ cover,
                            unsigned char* __restrict__ need, unsigned char* __restrict__ out) {
@@ -486,7 +498,7 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
         const int tile = ty * vi.tiles_x + tx;
         if (cb.need && !cb.need[vi.tile + tile]) continue;
         const long long key = vi.tile + tile;
-        const int slot = atomicAdd(cb.count + key, 1);
+        const int slot = cov_claim(cb, key);
         if (slot < kCovCap)
             cb.bins[key * kCovCap + slot] = f;
         else
@@ -521,7 +533,7 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
             const int tile = ty * qi.tiles_x + tx;
             const long long key = qi.tile + tile;
             if (cb.need && !cb.need[key]) continue;
-            const int slot = atomicAdd(cb.count + key, 1);
+            const int slot = cov_claim(cb, key);
             if (slot < kCovCap)
                 cb.bins[key * kCovCap + slot] = qf;
             else
@@ -530,17 +542,17 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
     }
 }
 
-// Persistent CTAs over the (view, tile) pairs, one thread per pixel of the
-// current tile: a pixel stops at the first binned triangle that covers it,
-// the tile at the chunk after which all its pixels are covered.  Tiles
-// without entries (most of them when a coverage hint was given) cost one
-// count load instead of a CTA launch each.
+// Persistent CTAs over the tiles that received entries (the binning pass
+// lists them), one thread per pixel of the current tile: a pixel stops at the
+// first binned triangle that covers it, the tile at the chunk after which all
+// its pixels are covered.
 __global__ void __launch_bounds__(kCovTile* kCovTile) k_cov_tile(int F, long long n_keys, CovBins cb,
                                                                   const __grid_constant__ ImgLayout L) {
     __shared__ CovTileTri s_t[kCovTile * kCovTile];
-    for (long long key = blockIdx.x; key < n_keys; key += gridDim.x) {
+    const int listed = *cb.n_tiles;
+    for (int it = blockIdx.x; it < listed; it += gridDim.x) {
+        const long long key = cb.tiles[it];
         const int n = min(cb.count[key], kCovCap);
-        if (n == 0) continue;  // CTA-uniform
         int tile;
         const int view = view_of_tile(L, key, tile);
         const ViewImg vi = view_img(L, view);
@@ -851,9 +863,10 @@ __device__ __forceinline__ void sil_pixel_warp(long long view, const ViewImg& vi
 // Four consecutive pixels per thread, grid (pixel blocks of one view, views):
 // one 4-byte DT load and 16-byte stores when the buffers allow (vec), and
 // 32-bit index arithmetic.  Most pixels are not on the boundary and only
-// write their zero outputs; in the vec path the warp takes its boundary
-// pixels one at a time, all lanes together (sil_pixel_warp), instead of
-// leaving one lane to search while the others wait.
+// write their zero outputs; in the vec path each boundary pixel is searched
+// by a whole warp (sil_pixel_warp), the block's boundary pixels dealt to its
+// warps in turn, instead of leaving one lane to search while the others wait.
+// Launched with 256 threads (the shared lists hold the block's 1024 pixels).
 __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_constant__ ImgLayout L, SilGrid g,
                              const float* __restrict__ p2d, const unsigned char* __restrict__ dt,
                              const float* __restrict__ crops, float* __restrict__ residual1,
@@ -866,7 +879,15 @@ __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_const
     const unsigned char* D = dt + vi.pix;
     const long long i0 = vi.pix + p0;
     if (vec) {  // P % 4 == 0 and aligned buffers: all four pixels of an active thread exist
-        const bool active = p0 < P;  // no early exit: the warp's lanes all take part below
+        // The block's boundary pixels are listed in shared memory and dealt to
+        // its warps in turn (a contour running along a row can put dozens in
+        // one warp's 128 pixels); their results come back through shared
+        // memory to the threads that own the pixels and store them.
+        __shared__ int s_n;
+        __shared__ unsigned short s_list[4 * 256];
+        __shared__ float2 s_r[4 * 256];
+        __shared__ float s_c[4 * 256];
+        const bool active = p0 < P;  // no early exit: every thread takes part in the barriers
         int dv[4] = {0, 0, 0, 0};
         if (active) {
             const uchar4 d4 = *reinterpret_cast<const uchar4*>(D + p0);
@@ -875,33 +896,34 @@ __global__ void __launch_bounds__(256, 5) k_sil_pixels(int N, const __grid_const
             dv[2] = d4.z;
             dv[3] = d4.w;
         }
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (dv[k] == 127) s_list[atomicAdd(&s_n, 1)] = (unsigned short)(4 * threadIdx.x + k);
+        __syncthreads();
+        const int n = s_n, lane = threadIdx.x & 31;
+        const int pb = 4 * (int)(blockIdx.x * blockDim.x);  // the block's first pixel
+        for (int e = threadIdx.x >> 5; e < n; e += blockDim.x >> 5) {  // warp-uniform
+            const int lp = s_list[e];
+            float a0, a1, cl;
+            sil_pixel_warp(view, vi, pb + lp, N, g, p2d, D, crops, lane, a0, a1, cl);
+            if (lane == 0) {
+                s_r[lp] = make_float2(a0, a1);
+                s_c[lp] = cl;
+            }
+        }
+        __syncthreads();
         float r[8], c[4];
-        unsigned mine = 0;  // bit k: pixel k of this lane is a boundary pixel
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             r[2 * k] = r[2 * k + 1] = 0.f;
             c[k] = -1.f;
-            mine |= (dv[k] == 127 ? 1u : 0u) << k;
-        }
-        const int lane = threadIdx.x & 31;
-        unsigned any = __ballot_sync(0xffffffffu, mine != 0);
-        while (any) {
-            const int src = __ffs(any) - 1;
-            const unsigned m = __shfl_sync(0xffffffffu, mine, src);
-            const int k = __ffs(m) - 1;
-            const int p = __shfl_sync(0xffffffffu, p0, src) + k;
-            if (lane == src) mine &= mine - 1;
-            any = __ballot_sync(0xffffffffu, mine != 0);
-            float a0, a1, cl;
-            sil_pixel_warp(view, vi, p, N, g, p2d, D, crops, lane, a0, a1, cl);
-            if (lane == src) {
-#pragma unroll
-                for (int kk = 0; kk < 4; ++kk)
-                    if (kk == k) {
-                        r[2 * kk] = a0;
-                        r[2 * kk + 1] = a1;
-                        c[kk] = cl;
-                    }
+            if (dv[k] == 127) {
+                const float2 q = s_r[4 * threadIdx.x + k];
+                r[2 * k] = q.x;
+                r[2 * k + 1] = q.y;
+                c[k] = s_c[4 * threadIdx.x + k];
             }
         }
         if (active) {
@@ -1102,7 +1124,7 @@ bool pixels_by_four(const ImgLayout& L) {
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover, count, bins, rec, need, need_sum;
+    DevBuf faces, p2d, cover, count, bins, rec, need, need_sum, tile_list;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -1134,6 +1156,7 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     h->rec.release();
     h->need.release();
     h->need_sum.release();
+    h->tile_list.release();
     delete h;
     return HC_OK;
 }
@@ -1147,6 +1170,7 @@ static hc_status mesh_boundary_reserve_layout(hc_mesh_boundary h, long long view
     HC_TRY(h->rec.ensure(sizeof(CovTileTri) * (size_t)views * h->F));
     HC_TRY(h->need.ensure(frames * (size_t)L.T));
     HC_TRY(h->need_sum.ensure(sizeof(int) * frames * (size_t)L.T));
+    HC_TRY(h->tile_list.ensure(sizeof(int) * (frames * (size_t)L.T + 1)));
     return HC_OK;
 }
 
@@ -1195,6 +1219,8 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     cb.rec = h->rec.as<CovTileTri>();
     cb.need = nullptr;
     cb.need_sum = nullptr;
+    cb.n_tiles = h->tile_list.as<int>();
+    cb.tiles = cb.n_tiles + 1;
     if (face_hint) {
         // final flags of the vertices whose window the hint covers; open
         // window pixels and their tiles for the binned passes
@@ -1211,6 +1237,7 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
         HC_CUDA(cudaMemsetAsync(h->cover.ptr, 0, (size_t)(frames * L.P), s));
     }
     HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)n_keys, s));
+    HC_CUDA(cudaMemsetAsync(cb.n_tiles, 0, sizeof(int), s));
     k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
                                                                        reinterpret_cast<const float2*>(p2d), cb, L);
     HC_CHECK_LAUNCH();
