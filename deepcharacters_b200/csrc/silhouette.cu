@@ -312,6 +312,8 @@ struct CovBins {
     const int* need_sum;        // [tiles of the call] per view: inclusive 2-D prefix sums of need (NULL: none)
     int* tiles;                 // [tiles of the call]: the tiles that received an entry, in no order
     int* n_tiles;               // their number (cleared before the binning pass)
+    int* items;                 // [V*F]: hinted binning, the (view * F + triangle) pairs left by the cull
+    int* n_items;               // their number (cleared before the cull)
 };
 
 // a bin slot of tile `key`; the tile's first slot also lists the tile for the
@@ -450,13 +452,12 @@ __global__ void __launch_bounds__(kNeedSumThreads) k_need_sum(const __grid_const
 // to kCovSmall tiles are binned by their own thread, one counter atomic per
 // entry; larger boxes are taken by the whole warp, a tile per lane, reading
 // the record back from global memory.
-__global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
-                          CovBins cb, const __grid_constant__ ImgLayout L) {
-    // grid (triangle blocks, views): no 64-bit division per thread
-    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+// (all 32 lanes of the warp call it together: the big boxes are shared out
+// with warp votes; `sat` culls boxes without a needed tile)
+__device__ __forceinline__ void cov_bin_item(int view, int fi, bool live, int N, int F,
+                                             const int* __restrict__ faces, const float2* __restrict__ p2d,
+                                             const CovBins& cb, const ImgLayout& L, bool sat) {
     const unsigned lane = threadIdx.x & 31;
-    const bool live = fi < F;
-    const int view = blockIdx.y;
     const ViewImg vi = view_img(L, view);
     const long long i = (long long)view * F + fi;
     int f = 0;
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
     const int tx0 = t.x0 / kCovTile, ty0 = t.y0 / kCovTile;
     const int ntx = nonempty ? t.x1 / kCovTile - tx0 + 1 : 0;
     int nt = nonempty ? ntx * (t.y1 / kCovTile - ty0 + 1) : 0;
-    if (cb.need_sum && nt > 0 &&  // a box without a needed tile needs nothing
+    if (sat && nt > 0 &&  // a box without a needed tile needs nothing
         need_in_box(cb.need_sum + vi.tile, vi.tiles_x, tx0, ty0, t.x1 / kCovTile, t.y1 / kCovTile) == 0) {
         nonempty = false;
         nt = 0;
@@ -539,6 +540,55 @@ __global__ void __launch_bounds__(256, 4) k_cov_bin(int V, int N, int F, const i
             else
                 cov_sweep(cb, qi, tile, q);
         }
+    }
+}
+
+// the unhinted binning: every (view, triangle), grid (triangle blocks, views)
+__global__ void __launch_bounds__(256, 4) k_cov_bin(int N, int F, const int* __restrict__ faces,
+                                                    const float2* __restrict__ p2d, CovBins cb,
+                                                    const __grid_constant__ ImgLayout L) {
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    cov_bin_item(blockIdx.y, fi, fi < F, N, F, faces, p2d, cb, L, false);
+}
+
+// The hinted binning's first pass, light enough for full occupancy: the
+// (view, triangle) pairs whose tile box holds a needed tile (most hold none),
+// listed with one atomic per warp for k_cov_bin_list.
+__global__ void k_cov_cull(int N, int F, const int* __restrict__ faces, const float2* __restrict__ p2d,
+                           CovBins cb, const __grid_constant__ ImgLayout L) {
+    const int fi = blockIdx.x * blockDim.x + threadIdx.x;
+    const int view = blockIdx.y;
+    const ViewImg vi = view_img(L, view);
+    bool keep = false;
+    if (fi < F) {  // no early exit: the whole warp takes part in the vote
+        CoverTri t;
+        cover_tri(view, fi, N, vi.W, vi.H, faces, p2d, t);
+        keep = t.x1 >= t.x0 && t.y1 >= t.y0 &&
+               need_in_box(cb.need_sum + vi.tile, vi.tiles_x, t.x0 / kCovTile, t.y0 / kCovTile, t.x1 / kCovTile,
+                           t.y1 / kCovTile) > 0;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (!m) return;  // warp-uniform
+    const int lane = threadIdx.x & 31, first = __ffs(m) - 1;
+    int base = 0;
+    if (lane == first) base = atomicAdd(cb.n_items, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, first);
+    if (keep) cb.items[base + __popc(m & ((1u << lane) - 1u))] = view * F + fi;
+}
+
+// the hinted binning proper over the listed pairs (persistent, whole warps)
+__global__ void __launch_bounds__(256, 4) k_cov_bin_list(int N, int F, const int* __restrict__ faces,
+                                                         const float2* __restrict__ p2d, CovBins cb,
+                                                         const __grid_constant__ ImgLayout L) {
+    const int n = *cb.n_items;
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int base = 32 * gw; base < n; base += 32 * nw) {  // warp-uniform
+        const int i = base + lane;
+        const bool live = i < n;
+        const int item = live ? cb.items[i] : 0;
+        const int view = item / F;
+        cov_bin_item(view, item - view * F, live, N, F, faces, p2d, cb, L, false);
     }
 }
 
@@ -1114,6 +1164,19 @@ long long max_view_pixels(const ImgLayout& L) {
 }
 
 // every view's pixel count a multiple of 4 (so every view starts 4-aligned)
+// grid of a persistent kernel: as many CTAs as are resident at once (a
+// second partial wave would run its strided work after everything else),
+// never more than `items`
+template <typename K>
+unsigned resident_blocks(K kernel, int threads, long long items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
+    return (unsigned)std::max<long long>(1, std::min<long long>(items, (long long)sms * per_sm));
+}
+
 bool pixels_by_four(const ImgLayout& L) {
     for (int c = 0; c < L.n_cam; ++c)
         if (((long long)L.cam[c].W * L.cam[c].H) % 4 != 0) return false;
@@ -1124,7 +1187,7 @@ bool pixels_by_four(const ImgLayout& L) {
 
 struct hc_mesh_boundary_s {
     int F = 0, N = 0;
-    DevBuf faces, p2d, cover, count, bins, rec, need, need_sum, tile_list;
+    DevBuf faces, p2d, cover, count, bins, rec, need, need_sum, tile_list, items;
 };
 
 extern "C" hc_status hc_mesh_boundary_create(hc_mesh_boundary* out, const int32_t* faces, int32_t n_faces,
@@ -1157,6 +1220,7 @@ extern "C" hc_status hc_mesh_boundary_destroy(hc_mesh_boundary h) {
     h->need.release();
     h->need_sum.release();
     h->tile_list.release();
+    h->items.release();
     delete h;
     return HC_OK;
 }
@@ -1171,6 +1235,8 @@ static hc_status mesh_boundary_reserve_layout(hc_mesh_boundary h, long long view
     HC_TRY(h->need.ensure(frames * (size_t)L.T));
     HC_TRY(h->need_sum.ensure(sizeof(int) * frames * (size_t)L.T));
     HC_TRY(h->tile_list.ensure(sizeof(int) * (frames * (size_t)L.T + 1)));
+    HC_REQUIRE(views * h->F < (1ll << 31), "too many (view, triangle) pairs in one call");
+    HC_TRY(h->items.ensure(sizeof(int) * ((size_t)views * h->F + 1)));
     return HC_OK;
 }
 
@@ -1221,6 +1287,8 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     cb.need_sum = nullptr;
     cb.n_tiles = h->tile_list.as<int>();
     cb.tiles = cb.n_tiles + 1;
+    cb.n_items = h->items.as<int>();
+    cb.items = cb.n_items + 1;
     if (face_hint) {
         // final flags of the vertices whose window the hint covers; open
         // window pixels and their tiles for the binned passes
@@ -1238,21 +1306,19 @@ static hc_status mesh_boundary_run(hc_mesh_boundary h, void* stream, int32_t bat
     }
     HC_CUDA(cudaMemsetAsync(cb.count, 0, sizeof(int) * (size_t)n_keys, s));
     HC_CUDA(cudaMemsetAsync(cb.n_tiles, 0, sizeof(int), s));
-    k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>((int)views, h->N, h->F, h->faces.as<int>(),
-                                                                       reinterpret_cast<const float2*>(p2d), cb, L);
-    HC_CHECK_LAUNCH();
-    {
-        // persistent: as many CTAs as are resident at once (a second partial
-        // wave would run its strided keys after everything else)
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cov_tile, kCovTile * kCovTile, 0) != cudaSuccess ||
-            per_sm <= 0)
-            per_sm = 1;
-        const long long grid = std::max<long long>(1, std::min<long long>(n_keys, (long long)sms * per_sm));
-        k_cov_tile<<<(unsigned)grid, kCovTile * kCovTile, 0, s>>>(h->F, n_keys, cb, L);
+    const float2* p2 = reinterpret_cast<const float2*>(p2d);
+    if (face_hint) {  // cull, then bin the listed pairs
+        HC_CUDA(cudaMemsetAsync(cb.n_items, 0, sizeof(int), s));
+        k_cov_cull<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>(h->N, h->F, h->faces.as<int>(), p2, cb, L);
+        HC_CHECK_LAUNCH();
+        k_cov_bin_list<<<resident_blocks(k_cov_bin_list, 256, views * h->F / 256 + 1), 256, 0, s>>>(
+            h->N, h->F, h->faces.as<int>(), p2, cb, L);
+    } else {
+        k_cov_bin<<<dim3(div_up(h->F, 256), (unsigned)views), 256, 0, s>>>(h->N, h->F, h->faces.as<int>(), p2, cb, L);
     }
+    HC_CHECK_LAUNCH();
+    k_cov_tile<<<resident_blocks(k_cov_tile, kCovTile * kCovTile, n_keys), kCovTile * kCovTile, 0, s>>>(h->F, n_keys,
+                                                                                                      cb, L);
     HC_CHECK_LAUNCH();
     k_boundary_cover<<<div_up(nv, 256), 256, 0, s>>>(batch, n_cameras, h->N, L, p2d, h->cover.as<unsigned char>(),
                                                      face_hint != nullptr, is_boundary);
