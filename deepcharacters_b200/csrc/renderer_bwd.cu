@@ -40,6 +40,7 @@ struct BwdArgs {
     int B, C, N, F;
     long long Tb_frame;      // adjoint tiles per frame (all cameras)
     FastDiv fd_frame;        // division by Tb_frame (the call has < 2^31 adjoint tiles)
+    FastDiv fd_est;          // division by the staged tile edge BT + 2 ifs
     const int* tile_cam_b;   // camera of each adjoint tile of a frame
     int albedo, shading;
     int ifs, tfs;
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         const int cx0 = (int)gc.fd_tiles_x_b.mod(gtile, gc.fd_tiles_x_b.div(gtile)) * BT - A.ifs;
         const int off = 3 * cx0 - ((3 * cx0) & ~3);  // floats before the first halo column in a box row
         for (int i = threadIdx.x; i < e_st * e_st; i += BNT) {
-            const int r = i / e_st, c = i - r * e_st;
+            const int r = (int)A.fd_est.div((unsigned)i), c = i - r * e_st;
             const float* q = s_raw + r * kRawX + off + 3 * c;
             s_tgt2[buf][i] = make_float4(q[0], q[1], q[2], 0.f);
         }
@@ -803,6 +804,7 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.F = topo.F;
     A.Tb_frame = ws.Tb_frame;
     A.fd_frame = FastDiv((unsigned)ws.Tb_frame);
+    A.fd_est = FastDiv((unsigned)(BT + 2 * ifs));
     A.tile_cam_b = ws.tile_cam_b.as<int>();
     A.albedo = albedo;
     A.shading = shading;

@@ -211,7 +211,7 @@ struct BinSink {
     }
 };
 
-__global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int TS, int cap,
+__global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int TS, int ts_shift, int cap,
                       const int3* __restrict__ faces, const float4* __restrict__ proj,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
@@ -269,10 +269,10 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
     const bool nonempty = live && x1 >= x0 && y1 >= y0;
     int tx0 = 0, tx1 = -1, ty0 = 0, ty1 = -1;
     if (nonempty) {
-        tx0 = x0 / TS;
-        tx1 = x1 / TS;
-        ty0 = y0 / TS;
-        ty1 = y1 / TS;
+        tx0 = x0 >> ts_shift;  // TS = 2^ts_shift; the box is non-empty, so x0 <= x1 are >= 0
+        tx1 = x1 >> ts_shift;
+        ty0 = y0 >> ts_shift;
+        ty1 = y1 >> ts_shift;
     }
     const int ntx = tx1 - tx0 + 1;
     const int nt = nonempty ? ntx * (ty1 - ty0 + 1) : 0;
@@ -313,8 +313,8 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
             qfp.b[e] = __shfl_sync(0xffffffffu, fp.b[e], src);
             qfp.c[e] = __shfl_sync(0xffffffffu, fp.c[e], src);
         }
-        const int qtx0 = qx0 / TS, qty0 = qy0 / TS, qntx = qx1 / TS - qtx0 + 1;
-        const int qnt = qntx * (qy1 / TS - qty0 + 1);
+        const int qtx0 = qx0 >> ts_shift, qty0 = qy0 >> ts_shift, qntx = (qx1 >> ts_shift) - qtx0 + 1;
+        const int qnt = qntx * ((qy1 >> ts_shift) - qty0 + 1);
         // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32
         const int step_r = 32 / qntx, step_c = 32 - step_r * qntx;
         int cr = (int)lane / qntx, cc = (int)lane - cr * qntx;
@@ -969,8 +969,10 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     HC_CHECK_LAUNCH();
     HC_REQUIRE(V <= 65535, "too many views in one call (%d)", V);
     HC_REQUIRE(tiles < (1ll << 31), "too many tiles in one call (%lld)", tiles);
+    const int ts_shift = TS == 8 ? 3 : (TS == 16 ? 4 : 5);
+    HC_REQUIRE(TS == (1 << ts_shift), "tile size %d is not 8, 16 or 32", TS);
     k_bin<<<dim3(div_up(F, 256), V), 256, 0, s>>>(
-        V, C, F, N, TS, ws.bin_cap, topo.faces.as<int3>(), ws.proj.as<float4>(), cams, tf, tv, tstate,
+        V, C, F, N, TS, ts_shift, ws.bin_cap, topo.faces.as<int3>(), ws.proj.as<float4>(), cams, tf, tv, tstate,
         ws.bins.as<int>(),
         ws.spill.as<int2>(), ws.spill_cap, ws.spill_keys.as<unsigned long long>(), ws.spill_tile_cap, stats);
     HC_CHECK_LAUNCH();
