@@ -315,9 +315,12 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
         }
         const int qtx0 = qx0 >> ts_shift, qty0 = qy0 >> ts_shift, qntx = (qx1 >> ts_shift) - qtx0 + 1;
         const int qnt = qntx * ((qy1 >> ts_shift) - qty0 + 1);
-        // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32
-        const int step_r = 32 / qntx, step_c = 32 - step_r * qntx;
-        int cr = (int)lane / qntx, cc = (int)lane - cr * qntx;
+        // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32.
+        // floor(a / n) for a <= 32, n <= 4096 from one reciprocal: (a + 1/2) / n
+        // is at least 1/(2n) from an integer, far above the float error
+        const float rq = 1.f / (float)qntx;
+        const int step_r = (int)(32.5f * rq), step_c = 32 - step_r * qntx;
+        int cr = (int)(((float)lane + 0.5f) * rq), cc = (int)lane - cr * qntx;
         for (int k = lane; k < qnt; k += 32) {
             const int tx = qtx0 + cc;
             const int ty = qty0 + cr;

@@ -518,8 +518,10 @@ __device__ __forceinline__ void cov_bin_item(int view, int fi, bool live, int N,
         const int qtx0 = qx0 / kCovTile, qty0 = qy0 / kCovTile, qntx = qx1 / kCovTile - qtx0 + 1;
         const int qnt = qntx * (qy1 / kCovTile - qty0 + 1);
         // lane's tile k = lane + 32 j at (row cr, column cc), stepped by 32
-        const int step_r = 32 / qntx, step_c = 32 - step_r * qntx;
-        int cr = (int)lane / qntx, cc = (int)lane - cr * qntx;
+        // (floor(a / n) for a <= 32 from one reciprocal, as in the raster binning)
+        const float rq = 1.f / (float)qntx;
+        const int step_r = (int)(32.5f * rq), step_c = 32 - step_r * qntx;
+        int cr = (int)(((float)lane + 0.5f) * rq), cc = (int)lane - cr * qntx;
         for (int k = lane; k < qnt; k += 32) {
             const int tx = qtx0 + cc, ty = qty0 + cr;
             cc += step_c;
