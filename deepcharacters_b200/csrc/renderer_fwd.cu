@@ -622,10 +622,10 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     int best_f = 0x7fffffff;
     int ties = 0;
     int best_e = -1;  // bin entry (base + slot) of the winner, -1 when it came from the spill
-    // Each staged chunk is sorted by (back-facing, depth lower bound rounded
-    // down to a multiple of 2^SB) and staged once: its front faces are tested
-    // first, nearest bound first, then its back faces.  A triangle whose rounded bound
-    // exceeds the pixel's current best depth can neither win nor tie, and
+    // Each staged chunk is sorted by (back-facing, depth lower bound) and
+    // staged once: its front faces are tested first, nearest bound first, then
+    // its back faces.  A triangle whose bound exceeds the pixel's current best
+    // depth can neither win nor tie, and
     // neither can any triangle after it in the same run (their bounds are at
     // least as large), so a pixel stops scanning a run there.  The result is
     // the same minimum (depth, id) as one unordered pass.  Per pixel a
@@ -633,7 +633,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
     // column and a row bit mask relative to the tile) and in its conservative
     // footprint.
     //
-    // Sort: 32-bit keys (facing | rounded bound | slot) are distinct; each
+    // Sort: 32-bit keys (facing | bound | slot) are distinct; each
     // warp sorts its 32 keys with a shuffle bitonic network, and a key's rank
     // in the chunk is its lane plus its lower bound in every other warp's
     // sorted keys (5-step binary searches).
@@ -654,11 +654,12 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_r
                     const TriFrame tf = tri_frame[(long long)b * A.F + f];
                     const int x0 = tv.x01 & 0xffff, x1 = tv.x01 >> 16;
                     const int y0 = tv.y01 & 0xffff, y1 = tv.y01 >> 16;
-                    // rounded bound, kept below the all-ones key of an empty slot
-                    const unsigned coarse = min((unsigned)(tv.dqmin & 0x7fffffff) >> SB, (1u << (31 - SB)) - 2u);
+                    // the bound, clamped to the key's 31 - SB bits (exact below ~2^25 quanta, a
+                    // lower bound above) and kept below the all-ones key of an empty slot
+                    const unsigned coarse = min((unsigned)(tv.dqmin & 0x7fffffff), (1u << (31 - SB)) - 2u);
                     t.hdr = make_int4((int)bit_range(max(x0 - tx * TS, 0), min(x1 - tx * TS, TS - 1)),
                                       (int)bit_range(max(y0 - ty * TS, 0), min(y1 - ty * TS, TS - 1)),
-                                      (int)(coarse << SB), f);
+                                      (int)coarse, f);
                     t.ea = tv.e01;
                     t.nm = make_float4(tv.num, tv.e2c.z, tv.e2c.w, tv.e2o.x);
                     t.eb = make_float4(tv.e2c.x, tv.e2c.y, 0.f, 0.f);
