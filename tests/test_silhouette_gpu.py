@@ -1,5 +1,7 @@
 """Camera projection, projected-mesh boundary and the multi-view silhouette
 loss on the GPU against the reference kernels and the FP64 oracle."""
+import os
+
 import numpy as np
 import pytest
 import torch
@@ -253,3 +255,45 @@ def test_fused_squared_loss_matches_the_separate_passes(scene):
     torch.cuda.synchronize()
     assert float(ref.abs().max()) > 0
     assert nrel(out, ref) < 1e-6  # float atomics: equal up to summation order
+
+
+def test_mesh_boundary_with_an_overflowing_coverage_tile():
+    """300 small triangles inside one 8x8 coverage tile: more than its bin
+    holds (256 entries), so the pairs beyond it take the sweep path.  Probe
+    vertices around that tile and the triangles' own vertices get the same
+    flags with no hint and with a hint that names no face (every window
+    left open), the reference kernels' flags, and those of the FP64 oracle up
+    to pixel centres on its tolerance."""
+    from deepcharacters_b200.silhouette import MeshBoundaryEngine
+    W = H = 48
+    rng = np.random.default_rng(17)
+    P, F = [], []
+    for _ in range(300):  # triangles of 1.5-3.5 px inside the pixel square [16, 24)^2
+        c = rng.uniform(16.5, 23.5, 2)
+        i = len(P)
+        for _ in range(3):
+            P.append(tuple(np.clip(c + rng.uniform(-1.75, 1.75, 2), 16.0, 24.0)))
+        F.append((i, i + 1, i + 2))
+    for y in range(12, 29, 2):  # probes around the tile
+        for x in range(12, 29, 2):
+            P.append((x + 0.25, y + 0.75))
+    faces = np.asarray(F, np.int32)
+    N = len(P)
+    # points at z = 1000 mm seen by a camera with a 1000 px focal length land on (u, v)
+    pts = np.concatenate([np.asarray(P, np.float32), np.full((N, 1), 1000.0, np.float32)], 1)[None]
+    extr = np.asarray([[1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0]], np.float32)
+    intr = np.asarray([[1000, 0, 0, 0, 1000, 0, 0, 0, 1]], np.float32)
+    eng = MeshBoundaryEngine(faces, N)
+    ours = eng.forward(_t(pts), _t(extr), _t(intr), W, H).clone()
+    hint = torch.full((1, 1, H, W), -1, dtype=torch.int32, device=DEV)
+    hinted = eng.forward(_t(pts), _t(extr), _t(intr), W, H, face_hint=hint)
+    torch.cuda.synchronize()
+    assert torch.equal(ours, hinted)
+    flags = ours.cpu().numpy()
+    assert 0 < int(flags.sum()) < N  # covered and open windows both occur
+    if O.ref_available() and os.path.exists(O.REF_MB_LIB):
+        ref = O.ref_mesh_boundary(faces, _t(pts), _t(extr), _t(intr), W, H)
+        assert torch.equal(ours, ref.to(ours.device).view_as(ours))
+    p2d = SO.project(pts, None, extr, intr, True)
+    ora = SO.mesh_boundary(faces, p2d, W, H)
+    assert int((flags != ora).sum()) <= 2  # FP64 differs only where a centre sits on the tolerance
