@@ -128,6 +128,8 @@ class DeformRenderChain:
             self.buf.update(weights=self.skin_w.unsqueeze(0).expand(B, N, K).contiguous(), gjp=e(B, self.skin.J, 3),
                             gja=e(B, self.skin.J, 3), dq=e(B, self.skin.S, 8), outw=e(B, N, K), gw=e(B, N, K))
         self.loss = torch.zeros((3,), device=dev)
+        # the stream of the silhouette branch (step)
+        self._side = torch.cuda.Stream(device=self.loss.device) if self.loss.is_cuda else None
         self.ws = torch.zeros((8,), device=dev, dtype=torch.float64)
 
     def forward(self):
@@ -190,10 +192,11 @@ class DeformRenderChain:
         L("hc_camera_projection_backward", s, B, C, N, P(o["gp2d"]), P(o["v"]), P(i["extr"]), P(i["intr"]), 1,
           P(o["gv_sil"]))
 
-    def backward(self):
+    def backward(self, join=None):
         """Raster adjoint, the sum of the two vertex-position gradients, then the
         deformation's adjoint: EG (and the node-skinning adjoint to the joint
-        angles), or the vertex DQ skinning's to the joint angles."""
+        angles), or the vertex DQ skinning's to the joint angles.  ``join``: a
+        stream whose work (the silhouette branch) the sum waits for."""
         L, P, s = _lib.call, _lib.ptr, _stream()
         i, o = self.inp, self.buf
         B, N = self.B, self.N
@@ -205,6 +208,8 @@ class DeformRenderChain:
             L("hc_renderer_backward", self.rend.handle, s, B, P(o["grad_img"]), P(o["v"]), P(i["colors"]),
               P(i["texture"]), *self.tex_hw, P(i["sh"]), P(i["target"]), P(o["vnormal"]), P(o["bary"]),
               P(o["face"]), P(i["extr"]), P(i["intr"]), P(o["gv"]), P(o["gcol"]), None, P(o["gsh"]))
+        if join is not None:
+            torch.cuda.current_stream().wait_stream(join)
         L("hc_add_inplace", s, B * N * 3, P(o["gv"]), P(o["gv_sil"]))
         if self.deformation == "dq":  # joint angles (and skin weights) through the vertex DQ skinning
             L("hc_dq_skinning_backward", self.skin.handle, s, B, P(o["gv"]), P(o["v"]), P(o["gjp"]), P(o["gja"]),
@@ -253,10 +258,23 @@ class DeformRenderChain:
         return self.rend.stats()
 
     def step(self):
+        """One training step.  After the forward stage the silhouette branch
+        (boundary, loss and its adjoint) and the raster adjoint are independent
+        until their vertex-position gradients are summed, so the silhouette
+        branch runs on a second stream beside the raster adjoint (its kernels
+        wait on gathers and leave issue slots that the adjoint uses), joined
+        before the sum; a captured graph keeps the two branches."""
         self.forward()
-        self.silhouette_forward()
-        self.silhouette_backward()
-        self.backward()
+        if self.loss.is_cuda:
+            self._side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(self._side):
+                self.silhouette_forward()
+                self.silhouette_backward()
+            self.backward(join=self._side)
+        else:
+            self.silhouette_forward()
+            self.silhouette_backward()
+            self.backward()
 
     def capture_step(self, inputs: dict | None = None) -> torch.cuda.CUDAGraph:
         """Capture one step (forward, silhouette, both adjoints) in a CUDA
