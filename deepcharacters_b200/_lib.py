@@ -33,6 +33,7 @@ _SIGS: dict[str, list] = {
                                vp, vp, vp],
     "hc_renderer_stats": [vp, vp, c_i64_p, c_i64_p],
     "hc_renderer_set_gradient_parity": [vp, C.c_int32],
+    "hc_renderer_set_adjoint_schedule": [vp, C.c_int32],
     "hc_eg_create": [C.POINTER(vp), C.c_int32, vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                      C.c_int32, vp, vp],
     "hc_eg_destroy": [vp],

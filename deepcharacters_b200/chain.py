@@ -128,8 +128,11 @@ class DeformRenderChain:
             self.buf.update(weights=self.skin_w.unsqueeze(0).expand(B, N, K).contiguous(), gjp=e(B, self.skin.J, 3),
                             gja=e(B, self.skin.J, 3), dq=e(B, self.skin.S, 8), outw=e(B, N, K), gw=e(B, N, K))
         self.loss = torch.zeros((3,), device=dev)
-        # the stream of the silhouette branch (step)
+        # the stream of the silhouette branch (step), and the adjoint's static
+        # tile schedule, under which CTAs that run out early make room for it
         self._side = torch.cuda.Stream(device=self.loss.device) if self.loss.is_cuda else None
+        if self._side is not None:
+            _lib.call("hc_renderer_set_adjoint_schedule", self.rend.handle, 0)
         self.ws = torch.zeros((8,), device=dev, dtype=torch.float64)
 
     def forward(self):

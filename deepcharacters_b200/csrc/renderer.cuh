@@ -395,6 +395,8 @@ struct RasterWorkspace {
     DevBuf proj;  // float4 [V,N]: projected vertices of the current call
     DevBuf l1_part;  // per raster tile: float L1 sum, unsigned count (fused L1 only)
     DevBuf claim;    // the tile resolve's tile counter
+    DevBuf claim_b;  // the adjoint's tile counter
+    int adjoint_dynamic = 1;  // the adjoint's tile schedule (hc_renderer_set_adjoint_schedule)
     KernelClock clock;
 };
 

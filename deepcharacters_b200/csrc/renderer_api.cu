@@ -368,6 +368,13 @@ extern "C" hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t pari
     return HC_OK;
 }
 
+extern "C" hc_status hc_renderer_set_adjoint_schedule(hc_renderer h, int32_t dynamic) {
+    clear_error();
+    HC_REQUIRE(h, "invalid handle");
+    h->ws.adjoint_dynamic = dynamic ? 1 : 0;
+    return HC_OK;
+}
+
 extern "C" hc_status hc_renderer_set_kernel_timing(hc_renderer h, int32_t enable) {
     clear_error();
     HC_REQUIRE(h, "invalid handle");

@@ -66,6 +66,7 @@ struct BwdArgs {
     const L1State* l1_state;
     const float* l1_render;          // [V,H,W,3]
     int* err;                        // bit 2: a target copy did not complete (RasterStats::overflow)
+    unsigned* claim;                 // tile counter of the persistent CTAs (cleared before the launch)
     const unsigned char* l1_mask;    // [V,H,W] or NULL
 };
 
@@ -232,7 +233,7 @@ __device__ __forceinline__ void taps_fs(const float4* s_tgt, int s0, float3 G, f
 // whose albedo has no parameters (normal, lighting, mask, position, depth, uv).
 enum { kAlbVcol = 0, kAlbTex = 1, kAlbNone = 2, kAlbTexBilinear = 3 };
 
-template <bool SHADED, int ALB, bool PARITY>
+template <bool SHADED, int ALB, bool PARITY, bool DYN>
 __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, const ViewCam* __restrict__ cams, long long n_tiles,
                                                                      const __grid_constant__ CUtensorMap tmap,
                                                                      int use_tma) {
@@ -321,19 +322,32 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tma_box(&tmap, smem_u32(s_raw), smem_u32(&s_mbar), x, y, sv, raw_bytes);
     };
-    if (tma) {
-        if (threadIdx.x == 0) {
+    // Tiles are taken one ahead (the next tile's target copy is issued while
+    // this one is processed).  DYN: the CTAs claim tiles from a counter, so
+    // tiles of uneven cost balance and a CTA that starts late takes fewer
+    // (thread 0 writes the ring slot of the next iteration; a barrier
+    // separates every write of a slot from its reads).  Static: CTA i takes
+    // tiles i, i + grid, ..., and CTAs that run out early free their SM for
+    // concurrent work.
+    __shared__ int s_claimed[2];
+    if (threadIdx.x == 0) {
+        if constexpr (DYN) s_claimed[0] = (int)atomicAdd(A.claim, 1u);
+        if (tma) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)) : "memory");
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
-        __syncthreads();
-        if (threadIdx.x == 0 && (long long)blockIdx.x < n_tiles) tma_issue(blockIdx.x);
-    } else if (staged && (long long)blockIdx.x < n_tiles) {
-        stage(blockIdx.x, 0);
+    }
+    if (DYN || tma) __syncthreads();
+    long long g;
+    if constexpr (DYN) g = s_claimed[0];
+    else g = blockIdx.x;
+    if (tma) {
+        if (threadIdx.x == 0 && g < n_tiles) tma_issue(g);
+    } else if (staged && g < n_tiles) {
+        stage(g, 0);
     }
     asm volatile("cp.async.commit_group;\n" ::);
-    int it = 0;
-    for (long long g = blockIdx.x; g < n_tiles; g += gridDim.x, ++it) {
+    for (int it = 0; g < n_tiles; ++it) {  // CTA-uniform
     const int buf = tma ? 0 : it & 1;
     const float4* s_tgt = s_tgt2[buf];
     if (tma) {
@@ -356,9 +370,26 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
             s_tgt2[buf][i] = make_float4(q[0], q[1], q[2], 0.f);
         }
         __syncthreads();
-        if (threadIdx.x == 0 && g + gridDim.x < n_tiles) tma_issue(g + gridDim.x);
-    } else if (staged && g + gridDim.x < n_tiles) {
-        stage(g + gridDim.x, buf ^ 1);
+        if (threadIdx.x == 0) {
+            long long nx;
+            if constexpr (DYN) {
+                nx = atomicAdd(A.claim, 1u);
+                s_claimed[(it + 1) & 1] = (int)nx;
+            } else {
+                nx = g + gridDim.x;
+            }
+            if (nx < n_tiles) tma_issue(nx);
+        }
+    } else {
+        long long nx;
+        if constexpr (DYN) {
+            if (threadIdx.x == 0) s_claimed[(it + 1) & 1] = (int)atomicAdd(A.claim, 1u);
+            __syncthreads();  // every thread stages the next tile
+            nx = s_claimed[(it + 1) & 1];
+        } else {
+            nx = g + gridDim.x;
+        }
+        if (staged && nx < n_tiles) stage(nx, buf ^ 1);
     }
     asm volatile("cp.async.commit_group;\n" ::);
     const unsigned fb = A.fd_frame.div((unsigned)g);
@@ -688,6 +719,8 @@ __global__ void __launch_bounds__(BNT, SHADED ? 2 : 4) k_render_grad(BwdArgs A, 
         }
     }
     __syncthreads();  // the next iteration's prefetch reuses this tile's buffer
+    if constexpr (DYN) g = s_claimed[(it + 1) & 1];
+    else g += gridDim.x;
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
@@ -835,6 +868,10 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
     A.l1_mask = l1 ? l1->mask : nullptr;
     const long long tiles = (long long)B * ws.Tb_frame;
     HC_REQUIRE(tiles < (1ll << 31), "too many adjoint tiles in one call (%lld)", tiles);
+    HC_TRY(ws.claim_b.ensure(sizeof(unsigned)));
+    A.claim = ws.claim_b.as<unsigned>();
+    const bool dyn = ws.adjoint_dynamic != 0;
+    if (dyn) HC_CUDA(cudaMemsetAsync(A.claim, 0, sizeof(unsigned), s));
     // the target's tensor map for the TMA staging, where its layout allows it
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
@@ -845,10 +882,14 @@ hc_status raster_backward(const Topology& topo, RasterWorkspace& ws, DevBuf& nrm
                     : albedo == kTexturedBilinear ? kAlbTexBilinear : kAlbNone;
     const int sel = (shaded ? 8 : 0) + alb * 2 + (parity ? 1 : 0);
     switch (sel) {
-#define HC_GRAD_CASE(SH, AL, PA) \
-    case (SH ? 8 : 0) + AL * 2 + PA:                                                                    \
-        k_render_grad<SH, AL, PA><<<persistent_grid(k_render_grad<SH, AL, PA>, tiles), BNT, 0, s>>>(A, cams, \
-                                                                                              tiles, tmap, use_tma); \
+#define HC_GRAD_CASE(SH, AL, PA)                                                                              \
+    case (SH ? 8 : 0) + AL * 2 + PA:                                                                          \
+        if (dyn)                                                                                              \
+            k_render_grad<SH, AL, PA, true><<<persistent_grid(k_render_grad<SH, AL, PA, true>, tiles), BNT, 0, s>>>( \
+                A, cams, tiles, tmap, use_tma);                                                               \
+        else                                                                                                  \
+            k_render_grad<SH, AL, PA, false><<<persistent_grid(k_render_grad<SH, AL, PA, false>, tiles), BNT, 0, s>>>( \
+                A, cams, tiles, tmap, use_tma);                                                               \
         break;
         HC_GRAD_CASE(false, kAlbVcol, false)
         HC_GRAD_CASE(false, kAlbVcol, true)

@@ -128,6 +128,12 @@ class RendererEngine:
         """True: the reference's barycentric-Jacobian formula; False (default): exact closed form."""
         _lib.call("hc_renderer_set_gradient_parity", self._h, int(bool(parity)))
 
+    def set_adjoint_schedule(self, dynamic: bool):
+        """True (default): the adjoint's CTAs claim tiles from a counter; False:
+        a fixed tile stride per CTA (leaves SMs free early for work running
+        concurrently on another stream).  Same results either way."""
+        _lib.call("hc_renderer_set_adjoint_schedule", self._h, int(bool(dynamic)))
+
     def stats(self) -> tuple[int, int]:
         b = C.c_int64()
         s = C.c_int64()

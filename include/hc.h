@@ -196,6 +196,15 @@ hc_status hc_renderer_backward_l1(hc_renderer h, void* stream, int32_t batch, co
 hc_status hc_renderer_set_gradient_parity(hc_renderer h, int32_t parity);
 
 /*
+ * Tile schedule of the adjoint's persistent CTAs (no reference counterpart).
+ * 1 (default): the CTAs claim tiles from a counter, which balances tiles of
+ * uneven cost; 0: CTA i takes tiles i, i + grid, ..., so CTAs that run out
+ * early free their SM, which serves a caller that runs independent work on
+ * another stream at the same time.  Results are the same either way.
+ */
+hc_status hc_renderer_set_adjoint_schedule(hc_renderer h, int32_t dynamic);
+
+/*
  * Raster statistics of the last forward on this handle: triangle/tile pairs
  * binned and pairs that overflowed a tile bin and took the atomic spill path.
  * Synchronises `stream`; host output pointers, either may be NULL.

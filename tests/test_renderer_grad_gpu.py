@@ -132,3 +132,28 @@ def test_backward_through_autograd_matches_direct_call():
     assert verts.grad is not None and float(verts.grad.abs().sum()) > 0
     assert float(colors.grad.abs().sum()) > 0
     assert float(target.grad.abs().max()) == 0 and float(extr.grad.abs().max()) == 0
+
+
+@pytest.mark.parametrize("parity", [False, True])
+def test_adjoint_tile_schedules_agree(parity):
+    """The dynamic (counter) and static (strided) tile schedules of the adjoint's
+    persistent CTAs give the same gradients, up to the order of float atomics."""
+    sc = S.render_scene(5, batch=2, views=3, width=160, height=128, seed=9)
+    eng = RendererEngine(sc["faces"], sc["texcoords"], sc["N"], 3, 160, 128, "vertexColor", "shaded", 2, 2)
+    eng.set_gradient_parity(parity)
+    verts, colors, tex, sh = _t(sc["verts"]), _t(sc["colors"]), _t(sc["texture"]), _t(sc["sh"])
+    extr, intr, target = _t(sc["extr"]), _t(sc["intr"]), _t(sc["target"])
+    bary, face, render, vnormal = eng.forward(verts, colors, tex, sh, extr, intr)[:4]
+    g = torch.randn(render.shape, device=DEV, generator=torch.Generator(DEV).manual_seed(2))
+    out = {}
+    for dyn in (True, False):
+        eng.set_adjoint_schedule(dyn)
+        out[dyn] = [t.clone() if t is not None else None for t in
+                    renderer_backward(eng, g, verts, colors, tex, sh, target, vnormal, bary, face, extr, intr)]
+    torch.cuda.synchronize()
+    assert int((face >= 0).sum()) > 1000
+    for a, b in zip(out[True], out[False]):
+        if a is None:
+            continue
+        assert float(b.abs().max()) > 0
+        assert nrel(a, b) < 1e-6
