@@ -224,17 +224,14 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
     const long long i = (long long)view * F + fi;
     int f = 0;
     int x0 = 0, x1 = -1, y0 = 0, y1 = -1;
-    int W = 0, H = 0, tiles_x = 1;
-    long long tile_base = 0;
+    // the view is the block's (grid y), so its image and tile grid are the same in every lane
+    const ViewCam& cam = cams[view];
+    const int W = cam.W, H = cam.H, tiles_x = cam.tiles_x;
+    const long long tile_base = cam.tile_base;
     Footprint fp;
     if (live) {
         f = fi;
         const int b = view / C;
-        const ViewCam& cam = cams[view];
-        W = cam.W;
-        H = cam.H;
-        tiles_x = cam.tiles_x;
-        tile_base = cam.tile_base;
         const int3 id = faces[f];
         const float4* PV = proj + (long long)view * N;
         const float4 q0 = PV[id.x], q1 = PV[id.y], q2 = PV[id.z];
@@ -301,9 +298,9 @@ __global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int 
     while (pending) {
         const int src = __ffs(pending) - 1;
         pending &= pending - 1;
-        const int qv = __shfl_sync(0xffffffffu, view, src), qf = __shfl_sync(0xffffffffu, f, src);
-        const int qtiles_x = __shfl_sync(0xffffffffu, tiles_x, src);
-        const long long qbase = __shfl_sync(0xffffffffu, tile_base, src);
+        const int qv = view, qf = __shfl_sync(0xffffffffu, f, src);
+        const int qtiles_x = tiles_x;
+        const long long qbase = tile_base;
         const int qx0 = __shfl_sync(0xffffffffu, x0, src), qx1 = __shfl_sync(0xffffffffu, x1, src);
         const int qy0 = __shfl_sync(0xffffffffu, y0, src), qy1 = __shfl_sync(0xffffffffu, y1, src);
         Footprint qfp;
