@@ -166,10 +166,9 @@ __global__ void k_project_vertices(int V, int C, int N, const float* __restrict_
 //
 // The pixel bbox is the reference's projectFacesDevice (CUDABasedRasterization.cu:
 // 184-208): projected vertex extent +-0.5 px, clamped to the image, truncated to
-// int.  Each (view, triangle) appends itself to every tile its bbox touches.
-// Lanes of a warp that hit the same tile share one atomicAdd on the tile
-// counter (match + ballot + popc); entries beyond the tile's capacity go to
-// the spill list.
+// int.  Each (view, triangle) appends itself to every tile its bbox touches
+// and its footprint reaches, taking a slot with one atomicAdd on the tile's
+// counter; entries beyond the tile's capacity go to the spill list.
 // ---------------------------------------------------------------------------
 constexpr int kBinSmall = 9;  // tiles a thread bins on its own (a 3x3 box of tiles)
 
@@ -211,7 +210,7 @@ struct BinSink {
     }
 };
 
-__global__ void __launch_bounds__(256, 5) k_bin(int V, int C, int F, int N, int TS, int ts_shift, int cap,
+__global__ void __launch_bounds__(256, 6) k_bin(int V, int C, int F, int N, int TS, int ts_shift, int cap,
                       const int3* __restrict__ faces, const float4* __restrict__ proj,
                       const ViewCam* __restrict__ cams, const TriFrame* __restrict__ tri_frame,
                       TriView* __restrict__ tri_view, int2* __restrict__ tile_state, int* __restrict__ bins,
@@ -566,7 +565,7 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
 }
 
 template <int TS>
-__global__ void __launch_bounds__(TS* TS, TS == 8 ? 18 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, FastDiv fd_frame,
+__global__ void __launch_bounds__(TS* TS, TS == 8 ? 20 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, FastDiv fd_frame,
                                                    const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
                                                    const TriFrame* __restrict__ tri_frame,
