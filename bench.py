@@ -529,8 +529,7 @@ def run_ours_c3(args, world, rank, local):
     parity = args.adjoint == "parity"
     ch = DeformRenderChain(sc, dev, frames, VIEWS, ws, hs, W_SIL, W_SIL1, gradient_parity=parity, deformation="dq")
     gcol_shared = torch.zeros((sc["N"], 3), device=dev)
-    cands = ((8, 128), (8, 256), (16, 256), (16, 512), (32, 512), (32, 1024))
-    tune = ch.autotune(cands) if not args.no_autotune else {}
+    tune = ch.autotune() if not args.no_autotune else {}
     binned, spilled = ch.check()
     for _ in range(2):
         ch.step()

@@ -226,7 +226,8 @@ class DeformRenderChain:
             L("hc_pose2eg_backward", self.skin.handle, s, B, P(i["dofs"]), self.M, P(self.node_vertex),
               P(self.skin_w), P(o["gsT"]), P(o["gsA"]), P(o["gdofs"]))
 
-    def autotune(self, candidates=((8, 128), (8, 256), (16, 256), (16, 512), (32, 512), (32, 1024)), reps: int = 3):
+    def autotune(self, candidates=((8, 128), (8, 256), (8, 512), (8, 1024), (16, 256), (16, 512), (16, 1024),
+                                   (32, 512), (32, 1024)), reps: int = 3):
         """Pick the raster's bin-tile size and bin capacity by timing the
         forward stage on the current inputs (CUDA events, after a warm-up
         call per candidate); candidates whose spill capacity overflows are
