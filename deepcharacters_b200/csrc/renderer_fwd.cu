@@ -564,7 +564,10 @@ __device__ __forceinline__ unsigned bit_range(int lo, int hi) {
     return hi < lo ? 0u : ((2u << hi) - 1u) & ~((1u << lo) - 1u);
 }
 
-template <int TS>
+// TIES: the call asked for the per-pixel count of hits at the winning depth
+// (diagnostics); without it the count is compiled out, which frees a register
+// of the scan and shortens its updates
+template <int TS, bool TIES>
 __global__ void __launch_bounds__(TS* TS, TS == 8 ? 20 : (TS == 16 ? 5 : 1)) k_resolve(ShadeArgs A, FastDiv fd_frame,
                                                    const int* __restrict__ tile_cam, int cap,
                                                    const ViewCam* __restrict__ cams,
@@ -770,7 +773,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 20 : (TS == 16 ? 5 : 1)) k_r
             A.render[3 * pix + 1] = 0.f;
             A.render[3 * pix + 2] = 0.f;
             if (A.depth_q) A.depth_q[pix] = 0x7fffffff;
-            if (A.tie_count) A.tie_count[pix] = 0;
+            if (TIES) A.tie_count[pix] = 0;
         } else {
             // the fused L1's target, loaded before this pixel's stores (which
             // the compiler may not move it past)
@@ -806,7 +809,7 @@ __global__ void __launch_bounds__(TS* TS, TS == 8 ? 20 : (TS == 16 ? 5 : 1)) k_r
             A.render[3 * pix + 1] = col.y;
             A.render[3 * pix + 2] = col.z;
             if (A.depth_q) A.depth_q[pix] = (int)best_d;
-            if (A.tie_count) A.tie_count[pix] = ties;
+            if (TIES) A.tie_count[pix] = ties;
             if (l1m) {
                 const float d0 = l1_diff(col.x, tg.x), d1 = l1_diff(col.y, tg.y), d2 = l1_diff(col.z, tg.z);
                 l1s = fabsf(d0) + fabsf(d1) + fabsf(d2);
@@ -1029,8 +1032,14 @@ hc_status raster_forward(const Topology& topo, RasterWorkspace& ws, cudaStream_t
     ws.clock.begin(kKResolve, s);
 #define HC_RESOLVE_CASE(TSV)                                                                                   \
     case TSV:                                                                                                  \
-        k_resolve<TSV><<<resident_grid(k_resolve<TSV>, TSV * TSV, tiles), TSV * TSV, 0, s>>>(                  \
-            A, FastDiv((unsigned)ws.T_frame), tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill, ws.spill_tile_cap, tiles, claim); \
+        if (A.tie_count)                                                                                       \
+            k_resolve<TSV, true><<<resident_grid(k_resolve<TSV, true>, TSV * TSV, tiles), TSV * TSV, 0, s>>>(  \
+                A, FastDiv((unsigned)ws.T_frame), tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill,       \
+                ws.spill_tile_cap, tiles, claim);                                                              \
+        else                                                                                                   \
+            k_resolve<TSV, false><<<resident_grid(k_resolve<TSV, false>, TSV * TSV, tiles), TSV * TSV, 0, s>>>( \
+                A, FastDiv((unsigned)ws.T_frame), tcam, ws.bin_cap, cams, tf, tv, tstate, kbins, kspill,       \
+                ws.spill_tile_cap, tiles, claim);                                                              \
         break;
     switch (TS) {
         HC_RESOLVE_CASE(8)
