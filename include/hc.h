@@ -580,7 +580,8 @@ hc_status hc_silhouette_backward_scaled_sized(void* stream, int32_t batch, int32
  *   4 * (B*C * (3 * (ceil(U/30)+3) * (ceil(V/30)+3) + N) + 1) <= 8 MiB,
  * e.g. 8 views of 1024x1024 with N = 40,962; larger calls return
  * HC_ERR_INVALID.  The first call on a device resolves the array's device
- * address with that device current.  All calls on a device share the one array and it keeps the last call's contents: calls
+ * address with that device current; make that first call before any stream
+ * capture begins.  All calls on a device share the one array and it keeps the last call's contents: calls
  * whose kernels overlap on the GPU (e.g. issued on different streams) race,
  * so order them on one stream.
  */
